@@ -1,0 +1,537 @@
+"""B200 Cunningham-chain search engine: Python host side over the C ABI.
+
+The compute path is libccs.so (hand-written sm_100a CUDA behind include/ccs.h);
+this module only marshals arguments.  There is no CPU fallback: every compute
+call raises when the shared library or a GPU is missing.
+
+Names follow the reference (nmicic/cunningham-chain-search) where a
+counterpart exists: compute_forbidden_residues (v13:771), Engine.bases
+(generate_bases, v13:907), Engine.filter_range (one K1 batch, v13:1551 /
+3764-3795), Engine.prove (K2 / prove_survivors_mt, v13:1462 / 1967),
+format_chain_line (v13:2030-2033).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libccs.so")
+
+# status codes (include/ccs.h)
+OK, ERR_INVALID, ERR_CUDA, OVERFLOW, ERR_NOMEM, ERR_TIMEOUT, ERR_BUSY, ERR_NOT_FOUND, \
+    ERR_CANCELLED, PENDING = range(10)
+STATUS_NAMES = ["OK", "ERR_INVALID", "ERR_CUDA", "OVERFLOW", "ERR_NOMEM", "ERR_TIMEOUT",
+                "ERR_BUSY", "ERR_NOT_FOUND", "ERR_CANCELLED", "PENDING"]
+
+PRIME_MR, PRIME_BPSW = 0, 1
+PROVE_ROOTS, PROVE_FULL = 0, 1
+CHAIN_IS_ROOT, CHAIN_TARGET = 1, 2
+
+# reference parameter set (src/cuda/cc18_filter_cuda_CpC_v13.cu:174-201)
+REF_CRT = (5, 7, 11, 13, 17, 19)
+REF_WHEEL = (23, 29, 31)
+REF_L2 = (37, 41, 43, 47, 53, 59, 61)
+REF_EXT = (67, 71, 73, 79, 83, 89, 97)
+V13_WITNESSES = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71)
+
+
+def primes_in(lo, hi):
+    """primes p with lo <= p < hi"""
+    if hi <= 2:
+        return []
+    s = np.ones(hi, dtype=bool)
+    s[:2] = False
+    for p in range(2, int(hi ** 0.5) + 1):
+        if s[p]:
+            s[p * p::p] = False
+    return [int(p) for p in np.nonzero(s)[0] if p >= lo]
+
+
+REF_LINE = tuple(primes_in(101, 864))
+
+
+def reference_stages():
+    """L2 37..61 and ext-L2 67..97 from position 0, line sieve 101..863 from
+    position 1 (v13:793-846)."""
+    return [(REF_L2, 0), (REF_EXT, 0), (REF_LINE, 1)]
+
+
+def compute_forbidden_residues(q, chain_len, pos_lo=0):
+    """Residues n mod q that make some chain member p_i = 2^i (n+1) - 1,
+    i in [pos_lo, min(chain_len, q)), divisible by q (v13:771-787)."""
+    out = set()
+    inv2 = (q + 1) // 2
+    x = 1
+    for i in range(min(chain_len, q)):
+        if i >= pos_lo:
+            out.add((x - 1) % q)
+        x = x * inv2 % q
+    return sorted(out)
+
+
+class CCSError(RuntimeError):
+    def __init__(self, status, msg):
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"{name}: {msg}")
+        self.status = status
+
+
+# ---------------------------------------------------------------------------
+# ctypes structures (mirror include/ccs.h)
+# ---------------------------------------------------------------------------
+class _Stage(C.Structure):
+    _fields_ = [("primes", C.POINTER(C.c_uint32)), ("n_primes", C.c_uint32),
+                ("pos_lo", C.c_uint32)]
+
+
+class _Params(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("target", C.c_uint32), ("depth", C.c_uint32),
+                ("bits", C.c_uint32),
+                ("crt_primes", C.POINTER(C.c_uint32)), ("n_crt", C.c_uint32),
+                ("wheel_primes", C.POINTER(C.c_uint32)), ("n_wheel", C.c_uint32),
+                ("stages", C.POINTER(_Stage)), ("n_stages", C.c_uint32),
+                ("max_bases", C.c_uint32),
+                ("witnesses", C.POINTER(C.c_uint64)), ("n_witnesses", C.c_uint32),
+                ("primality", C.c_uint32), ("prove_mode", C.c_uint32), ("flags", C.c_uint32)]
+
+
+class _Info(C.Structure):
+    _fields_ = [("lattice_m", C.c_uint64), ("wheel_period", C.c_uint32), ("n_bases", C.c_uint32),
+                ("n_lines", C.c_uint64), ("candidates_per_tile", C.c_uint64),
+                ("target", C.c_uint32), ("depth", C.c_uint32), ("bits", C.c_uint32),
+                ("n_filter_primes", C.c_uint32), ("expected_tests", C.c_double),
+                ("pass_rate", C.c_double), ("launches", C.c_uint64)]
+
+
+class _Range(C.Structure):
+    _fields_ = [("tile_start_lo", C.c_uint64), ("tile_start_hi", C.c_uint64),
+                ("n_tiles", C.c_uint64), ("profile", C.c_uint32), ("bits", C.c_uint32)]
+
+
+class _RangeResult(C.Structure):
+    _fields_ = [("n_survivors", C.c_uint64), ("n_chains", C.c_uint64), ("n_primes", C.c_uint64),
+                ("candidates", C.c_uint64), ("surv_offset", C.c_uint64),
+                ("chain_offset", C.c_uint64), ("status", C.c_uint32), ("_pad", C.c_uint32)]
+
+
+class _Tuning(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("unit_words", C.c_uint32), ("split_prime", C.c_uint32)]
+
+
+# exported symbols of include/ccs.h, with their ctypes signatures
+_vp = C.c_void_p
+_u64 = C.c_uint64
+_SIGS = {
+    "ccs_describe": (C.c_int, [C.POINTER(_Params), C.POINTER(_Info), C.POINTER(_u64), C.c_uint32]),
+    "ccs_create": (C.c_int, [C.POINTER(_Params), C.c_int, C.POINTER(_vp)]),
+    "ccs_destroy": (C.c_int, [_vp]),
+    "ccs_get_info": (C.c_int, [_vp, C.POINTER(_Info)]),
+    "ccs_get_bases": (C.c_int, [_vp, C.POINTER(_u64), C.c_uint32]),
+    "ccs_last_error": (C.c_char_p, []),
+    "ccs_abi_version": (C.c_int, []),
+    "ccs_filter_range": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
+    "ccs_prove": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64),
+                            C.POINTER(_u64), _vp]),
+    "ccs_search_range_host": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp,
+                                        _u64, C.POINTER(_u64), C.POINTER(_u64)]),
+    "ccs_walk_numbers": (C.c_int, [_vp, _vp, _u64, C.c_uint32, _vp, _vp]),
+    "ccs_batch_create": (C.c_int, [C.POINTER(_vp), C.c_uint32, C.c_uint32, _u64, _u64,
+                                   C.POINTER(_vp)]),
+    "ccs_batch_destroy": (C.c_int, [_vp]),
+    "ccs_batch_run": (C.c_int, [_vp, C.POINTER(_Range), C.c_uint32, C.POINTER(_RangeResult),
+                                _vp, _vp, _vp]),
+    "ccs_batch_last_ms": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "ccs_get_tuning": (C.c_int, [_vp, C.POINTER(_Tuning)]),
+    "ccs_measure_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "ccs_set_tuning": (C.c_int, [_vp, C.POINTER(_Tuning)]),
+}
+
+_LIB = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libccs.so; raises when it is missing (no fallback)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise ImportError(f"libccs.so not built at {path}; run cunningham-chain-search_b200/build.py")
+        lib = C.CDLL(path)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def _check(status, what=""):
+    if status != OK:
+        msg = load_library().ccs_last_error().decode(errors="replace")
+        raise CCSError(status, f"{what}: {msg}" if what else msg)
+
+
+def _split128(v):
+    v = int(v)
+    if v < 0 or v >= 1 << 128:
+        raise ValueError("value must be a u128")
+    return v & (2**64 - 1), v >> 64
+
+
+def _u32arr(xs):
+    a = (C.c_uint32 * max(len(xs), 1))(*[int(x) for x in xs])
+    return a
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("a CUDA device is required: the engine has no CPU path")
+    return torch
+
+
+SURVIVOR_DTYPE = np.dtype([("base_idx", "<u4"), ("k_offset", "<u4"), ("tile_idx", "<u4"),
+                           ("_pad", "<u4")])
+CHAIN_DTYPE = np.dtype([("base_idx", "<u4"), ("k_offset", "<u4"), ("tile_idx", "<u4"),
+                        ("chain_len", "<u4"), ("root", "<u4", (6,)), ("flags", "<u4"),
+                        ("survivor", "<u4")])
+
+
+def chain_root_int(rec):
+    return sum(int(x) << (32 * i) for i, x in enumerate(rec["root"]))
+
+
+def format_chain_line(chain_len, root, target, is_root=True):
+    """Reference output line "[TARGET ][NON-ROOT ]CC<len> 0x<HEX> <bits>"
+    (v13:2030-2033)."""
+    tag = ("TARGET " if chain_len >= target else "") + ("" if is_root else "NON-ROOT ")
+    return f"{tag}CC{chain_len} 0x{root:X} {root.bit_length()}"
+
+
+def _make_params(target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, stages=None,
+                 max_bases=0, witnesses=V13_WITNESSES, primality=PRIME_BPSW, prove_mode=PROVE_FULL):
+    """ccs_params plus the buffers it points to (keep both alive)."""
+    if stages is None:
+        stages = reference_stages()
+    keep = []
+    crt_a = _u32arr(crt)
+    wheel_a = _u32arr(wheel)
+    st = (_Stage * len(stages))()
+    for i, (primes, pos_lo) in enumerate(stages):
+        pa = _u32arr(primes)
+        keep.append(pa)
+        st[i].primes = C.cast(pa, C.POINTER(C.c_uint32))
+        st[i].n_primes = len(primes)
+        st[i].pos_lo = pos_lo
+    wit = (C.c_uint64 * max(len(witnesses), 1))(*witnesses)
+    keep += [crt_a, wheel_a, st, wit]
+    p = _Params()
+    p.kind = 1
+    p.target = target
+    p.depth = depth if depth is not None else target
+    p.bits = bits
+    p.crt_primes = C.cast(crt_a, C.POINTER(C.c_uint32))
+    p.n_crt = len(crt)
+    p.wheel_primes = C.cast(wheel_a, C.POINTER(C.c_uint32))
+    p.n_wheel = len(wheel)
+    p.stages = C.cast(st, C.POINTER(_Stage))
+    p.n_stages = len(stages)
+    p.max_bases = max_bases
+    p.witnesses = C.cast(wit, C.POINTER(C.c_uint64))
+    p.n_witnesses = len(witnesses)
+    p.primality = primality
+    p.prove_mode = prove_mode
+    return p, keep
+
+
+def describe(**kw):
+    """Host-only lattice description (ccs_describe): info dict and base list.
+    Needs no GPU."""
+    lib = load_library()
+    p, keep = _make_params(**kw)
+    inf = _Info()
+    cap = 1 << 16
+    bases = (C.c_uint64 * cap)()
+    _check(lib.ccs_describe(C.byref(p), C.byref(inf), bases, cap), "ccs_describe")
+    info = {f: getattr(inf, f) for f, _ in _Info._fields_}
+    return info, [int(bases[i]) for i in range(info["n_bases"])]
+
+
+# configurations named by the workloads they describe
+def config_cc16_scale():
+    """CC18-style GPU filter scale: W = 31#, depth 16, stage primes
+    37..2^10 / 2^10..2^14 / 2^14..2^17 at chain positions 0..15."""
+    return dict(target=16, depth=16, bits=88,
+                stages=[(primes_in(37, 1 << 10), 0), (primes_in(1 << 10, 1 << 14), 0),
+                        (primes_in(1 << 14, 1 << 17), 0)])
+
+
+def config_cpu_method():
+    """The CPU-method lattice: W = 23#, depth 8, primes 29..1021 at positions 0..7."""
+    return dict(target=8, depth=8, bits=64, wheel=(23,), stages=[(primes_in(29, 1022), 0)])
+
+
+class Engine:
+    """One lattice + filter + prover parameter set on one GPU (ccs_create)."""
+
+    def __init__(self, target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, stages=None,
+                 max_bases=0, witnesses=V13_WITNESSES, primality=PRIME_BPSW,
+                 prove_mode=PROVE_FULL, device=0):
+        lib = load_library()
+        if stages is None:
+            stages = reference_stages()
+        p, self._keep = _make_params(target, depth, bits, crt, wheel, stages, max_bases, witnesses,
+                                     primality, prove_mode)
+        h = _vp()
+        _check(lib.ccs_create(C.byref(p), device, C.byref(h)), "ccs_create")
+        self.h = h
+        self.device = device
+        self.target = target
+        self.bits = bits
+        self.stages = stages
+        inf = _Info()
+        _check(lib.ccs_get_info(self.h, C.byref(inf)))
+        self.info = {f: getattr(inf, f) for f, _ in _Info._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().ccs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- lattice facts -----------------------------------------------------
+    def bases(self):
+        n = self.info["n_bases"]
+        a = (C.c_uint64 * n)()
+        _check(load_library().ccs_get_bases(self.h, a, n))
+        return [int(x) for x in a]
+
+    def launches(self):
+        inf = _Info()
+        _check(load_library().ccs_get_info(self.h, C.byref(inf)))
+        return inf.launches
+
+    @property
+    def candidates_per_tile(self):
+        return self.info["candidates_per_tile"]
+
+    def tuning(self):
+        t = _Tuning()
+        _check(load_library().ccs_get_tuning(self.h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in _Tuning._fields_}
+
+    def set_tuning(self, **kw):
+        t = _Tuning()
+        _check(load_library().ccs_get_tuning(self.h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _check(load_library().ccs_set_tuning(self.h, C.byref(t)), "ccs_set_tuning")
+
+    # --- device path -------------------------------------------------------
+    def filter_range(self, tile_start, n_tiles, cap=1 << 20, out=None, stream=None):
+        """Survivors of tiles [tile_start, tile_start + n_tiles) as an int32
+        CUDA tensor [n, 4] (reference Survivor records, uint32 bit patterns).
+        Raises CCSError(OVERFLOW) when more than cap survive."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty((cap, 4), dtype=torch.int32, device=f"cuda:{self.device}")
+        cap = out.shape[0]
+        lo, hi = _split128(tile_start)
+        n = _u64(0)
+        s = stream.cuda_stream if stream is not None else None
+        st = load_library().ccs_filter_range(self.h, lo, hi, int(n_tiles), out.data_ptr(), cap,
+                                             C.byref(n), s)
+        if st == OVERFLOW:
+            raise CCSError(st, f"{n.value} survivors > cap {cap}")
+        _check(st, "ccs_filter_range")
+        return out[: n.value]
+
+    def prove(self, survivors, tile_start, cap=1 << 16, out=None, stream=None):
+        """Chain records [n, 12] (int32) for device survivors; also returns the
+        count of survivors that tested prime."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty((cap, 12), dtype=torch.int32, device=f"cuda:{self.device}")
+        cap = out.shape[0]
+        lo, hi = _split128(tile_start)
+        n = _u64(0)
+        pr = _u64(0)
+        s = stream.cuda_stream if stream is not None else None
+        sv = survivors.contiguous()
+        st = load_library().ccs_prove(self.h, sv.data_ptr() if sv.numel() else None, sv.shape[0],
+                                      lo, hi, out.data_ptr(), cap, C.byref(n), C.byref(pr), s)
+        if st == OVERFLOW:
+            raise CCSError(st, f"{n.value} chains > cap {cap}")
+        _check(st, "ccs_prove")
+        return out[: n.value], pr.value
+
+    def walk_numbers(self, numbers, limbs=6):
+        """Forward chain length of every given int (0 when not prime)."""
+        torch = _torch()
+        arr = np.zeros((len(numbers), limbs), dtype=np.uint32)
+        for i, v in enumerate(numbers):
+            v = int(v)
+            if v.bit_length() > 32 * limbs:
+                raise ValueError("number wider than limbs")
+            for w in range(limbs):
+                arr[i, w] = (v >> (32 * w)) & 0xFFFFFFFF
+        dev = torch.from_numpy(arr.view(np.int32)).to(f"cuda:{self.device}")
+        out = torch.zeros(len(numbers), dtype=torch.int32, device=dev.device)
+        _check(load_library().ccs_walk_numbers(self.h, dev.data_ptr(), len(numbers), limbs,
+                                               out.data_ptr(), None), "ccs_walk_numbers")
+        return out.cpu().numpy().astype(np.int64)
+
+    def walk_numbers_dev(self, numbers_dev, limbs, lengths_dev):
+        _check(load_library().ccs_walk_numbers(self.h, numbers_dev.data_ptr(), numbers_dev.shape[0],
+                                               limbs, lengths_dev.data_ptr(), None))
+
+    # --- host path (reference boundary: host buffers, copies included) -----
+    def search_range_host(self, tile_start, n_tiles, surv_cap=1 << 20, chain_cap=1 << 16):
+        """Filter + prove through host buffers.  Returns (survivors, chains,
+        primes) as numpy structured arrays."""
+        lo, hi = _split128(tile_start)
+        surv = np.zeros(surv_cap, dtype=SURVIVOR_DTYPE)
+        ch = np.zeros(chain_cap, dtype=CHAIN_DTYPE)
+        ns, nc, npr = _u64(0), _u64(0), _u64(0)
+        st = load_library().ccs_search_range_host(
+            self.h, lo, hi, int(n_tiles), surv.ctypes.data, surv_cap, C.byref(ns),
+            ch.ctypes.data, chain_cap, C.byref(nc), C.byref(npr))
+        _check(st, "ccs_search_range_host")
+        return surv[: ns.value], ch[: nc.value], npr.value
+
+    def reconstruct(self, tile_start, base_idx, k_offset, tile_idx, bases=None):
+        """n = ((tile_start + tile_idx) * WP + k_offset) * M + base (v13:1479-1492)."""
+        bases = bases if bases is not None else self.bases()
+        return ((int(tile_start) + int(tile_idx)) * self.info["wheel_period"] + int(k_offset)) \
+            * self.info["lattice_m"] + bases[int(base_idx)]
+
+
+class Batch:
+    """Many uneven ranges in one persistent filter launch + one prove launch,
+    replayed from a CUDA graph (ccs_batch_*)."""
+
+    def __init__(self, engines, max_ranges, surv_cap=1 << 20, chain_cap=1 << 18):
+        lib = load_library()
+        arr = (_vp * len(engines))(*[e.h for e in engines])
+        h = _vp()
+        _check(lib.ccs_batch_create(arr, len(engines), max_ranges, surv_cap, chain_cap, C.byref(h)),
+               "ccs_batch_create")
+        self.h = h
+        self.engines = engines
+        self.max_ranges = max_ranges
+        self.surv_cap = surv_cap
+        self.chain_cap = chain_cap
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().ccs_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, ranges, want_records=True):
+        """ranges: list of (tile_start, n_tiles, profile, bits).  Returns
+        (results list of dicts, survivors, chains); survivor records carry the
+        range index in their last word."""
+        lib = load_library()
+        n = len(ranges)
+        rr = (_Range * max(n, 1))()
+        for i, (ts, nt, prof, bits) in enumerate(ranges):
+            lo, hi = _split128(ts)
+            rr[i].tile_start_lo, rr[i].tile_start_hi = lo, hi
+            rr[i].n_tiles = nt
+            rr[i].profile = prof
+            rr[i].bits = bits
+        res = (_RangeResult * max(n, 1))()
+        surv = np.zeros(self.surv_cap if want_records else 0, dtype=SURVIVOR_DTYPE)
+        ch = np.zeros(self.chain_cap if want_records else 0, dtype=CHAIN_DTYPE)
+        st = lib.ccs_batch_run(self.h, rr, n, res, surv.ctypes.data if want_records else None,
+                               ch.ctypes.data if want_records else None, None)
+        _check(st, "ccs_batch_run")
+        out = [{f: getattr(res[i], f) for f, _ in _RangeResult._fields_} for i in range(n)]
+        ns = sum(o["n_survivors"] for o in out)
+        nc = sum(o["n_chains"] for o in out)
+        return out, surv[:ns], ch[:nc]
+
+    def last_ms(self):
+        ms = C.c_float(0)
+        _check(load_library().ccs_batch_last_ms(self.h, C.byref(ms)))
+        return ms.value
+
+
+# ---------------------------------------------------------------------------
+# range planning (v13:411-518, 3480-3573): bit range, binary prefix, lanes
+# ---------------------------------------------------------------------------
+def parse_prefix(s):
+    """'0b1...' -> (value, bits); same validation as v13 parse_prefix (v13:411-445)."""
+    if not (s.startswith("0b") or s.startswith("0B")):
+        raise ValueError("--prefix must be binary format (0b...)")
+    d = s[2:]
+    if not d:
+        raise ValueError("--prefix has no digits after 0b")
+    if d[0] != "1":
+        raise ValueError("binary prefix must start with 1")
+    if any(ch not in "01" for ch in d):
+        raise ValueError("invalid character in binary prefix")
+    if len(d) > 126:
+        raise ValueError("prefix too long (max 126 bits)")
+    return int(d, 2), len(d)
+
+
+def bit_tile_range(bits, bases, M, WP):
+    """Tiles whose candidates can have `bits` bits (v13:3480-3492):
+    [k_min / WP, k_max / WP + 1)."""
+    n_min, n_max = 1 << (bits - 1), (1 << bits) - 1
+    k_min = (n_min - max(bases)) // M
+    k_max = (n_max - min(bases)) // M
+    return k_min // WP, k_max // WP + 1
+
+
+def prefix_tile_range(bits, prefix_value, prefix_bits, bases, M, WP):
+    """Tiles producing candidates with the given top bits (v13:464-518)."""
+    shift = bits - prefix_bits
+    cmin = prefix_value << shift
+    cmax = ((prefix_value + 1) << shift) - 1
+    vmin, vmax = 1 << (bits - 1), (1 << bits) - 1
+    if cmax < vmin or cmin > vmax:
+        raise ValueError("prefix does not overlap the bit range")
+    cmin, cmax = max(cmin, vmin), min(cmax, vmax)
+    k_min = -(-(cmin - max(bases)) // M) if cmin > max(bases) else 0
+    k_max = (cmax - min(bases)) // M
+    if k_min > k_max:
+        raise ValueError("prefix produces empty k-range")
+    return k_min // WP, k_max // WP + 1
+
+
+def lane_range(tile_min, tile_max, lanes, lane_id):
+    """Contiguous lane lane_id of lanes over [tile_min, tile_max); the
+    remainder goes to the first lanes (v13:3533-3554).  Also the multi-GPU
+    shard function: rank r of N takes lane r."""
+    if not 0 <= lane_id < lanes:
+        raise ValueError("lane id out of range")
+    total = tile_max - tile_min
+    size, rem = divmod(total, lanes)
+    start = tile_min + lane_id * size + min(lane_id, rem)
+    end = start + size + (1 if lane_id < rem else 0)
+    return start, end
+
+
+def measure_int32_peak(device=0):
+    """Measured INT32 ALU issue rate in tera-ops/s (ccs_measure_int32_peak)."""
+    t = C.c_double(0)
+    _check(load_library().ccs_measure_int32_peak(device, C.byref(t)), "ccs_measure_int32_peak")
+    return t.value

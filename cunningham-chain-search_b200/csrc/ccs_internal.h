@@ -1,0 +1,113 @@
+// Internal definitions shared by the host builder and the CUDA kernels.
+//
+// Lattice model.  The reference enumerates n = (tile*WP + k)*M + base with a
+// mod-6 bucket per (tile, base) (v13:1551-1630).  Writing tile = 6J + c shows
+// that every candidate is n = r + J*W with W = 6*M*WP and r = (c*WP + k)*M +
+// base, i.e. one residue r mod W (a "line") per admissible (base, k, c), and J
+// the block index.  The engine sweeps lines along J; the survivor set for a
+// tile range is identical to the reference's, only the visiting order differs.
+//
+// Residue arithmetic runs in "phase space": for a filter prime q with
+// w = W^{-1} mod q, the phase of n is u = n*w mod q = (r*w + J) mod q, which
+// advances by exactly 1 per block.  A candidate is killed by q when u lies in
+// G_q = {f*w mod q : f forbidden}.
+#pragma once
+#include <stdint.h>
+#include <vector>
+#include <string>
+
+namespace ccs {
+
+constexpr int kMaxStages = 4;
+constexpr int kMaxChain = 64;          // v13:164 MAX_CHAIN
+constexpr int kMaxDepth = 32;          // v13:159 MAX_SIEVE_CHAIN_LEN
+constexpr int kMaxLimbs = 6;           // 192-bit chain members
+constexpr int kNumA1 = 9;              // bit-sliced primes q < 64
+constexpr int kNumA2 = 6;              // bit-sliced primes 64 < q < 96 (96-bit windows)
+constexpr int kNumA3 = 7;              // bit-sliced primes 96 < q < 128 (128-bit windows)
+constexpr int kNumA = kNumA1 + kNumA2 + kNumA3;
+constexpr int kMaxProfiles = 8;
+constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
+
+// One bit-sliced ("level A") prime: the 64-candidate kill window is advanced
+// by two shifts per 64 blocks (see filter.cu).
+struct LevelA {
+    uint32_t q;
+    uint32_t s;          // A1: 64 mod q          A2/A3: unused
+    uint32_t t;          // A1: q - s             A2: q - 64   A3: q - 96
+    uint32_t winv;       // W^{-1} mod q
+    uint32_t ext[8];     // 256 bits: bit x = [x mod q in G_q]; all zero = dummy
+};
+
+// Per-prime constants for the per-candidate stages.
+struct PrimeC {
+    uint32_t q;
+    uint32_t magic;      // floor(2^32 / q)
+    uint32_t winv;       // W^{-1} mod q
+    uint32_t c32;        // 2^32 mod q
+    uint32_t off;        // level B: bitmap word offset; level C: list offset
+    uint32_t cnt;        // level C: list length
+    uint64_t magic64;    // floor(2^64 / q) (level C)
+};
+
+// Device line record: residue r mod W and its reference coordinates.
+struct Line {
+    uint32_t r_lo, r_hi;
+    uint32_t k;          // wheel offset (k_offset)
+    uint32_t bc;         // base_idx | (c << 16)   (c = tile mod 6 of the line)
+};
+
+// Constant-memory image of one profile (lattice + filter).
+struct ProfileConst {
+    uint64_t W;                      // 6*M*WP
+    uint32_t n_lines;
+    uint32_t nB, nC;                 // counts of per-candidate primes
+    uint32_t c32W_dummy;
+    LevelA A[kNumA];
+    const Line* lines;
+    const PrimeC* primesB;           // level B primes (ascending)
+    const uint32_t* bitmapB;         // G_q bitmaps of level B primes
+    const PrimeC* primesC;           // level C primes (ascending)
+    const uint32_t* listC;           // sorted G_q lists of level C primes
+};
+
+// Host-side profile (everything derived from ccs_params).
+struct HostProfile {
+    // parameters
+    uint32_t target = 18, depth = 18, bits = 89;
+    std::vector<uint32_t> crt, wheel;
+    struct Stage { std::vector<uint32_t> primes; uint32_t pos_lo; };
+    std::vector<Stage> stages;
+    uint32_t max_bases = 0;
+    std::vector<uint64_t> witnesses;
+    uint32_t primality = 1, prove_mode = 1;
+
+    // lattice
+    uint64_t M = 0, W = 0;
+    uint32_t WP = 0;
+    std::vector<uint64_t> bases;
+    std::vector<uint32_t> tkm6;
+    std::vector<uint32_t> wheel_total;
+    std::vector<Line> lines;
+    uint64_t lines_per_class[6] = {0, 0, 0, 0, 0, 0};
+
+    // filter primes (merged over stages, ascending)
+    struct FPrime { uint32_t q; std::vector<uint32_t> forb; };
+    std::vector<FPrime> fprimes;
+    double expected_tests = 0, pass_rate = 1;
+
+    // device-facing tables
+    LevelA A[kNumA];
+    std::vector<PrimeC> primesB, primesC;
+    std::vector<uint32_t> bitmapB, listC;
+    // index of every level-A/B prime for the per-range J0 mod q table
+    std::vector<uint32_t> range_primes;   // A slots (kNumA, dummies as 1) then B then C
+};
+
+// Builds the lattice and tables; returns "" or an error message.
+std::string build_profile(HostProfile& hp, uint32_t split_prime);
+
+uint32_t mod_inverse_u32(uint32_t a, uint32_t q);
+bool is_prime_u32(uint32_t n);
+
+}  // namespace ccs

@@ -1,0 +1,95 @@
+// Device-side records and launch helpers shared by the engine translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "ccs_internal.h"
+
+namespace ccs {
+
+constexpr int kSweepThreads = 256;
+
+// One lattice range as the device sees it.
+struct RangeDev {
+    uint32_t J0[4];          // floor(tile_start / 6), u128 limbs
+    uint32_t e0;             // tile_start mod 6
+    uint32_t n_tiles;        // tiles in the range (< 2^32)
+    uint32_t n_words;        // ceil(ceil((e0 + n_tiles) / 6) / 64)
+    uint32_t unit_words;     // words per work unit
+    uint32_t profile;        // constant-memory profile slot
+    uint32_t prime_base;     // offset of this profile's prime list (range setup)
+    uint32_t n_range_primes; // kNumA + nB + nC
+    uint32_t surv_cap;       // capacity of surv
+    uint32_t* surv_count;    // device counter (exact count, may exceed cap)
+    uint32_t* surv;          // 4 x u32 records
+    uint32_t* range_count;   // per-range survivor counter (may be null)
+    uint32_t range_id;       // written into the record's last word (0 on the plain path)
+    uint32_t tile_bias;      // added to tile_idx (chunked plain calls)
+};
+
+// header of a sweep launch, read on the device so graphs can be replayed
+struct SweepHeader {
+    uint32_t n_ranges;
+    uint32_t _pad;
+    uint64_t total_units;
+};
+
+// Level-C work queue.
+struct CQueue {
+    uint32_t* count;
+    uint32_t cap;
+    uint4* items;            // {line, j, range, 0}
+};
+
+// Prove-side description of one range.
+struct ProveRange {
+    uint32_t T0[4];          // tile_start (u128 limbs)
+    uint32_t bits;
+    uint32_t profile;
+    uint32_t target;
+    uint32_t _pad;
+    uint32_t* chain_count;   // per-range chain counter (may be null)
+    uint32_t* prime_count;   // per-range prime counter
+};
+
+// Prove launch: survivors of one or many ranges in one flat array.
+struct ProveArgs {
+    const ProveRange* ranges;
+    const uint32_t* surv;          // 4 x u32 records
+    const uint32_t* n_surv_dev;    // device count (null: use n_surv)
+    uint32_t n_surv;
+    uint32_t surv_cap;             // records readable
+    uint32_t range_from_pad;       // 1: record word 3 holds the range index
+    uint32_t* chains;              // 12 x u32 records
+    uint32_t* chain_count;         // global counter
+    uint32_t chain_cap;
+};
+
+// Prover constants per profile (constant memory).
+struct ProveConst {
+    const uint64_t* bases;   // device copy of the base list
+    uint32_t n_bases;
+    uint32_t WP;
+    uint32_t M;
+    uint32_t primality;      // CCS_PRIME_MR / CCS_PRIME_BPSW
+    uint32_t prove_mode;     // CCS_PROVE_ROOTS / CCS_PROVE_FULL
+    uint32_t n_wit;
+    uint32_t wit[32];
+};
+
+cudaError_t upload_profile_const(int slot, const ProfileConst& pc, cudaStream_t st);
+cudaError_t upload_prove_const(int slot, const ProveConst& pc, cudaStream_t st);
+cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, uint32_t max_ranges,
+                               const uint32_t* primes, uint32_t max_primes, uint32_t* jmod,
+                               uint32_t stride, cudaStream_t st);
+size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride);
+cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
+                         const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride, CQueue cq,
+                         uint32_t b_stride, uint32_t grid, cudaStream_t st);
+cudaError_t launch_levelc(const RangeDev* ranges, const uint32_t* jmod, uint32_t stride, CQueue cq,
+                          uint32_t grid, cudaStream_t st);
+cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
+cudaError_t launch_walk(const uint32_t* numbers, uint64_t n, uint32_t limbs, uint32_t* lengths,
+                        int profile, cudaStream_t st);
+int sweep_blocks_per_sm(uint32_t b_stride);
+
+}  // namespace ccs

@@ -1,0 +1,808 @@
+// C-ABI implementation: engine lifetime, plain per-range path, host-buffer
+// path, number walks and the batched (graph-replayed) executor.
+//
+// Reference behaviour replaced: gpu_upload_tables (v13:1065-1222), the
+// per-batch launch/copy sequence of the main loop (v13:3719-3906) and the
+// error policy (CUDA_CHECK -> exit, v13:142-149): every failure here is a
+// returned status plus a message in ccs_last_error().
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ccs.h"
+#include "ccs_internal.h"
+#include "ccs_kernels.cuh"
+
+using namespace ccs;
+
+namespace {
+
+thread_local std::string g_err;
+
+ccs_status fail(ccs_status st, const std::string& msg) {
+    g_err = msg;
+    return st;
+}
+
+#define CU(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? CCS_ERR_NOMEM : CCS_ERR_CUDA,   \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+// constant-memory profile slots, per device
+std::mutex g_slot_mu;
+uint32_t g_slots_used[64] = {0};
+
+int alloc_slot(int dev) {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    for (int s = 0; s < kMaxProfiles; s++)
+        if (!(g_slots_used[dev] & (1u << s))) { g_slots_used[dev] |= 1u << s; return s; }
+    return -1;
+}
+
+void free_slot(int dev, int s) {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    if (s >= 0) g_slots_used[dev] &= ~(1u << s);
+}
+
+const uint32_t kRefCrt[] = {5, 7, 11, 13, 17, 19};
+const uint32_t kRefWheel[] = {23, 29, 31};
+const uint32_t kRefL2[] = {37, 41, 43, 47, 53, 59, 61};
+const uint32_t kRefExt[] = {67, 71, 73, 79, 83, 89, 97};
+const uint64_t kRefWit[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71};
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        free_();
+        n = count;
+        return cudaMalloc((void**)&p, sizeof(T) * (count ? count : 1));
+    }
+    void free_() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+}  // namespace
+
+struct ccs_engine {
+    int device = 0;
+    int slot = -1;
+    HostProfile hp;
+    ccs_tuning tune{};
+    int sms = 148;
+    cudaStream_t own_stream = nullptr;
+
+    // profile tables
+    DevBuf<Line> lines;
+    DevBuf<PrimeC> primesB, primesC;
+    DevBuf<uint32_t> bitmapB, listC, range_primes;
+    DevBuf<uint64_t> bases;
+
+    // plain-path working state
+    DevBuf<RangeDev> d_range;
+    DevBuf<ProveRange> d_prange;
+    DevBuf<uint64_t> d_prefix;
+    DevBuf<SweepHeader> d_hdr;
+    DevBuf<uint32_t> d_jmod;
+    DevBuf<uint32_t> d_counters;     // [0] surv, [1] cq, [2] chains, [3] primes
+    DevBuf<uint4> d_cq;
+    uint32_t cq_cap = 0;
+    // host-path scratch
+    DevBuf<uint32_t> d_surv_scratch, d_chain_scratch;
+    // pinned staging
+    void* h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    double levelc_rate = 0;          // fraction of candidates entering level C
+    uint64_t launches = 0;           // kernels launched by this engine
+};
+
+struct ccs_batch {
+    std::vector<ccs_engine*> prof;
+    int device = 0;
+    uint32_t max_ranges = 0;
+    uint64_t surv_cap = 0, chain_cap = 0;
+    uint32_t jstride = 0;
+    DevBuf<RangeDev> d_ranges;
+    DevBuf<ProveRange> d_pranges;
+    DevBuf<uint64_t> d_prefix;
+    DevBuf<SweepHeader> d_hdr;
+    DevBuf<uint32_t> d_jmod, d_primes;   // concatenated range-prime lists of all profiles
+    DevBuf<uint32_t> d_surv, d_chains;
+    DevBuf<uint32_t> d_counts;           // [0] surv [1] cq [2] chains [3] spare, then 3 per range
+    DevBuf<uint4> d_cq;
+    uint32_t cq_cap = 0;
+    std::vector<uint32_t> prime_base;    // per profile offset into d_primes
+    uint32_t max_range_primes = 0;
+    uint32_t b_stride = 0;
+    // pinned staging: ranges, prefix, header, counts
+    RangeDev* h_ranges = nullptr;
+    ProveRange* h_pranges = nullptr;
+    uint64_t* h_prefix = nullptr;
+    SweepHeader* h_hdr = nullptr;
+    uint32_t* h_counts = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0;
+    uint32_t grid = 0;
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+namespace {
+
+struct U128 {
+    uint64_t lo, hi;
+};
+
+inline unsigned __int128 mk128(uint64_t lo, uint64_t hi) {
+    return ((unsigned __int128)hi << 64) | lo;
+}
+
+void fill_J0(uint32_t (&J0)[4], unsigned __int128 v) {
+    for (int i = 0; i < 4; i++) J0[i] = (uint32_t)(v >> (32 * i));
+}
+
+uint32_t words_for(uint32_t e0, uint64_t n_tiles) {
+    uint64_t span = (e0 + n_tiles + 5) / 6;
+    return (uint32_t)((span + 63) / 64);
+}
+
+ccs_status upload_profile(ccs_engine* E, cudaStream_t st) {
+    HostProfile& hp = E->hp;
+    CU(E->lines.alloc(hp.lines.size()));
+    CU(cudaMemcpy(E->lines.p, hp.lines.data(), sizeof(Line) * hp.lines.size(), cudaMemcpyHostToDevice));
+    CU(E->primesB.alloc(hp.primesB.size()));
+    if (!hp.primesB.empty())
+        CU(cudaMemcpy(E->primesB.p, hp.primesB.data(), sizeof(PrimeC) * hp.primesB.size(), cudaMemcpyHostToDevice));
+    CU(E->primesC.alloc(hp.primesC.size()));
+    if (!hp.primesC.empty())
+        CU(cudaMemcpy(E->primesC.p, hp.primesC.data(), sizeof(PrimeC) * hp.primesC.size(), cudaMemcpyHostToDevice));
+    CU(E->bitmapB.alloc(hp.bitmapB.size()));
+    if (!hp.bitmapB.empty())
+        CU(cudaMemcpy(E->bitmapB.p, hp.bitmapB.data(), 4 * hp.bitmapB.size(), cudaMemcpyHostToDevice));
+    CU(E->listC.alloc(hp.listC.size()));
+    if (!hp.listC.empty())
+        CU(cudaMemcpy(E->listC.p, hp.listC.data(), 4 * hp.listC.size(), cudaMemcpyHostToDevice));
+    CU(E->range_primes.alloc(hp.range_primes.size()));
+    CU(cudaMemcpy(E->range_primes.p, hp.range_primes.data(), 4 * hp.range_primes.size(), cudaMemcpyHostToDevice));
+    CU(E->bases.alloc(hp.bases.size()));
+    CU(cudaMemcpy(E->bases.p, hp.bases.data(), 8 * hp.bases.size(), cudaMemcpyHostToDevice));
+
+    ProfileConst pc;
+    memset(&pc, 0, sizeof(pc));
+    pc.W = hp.W;
+    pc.n_lines = (uint32_t)hp.lines.size();
+    pc.nB = (uint32_t)hp.primesB.size();
+    pc.nC = (uint32_t)hp.primesC.size();
+    memcpy(pc.A, hp.A, sizeof(pc.A));
+    pc.lines = E->lines.p;
+    pc.primesB = E->primesB.p;
+    pc.bitmapB = E->bitmapB.p;
+    pc.primesC = E->primesC.p;
+    pc.listC = E->listC.p;
+    CU(upload_profile_const(E->slot, pc, st));
+
+    ProveConst pv;
+    memset(&pv, 0, sizeof(pv));
+    pv.bases = E->bases.p;
+    pv.n_bases = (uint32_t)hp.bases.size();
+    pv.WP = hp.WP;
+    pv.M = (uint32_t)hp.M;
+    pv.primality = hp.primality;
+    pv.prove_mode = hp.prove_mode;
+    pv.n_wit = (uint32_t)std::min<size_t>(hp.witnesses.size(), 32);
+    for (uint32_t i = 0; i < pv.n_wit; i++) pv.wit[i] = (uint32_t)hp.witnesses[i];
+    CU(upload_prove_const(E->slot, pv, st));
+    CU(cudaStreamSynchronize(st));
+    return CCS_OK;
+}
+
+uint32_t b_stride_of(uint32_t nB) {
+    uint32_t s = nB ? nB : 1;
+    return (s + 7) & ~7u;
+}
+
+// work units for one range
+uint64_t units_of(const ccs_engine* E, uint32_t n_words, uint32_t unit_words) {
+    uint64_t groups = (E->hp.lines.size() + 31) / 32;
+    uint64_t chunks = (n_words + unit_words - 1) / unit_words;
+    return groups * chunks;
+}
+
+uint32_t choose_unit_words(const ccs_engine* E, uint32_t n_words) {
+    uint32_t uw = E->tune.unit_words ? E->tune.unit_words : 256;
+    if (uw > n_words) uw = n_words ? n_words : 1;
+    return uw;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* ccs_last_error(void) { return g_err.c_str(); }
+int ccs_abi_version(void) { return CCS_ABI_VERSION; }
+
+static ccs_status params_to_profile(const ccs_params* params, HostProfile& hp) {
+    ccs_params def;
+    memset(&def, 0, sizeof(def));
+    const ccs_params& p = params ? *params : def;
+    if (p.kind != 0 && p.kind != CCS_KIND_FIRST)
+        return fail(CCS_ERR_INVALID, "only first-kind chains are supported");
+    hp.target = p.target ? p.target : 18;
+    hp.depth = p.depth ? p.depth : hp.target;
+    hp.bits = p.bits ? p.bits : 89;
+    if (p.crt_primes && p.n_crt) hp.crt.assign(p.crt_primes, p.crt_primes + p.n_crt);
+    else hp.crt.assign(kRefCrt, kRefCrt + 6);
+    if (p.wheel_primes && p.n_wheel) hp.wheel.assign(p.wheel_primes, p.wheel_primes + p.n_wheel);
+    else hp.wheel.assign(kRefWheel, kRefWheel + 3);
+    hp.stages.clear();
+    if (p.stages && p.n_stages) {
+        if (p.n_stages > (uint32_t)kMaxStages) return fail(CCS_ERR_INVALID, "too many stages");
+        for (uint32_t s = 0; s < p.n_stages; s++) {
+            HostProfile::Stage st;
+            if (p.stages[s].n_primes && !p.stages[s].primes) return fail(CCS_ERR_INVALID, "stage primes null");
+            st.primes.assign(p.stages[s].primes, p.stages[s].primes + p.stages[s].n_primes);
+            st.pos_lo = p.stages[s].pos_lo;
+            hp.stages.push_back(st);
+        }
+    } else {
+        HostProfile::Stage a, b, c;
+        a.primes.assign(kRefL2, kRefL2 + 7); a.pos_lo = 0;
+        b.primes.assign(kRefExt, kRefExt + 7); b.pos_lo = 0;
+        for (uint32_t q = 101; q <= 863; q++)
+            if (is_prime_u32(q)) c.primes.push_back(q);
+        c.pos_lo = 1;
+        hp.stages = {a, b, c};
+    }
+    hp.max_bases = p.max_bases;
+    if (p.witnesses && p.n_witnesses) {
+        if (p.n_witnesses > 32) return fail(CCS_ERR_INVALID, "at most 32 witnesses");
+        for (uint32_t i = 0; i < p.n_witnesses; i++)
+            if (p.witnesses[i] < 2 || p.witnesses[i] > 0xFFFFFFFFull)
+                return fail(CCS_ERR_INVALID, "witnesses must be in [2, 2^32)");
+        hp.witnesses.assign(p.witnesses, p.witnesses + p.n_witnesses);
+    } else {
+        hp.witnesses.assign(kRefWit, kRefWit + 20);
+    }
+    hp.primality = p.primality;
+    hp.prove_mode = p.prove_mode;
+    if (hp.primality > 1 || hp.prove_mode > 1) return fail(CCS_ERR_INVALID, "bad primality / prove_mode");
+    std::string err = build_profile(hp, 1024);
+    if (!err.empty()) return fail(CCS_ERR_INVALID, err);
+    if (hp.primesB.size() > (size_t)kMaxLevelB) return fail(CCS_ERR_INVALID, "too many level-B primes");
+    return CCS_OK;
+}
+
+static void fill_info(const HostProfile& hp, ccs_info* o) {
+    o->lattice_m = hp.M;
+    o->wheel_period = hp.WP;
+    o->n_bases = (uint32_t)hp.bases.size();
+    o->n_lines = hp.lines.size();
+    uint64_t tot = 0;
+    for (uint32_t w : hp.wheel_total) tot += w;
+    o->candidates_per_tile = tot / 6;
+    o->target = hp.target;
+    o->depth = hp.depth;
+    o->bits = hp.bits;
+    o->n_filter_primes = (uint32_t)hp.fprimes.size();
+    o->expected_tests = hp.expected_tests;
+    o->pass_rate = hp.pass_rate;
+    o->launches = 0;
+}
+
+ccs_status ccs_describe(const ccs_params* params, ccs_info* out, uint64_t* bases, uint32_t cap) {
+    if (!out) return fail(CCS_ERR_INVALID, "out is null");
+    HostProfile hp;
+    ccs_status s = params_to_profile(params, hp);
+    if (s != CCS_OK) return s;
+    fill_info(hp, out);
+    if (bases) {
+        uint32_t n = (uint32_t)std::min<size_t>(cap, hp.bases.size());
+        memcpy(bases, hp.bases.data(), 8 * n);
+        if (cap < hp.bases.size()) return fail(CCS_OVERFLOW, "bases capacity exceeded");
+    }
+    return CCS_OK;
+}
+
+ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out) {
+    if (!out) return fail(CCS_ERR_INVALID, "out is null");
+    *out = nullptr;
+    int ndev = 0;
+    CU(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev || device >= 64) return fail(CCS_ERR_INVALID, "bad device ordinal");
+    CU(cudaSetDevice(device));
+    ccs_engine* E = new ccs_engine();
+    E->device = device;
+    HostProfile& hp = E->hp;
+    {
+        ccs_status s = params_to_profile(params, hp);
+        if (s != CCS_OK) { delete E; return s; }
+    }
+    E->tune.block_threads = kSweepThreads;
+    E->tune.unit_words = 256;
+    E->tune.split_prime = 1024;
+    // fraction of candidates that reach level C
+    double f = 1.0;
+    for (auto& fp : hp.fprimes)
+        if (fp.q < E->tune.split_prime) f *= 1.0 - (double)fp.forb.size() / fp.q;
+    E->levelc_rate = hp.primesC.empty() ? 0.0 : f;
+
+    E->slot = alloc_slot(device);
+    if (E->slot < 0) { delete E; return fail(CCS_ERR_BUSY, "all constant-memory profile slots in use (max 8 engines per device)"); }
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    E->sms = prop.multiProcessorCount;
+    CU(cudaStreamCreateWithFlags(&E->own_stream, cudaStreamNonBlocking));
+    ccs_status st = upload_profile(E, E->own_stream);
+    if (st != CCS_OK) { ccs_destroy(E); return st; }
+    int bps = sweep_blocks_per_sm(b_stride_of((uint32_t)hp.primesB.size()));
+    E->tune.blocks_per_sm = bps > 0 ? (uint32_t)bps : 1;
+
+    // plain-path state
+    E->cq_cap = hp.primesC.empty() ? 1 : (1u << 24);
+    if (E->d_range.alloc(1) || E->d_prange.alloc(1) || E->d_prefix.alloc(2) || E->d_hdr.alloc(1) ||
+        E->d_jmod.alloc(hp.range_primes.size()) || E->d_counters.alloc(8) || E->d_cq.alloc(E->cq_cap)) {
+        ccs_destroy(E);
+        return fail(CCS_ERR_NOMEM, "device allocation failed");
+    }
+    E->h_stage_bytes = 1 << 16;
+    if (cudaMallocHost(&E->h_stage, E->h_stage_bytes) != cudaSuccess) {
+        ccs_destroy(E);
+        return fail(CCS_ERR_NOMEM, "pinned allocation failed");
+    }
+    *out = E;
+    return CCS_OK;
+}
+
+ccs_status ccs_destroy(ccs_engine* E) {
+    if (!E) return CCS_OK;
+    cudaSetDevice(E->device);
+    if (E->own_stream) cudaStreamSynchronize(E->own_stream);
+    E->lines.free_(); E->primesB.free_(); E->primesC.free_(); E->bitmapB.free_();
+    E->listC.free_(); E->range_primes.free_(); E->bases.free_();
+    E->d_range.free_(); E->d_prange.free_(); E->d_prefix.free_(); E->d_hdr.free_();
+    E->d_jmod.free_(); E->d_counters.free_(); E->d_cq.free_();
+    E->d_surv_scratch.free_(); E->d_chain_scratch.free_();
+    if (E->h_stage) cudaFreeHost(E->h_stage);
+    if (E->own_stream) cudaStreamDestroy(E->own_stream);
+    free_slot(E->device, E->slot);
+    delete E;
+    return CCS_OK;
+}
+
+ccs_status ccs_get_info(const ccs_engine* E, ccs_info* o) {
+    if (!E || !o) return fail(CCS_ERR_INVALID, "null argument");
+    fill_info(E->hp, o);
+    o->launches = E->launches;
+    return CCS_OK;
+}
+
+ccs_status ccs_get_bases(const ccs_engine* E, uint64_t* bases, uint32_t cap) {
+    if (!E || !bases) return fail(CCS_ERR_INVALID, "null argument");
+    uint32_t n = (uint32_t)std::min<size_t>(cap, E->hp.bases.size());
+    memcpy(bases, E->hp.bases.data(), 8 * n);
+    return cap < E->hp.bases.size() ? CCS_OVERFLOW : CCS_OK;
+}
+
+ccs_status ccs_get_tuning(const ccs_engine* E, ccs_tuning* t) {
+    if (!E || !t) return fail(CCS_ERR_INVALID, "null argument");
+    *t = E->tune;
+    return CCS_OK;
+}
+
+ccs_status ccs_set_tuning(ccs_engine* E, const ccs_tuning* t) {
+    if (!E || !t) return fail(CCS_ERR_INVALID, "null argument");
+    if (t->block_threads && t->block_threads != (uint32_t)kSweepThreads)
+        return fail(CCS_ERR_INVALID, "block_threads is fixed at 256 in this build");
+    if (t->unit_words > (1u << 20)) return fail(CCS_ERR_INVALID, "unit_words too large");
+    if (t->split_prime && t->split_prime != E->tune.split_prime)
+        return fail(CCS_ERR_INVALID, "split_prime is fixed at engine creation");
+    if (t->unit_words) E->tune.unit_words = t->unit_words;
+    if (t->blocks_per_sm) E->tune.blocks_per_sm = t->blocks_per_sm;
+    return CCS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plain path
+// ---------------------------------------------------------------------------
+static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_tiles, uint32_t bias,
+                               ccs_survivor* out, uint64_t cap, cudaStream_t st) {
+    HostProfile& hp = E->hp;
+    RangeDev* hr = (RangeDev*)E->h_stage;
+    uint64_t* hpre = (uint64_t*)((char*)E->h_stage + 1024);
+    SweepHeader* hh = (SweepHeader*)((char*)E->h_stage + 2048);
+    memset(hr, 0, sizeof(RangeDev));
+    unsigned __int128 J0 = ts / 6;
+    fill_J0(hr->J0, J0);
+    hr->e0 = (uint32_t)(ts % 6);
+    hr->n_tiles = (uint32_t)n_tiles;
+    hr->n_words = words_for(hr->e0, n_tiles);
+    hr->unit_words = choose_unit_words(E, hr->n_words);
+    hr->profile = (uint32_t)E->slot;
+    hr->prime_base = 0;
+    hr->n_range_primes = (uint32_t)hp.range_primes.size();
+    hr->surv_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
+    hr->surv_count = E->d_counters.p;
+    hr->surv = (uint32_t*)out;
+    hr->range_count = nullptr;
+    hr->range_id = 0;
+    hr->tile_bias = bias;
+    uint64_t units = units_of(E, hr->n_words, hr->unit_words);
+    hpre[0] = 0;
+    hpre[1] = units;
+    hh->n_ranges = 1;
+    hh->total_units = units;
+    CU(cudaMemcpyAsync(E->d_range.p, hr, sizeof(RangeDev), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->d_prefix.p, hpre, 16, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(E->d_hdr.p, hh, sizeof(SweepHeader), cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(E->d_counters.p + 1, 0, 4, st));
+    E->launches += hp.primesC.empty() ? 2 : 3;
+    CU(launch_range_setup(E->d_range.p, E->d_hdr.p, 1, E->range_primes.p,
+                          (uint32_t)hp.range_primes.size(), E->d_jmod.p,
+                          (uint32_t)hp.range_primes.size(), st));
+    CQueue cq{E->d_counters.p + 1, E->cq_cap, E->d_cq.p};
+    uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
+    uint64_t need = (units + (kSweepThreads / 32) - 1) / (kSweepThreads / 32);
+    if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
+    CU(launch_sweep(E->d_range.p, E->d_prefix.p, E->d_hdr.p, E->d_jmod.p,
+                    (uint32_t)hp.range_primes.size(), cq, b_stride_of((uint32_t)hp.primesB.size()),
+                    grid, st));
+    if (!hp.primesC.empty()) {
+        CU(launch_levelc(E->d_range.p, E->d_jmod.p, (uint32_t)hp.range_primes.size(), cq,
+                         (uint32_t)E->sms * 8, st));
+        uint32_t cqn = 0;
+        CU(cudaMemcpyAsync(hh, E->d_counters.p + 1, 4, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        cqn = *(uint32_t*)hh;
+        if (cqn > E->cq_cap)
+            return fail(CCS_OVERFLOW, "deferred-stage queue overflow (" + std::to_string(cqn) +
+                                          " > " + std::to_string(E->cq_cap) + "); use smaller ranges");
+    }
+    return CCS_OK;
+}
+
+ccs_status ccs_filter_range(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint64_t n_tiles,
+                            ccs_survivor* out_dev, uint64_t cap, uint64_t* n_out, void* stream) {
+    if (!E || !n_out) return fail(CCS_ERR_INVALID, "null argument");
+    if (cap && !out_dev) return fail(CCS_ERR_INVALID, "out_dev is null");
+    if (n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
+    unsigned __int128 ts = mk128(ts_lo, ts_hi);
+    if (ts + n_tiles < ts) return fail(CCS_ERR_INVALID, "tile range wraps 2^128");
+    CU(cudaSetDevice(E->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : E->own_stream;
+    CU(cudaMemsetAsync(E->d_counters.p, 0, 4, st));
+    *n_out = 0;
+    if (n_tiles) {
+        // chunk so the deferred level-C queue cannot overflow (4x margin)
+        uint64_t cpt = 0;
+        for (uint32_t w : E->hp.wheel_total) cpt += w;
+        cpt = cpt / 6 + 1;
+        uint64_t max_tiles = n_tiles;
+        if (E->levelc_rate > 0) {
+            double tiles = (double)E->cq_cap / (4.0 * E->levelc_rate * (double)cpt);
+            if (tiles < 6) tiles = 6;
+            if (tiles < (double)max_tiles) max_tiles = (uint64_t)tiles / 6 * 6;
+        }
+        for (uint64_t off = 0; off < n_tiles; off += max_tiles) {
+            uint64_t nt = std::min<uint64_t>(max_tiles, n_tiles - off);
+            ccs_status s = filter_chunk(E, ts + off, nt, (uint32_t)off, out_dev, cap, st);
+            if (s != CCS_OK) return s;
+        }
+    }
+    uint32_t cnt = 0;
+    CU(cudaMemcpyAsync(E->h_stage, E->d_counters.p, 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    cnt = *(uint32_t*)E->h_stage;
+    *n_out = cnt;
+    if (cnt > cap) return fail(CCS_OVERFLOW, "survivor capacity exceeded");
+    return CCS_OK;
+}
+
+ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv, uint64_t ts_lo,
+                     uint64_t ts_hi, ccs_chain* out_dev, uint64_t cap, uint64_t* n_out,
+                     uint64_t* primes_out, void* stream) {
+    if (!E || !n_out) return fail(CCS_ERR_INVALID, "null argument");
+    if (n_surv && !surv_dev) return fail(CCS_ERR_INVALID, "surv_dev is null");
+    if (cap && !out_dev) return fail(CCS_ERR_INVALID, "out_dev is null");
+    if (n_surv >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_surv must be < 2^32");
+    CU(cudaSetDevice(E->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : E->own_stream;
+    ProveRange* pr = (ProveRange*)((char*)E->h_stage + 4096);
+    memset(pr, 0, sizeof(ProveRange));
+    fill_J0(pr->T0, mk128(ts_lo, ts_hi));
+    pr->bits = E->hp.bits;
+    pr->profile = (uint32_t)E->slot;
+    pr->target = E->hp.target;
+    pr->chain_count = nullptr;
+    pr->prime_count = E->d_counters.p + 3;
+    CU(cudaMemcpyAsync(E->d_prange.p, pr, sizeof(ProveRange), cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(E->d_counters.p + 2, 0, 8, st));
+    ProveArgs a;
+    a.ranges = E->d_prange.p;
+    a.surv = (const uint32_t*)surv_dev;
+    a.n_surv_dev = nullptr;
+    a.n_surv = (uint32_t)n_surv;
+    a.surv_cap = (uint32_t)n_surv;
+    a.range_from_pad = 0;
+    a.chains = (uint32_t*)out_dev;
+    a.chain_count = E->d_counters.p + 2;
+    a.chain_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
+    uint32_t grid = (uint32_t)std::min<uint64_t>((n_surv + 127) / 128, (uint64_t)E->sms * 16);
+    CU(launch_prove(a, grid, st));
+    E->launches += 1;
+    uint32_t* hc = (uint32_t*)((char*)E->h_stage + 8192);
+    CU(cudaMemcpyAsync(hc, E->d_counters.p + 2, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    *n_out = hc[0];
+    if (primes_out) *primes_out = hc[1];
+    if (hc[0] > cap) return fail(CCS_OVERFLOW, "chain capacity exceeded");
+    return CCS_OK;
+}
+
+ccs_status ccs_search_range_host(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint64_t n_tiles,
+                                 ccs_survivor* surv_host, uint64_t surv_cap, uint64_t* n_surv,
+                                 ccs_chain* chains_host, uint64_t chain_cap, uint64_t* n_chains,
+                                 uint64_t* primes_out) {
+    if (!E || !n_surv || !n_chains) return fail(CCS_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(E->device));
+    uint64_t scap = std::max<uint64_t>(surv_cap, 1 << 16);
+    uint64_t ccap = std::max<uint64_t>(chain_cap, 1 << 16);
+    if (E->d_surv_scratch.n < 4 * scap) CU(E->d_surv_scratch.alloc(4 * scap));
+    if (E->d_chain_scratch.n < 12 * ccap) CU(E->d_chain_scratch.alloc(12 * ccap));
+    ccs_survivor* ds = (ccs_survivor*)E->d_surv_scratch.p;
+    ccs_chain* dc = (ccs_chain*)E->d_chain_scratch.p;
+    uint64_t ns = 0;
+    ccs_status s = ccs_filter_range(E, ts_lo, ts_hi, n_tiles, ds, scap, &ns, nullptr);
+    *n_surv = ns;
+    if (s != CCS_OK && s != CCS_OVERFLOW) return s;
+    uint64_t use = std::min(ns, scap);
+    uint64_t nc = 0;
+    ccs_status s2 = ccs_prove(E, ds, use, ts_lo, ts_hi, dc, ccap, &nc, primes_out, nullptr);
+    *n_chains = nc;
+    if (s2 != CCS_OK && s2 != CCS_OVERFLOW) return s2;
+    cudaStream_t st = E->own_stream;
+    if (surv_host && surv_cap)
+        CU(cudaMemcpyAsync(surv_host, ds, sizeof(ccs_survivor) * std::min(use, surv_cap),
+                           cudaMemcpyDeviceToHost, st));
+    if (chains_host && chain_cap)
+        CU(cudaMemcpyAsync(chains_host, dc, sizeof(ccs_chain) * std::min(nc, chain_cap),
+                           cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (ns > surv_cap || nc > chain_cap) return fail(CCS_OVERFLOW, "host capacity exceeded");
+    return s != CCS_OK ? s : s2;
+}
+
+ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t n, uint32_t limbs,
+                            uint32_t* lengths_dev, void* stream) {
+    if (!E) return fail(CCS_ERR_INVALID, "null engine");
+    if (limbs < 1 || limbs > (uint32_t)kMaxLimbs) return fail(CCS_ERR_INVALID, "limbs must be 1..6");
+    if (n && (!numbers_dev || !lengths_dev)) return fail(CCS_ERR_INVALID, "null buffer");
+    CU(cudaSetDevice(E->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : E->own_stream;
+    if (n) { CU(launch_walk(numbers_dev, n, limbs, lengths_dev, E->slot, st)); E->launches += 1; }
+    CU(cudaStreamSynchronize(st));
+    return CCS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched executor
+// ---------------------------------------------------------------------------
+ccs_status ccs_batch_destroy(ccs_batch* b) {
+    if (!b) return CCS_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->d_ranges.free_(); b->d_pranges.free_(); b->d_prefix.free_(); b->d_hdr.free_();
+    b->d_jmod.free_(); b->d_primes.free_(); b->d_surv.free_(); b->d_chains.free_();
+    b->d_counts.free_(); b->d_cq.free_();
+    if (b->h_ranges) cudaFreeHost(b->h_ranges);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return CCS_OK;
+}
+
+ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, uint32_t max_ranges,
+                            uint64_t surv_cap, uint64_t chain_cap, ccs_batch** out) {
+    if (!out || !profiles || !n_profiles || !max_ranges) return fail(CCS_ERR_INVALID, "bad argument");
+    if (surv_cap >= (1ull << 32) || chain_cap >= (1ull << 32)) return fail(CCS_ERR_INVALID, "caps must be < 2^32");
+    *out = nullptr;
+    ccs_batch* b = new ccs_batch();
+    b->device = profiles[0]->device;
+    for (uint32_t i = 0; i < n_profiles; i++) {
+        if (!profiles[i] || profiles[i]->device != b->device) { delete b; return fail(CCS_ERR_INVALID, "profiles must share one device"); }
+        b->prof.push_back(profiles[i]);
+    }
+    CU(cudaSetDevice(b->device));
+    b->max_ranges = max_ranges;
+    b->surv_cap = std::max<uint64_t>(surv_cap, 1);
+    b->chain_cap = std::max<uint64_t>(chain_cap, 1);
+    std::vector<uint32_t> allp;
+    uint32_t maxnb = 0;
+    bool any_c = false;
+    for (auto* E : b->prof) {
+        b->prime_base.push_back((uint32_t)allp.size());
+        allp.insert(allp.end(), E->hp.range_primes.begin(), E->hp.range_primes.end());
+        b->max_range_primes = std::max<uint32_t>(b->max_range_primes, (uint32_t)E->hp.range_primes.size());
+        maxnb = std::max<uint32_t>(maxnb, (uint32_t)E->hp.primesB.size());
+        any_c |= !E->hp.primesC.empty();
+    }
+    b->b_stride = b_stride_of(maxnb);
+    b->jstride = b->max_range_primes;
+    b->cq_cap = any_c ? (1u << 24) : 1;
+    size_t nc = 4 + 3 * (size_t)max_ranges;
+    if (b->d_ranges.alloc(max_ranges) || b->d_pranges.alloc(max_ranges) ||
+        b->d_prefix.alloc(max_ranges + 1) || b->d_hdr.alloc(1) ||
+        b->d_jmod.alloc((size_t)max_ranges * b->jstride) || b->d_primes.alloc(allp.size()) ||
+        b->d_surv.alloc(4 * b->surv_cap) || b->d_chains.alloc(12 * b->chain_cap) ||
+        b->d_counts.alloc(nc) || b->d_cq.alloc(b->cq_cap)) {
+        ccs_batch_destroy(b);
+        return fail(CCS_ERR_NOMEM, "batch device allocation failed");
+    }
+    CU(cudaMemcpy(b->d_primes.p, allp.data(), 4 * allp.size(), cudaMemcpyHostToDevice));
+    size_t hb = sizeof(RangeDev) * max_ranges + sizeof(ProveRange) * max_ranges +
+                8 * (max_ranges + 1) + sizeof(SweepHeader) + 4 * nc + 256;
+    void* h = nullptr;
+    if (cudaMallocHost(&h, hb) != cudaSuccess) { ccs_batch_destroy(b); return fail(CCS_ERR_NOMEM, "pinned alloc failed"); }
+    char* c = (char*)h;
+    b->h_ranges = (RangeDev*)c; c += sizeof(RangeDev) * max_ranges;
+    b->h_pranges = (ProveRange*)c; c += sizeof(ProveRange) * max_ranges;
+    b->h_prefix = (uint64_t*)c; c += 8 * (max_ranges + 1);
+    b->h_hdr = (SweepHeader*)c; c += sizeof(SweepHeader);
+    c = (char*)(((uintptr_t)c + 15) & ~(uintptr_t)15);
+    b->h_counts = (uint32_t*)c;
+    CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&b->ev0));
+    CU(cudaEventCreate(&b->ev1));
+    int bps = sweep_blocks_per_sm(b->b_stride);
+    b->grid = (uint32_t)b->prof[0]->sms * (uint32_t)std::max(bps, 1);
+
+    // record the whole batch once: H2D descriptors, setup, sweep, level C,
+    // prove, D2H counters.  Replays read the per-submission header on device.
+    cudaStream_t st = b->stream;
+    CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(b->d_ranges.p, b->h_ranges, sizeof(RangeDev) * max_ranges, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(b->d_pranges.p, b->h_pranges, sizeof(ProveRange) * max_ranges, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(b->d_prefix.p, b->h_prefix, 8 * (max_ranges + 1), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(b->d_hdr.p, b->h_hdr, sizeof(SweepHeader), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(b->d_counts.p, 0, 4 * nc, st);
+    launch_range_setup(b->d_ranges.p, b->d_hdr.p, max_ranges, b->d_primes.p, b->max_range_primes,
+                       b->d_jmod.p, b->jstride, st);
+    CQueue cq{b->d_counts.p + 1, b->cq_cap, b->d_cq.p};
+    launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, cq, b->b_stride,
+                 b->grid, st);
+    if (any_c) launch_levelc(b->d_ranges.p, b->d_jmod.p, b->jstride, cq, (uint32_t)b->prof[0]->sms * 8, st);
+    ProveArgs pa;
+    pa.ranges = b->d_pranges.p;
+    pa.surv = b->d_surv.p;
+    pa.n_surv_dev = b->d_counts.p;
+    pa.n_surv = 0;
+    pa.surv_cap = (uint32_t)b->surv_cap;
+    pa.range_from_pad = 1;
+    pa.chains = b->d_chains.p;
+    pa.chain_count = b->d_counts.p + 2;
+    pa.chain_cap = (uint32_t)b->chain_cap;
+    launch_prove(pa, (uint32_t)b->prof[0]->sms * 16, st);
+    cudaMemcpyAsync(b->h_counts, b->d_counts.p, 4 * nc, cudaMemcpyDeviceToHost, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &b->graph);
+    if (ce != cudaSuccess) { ccs_batch_destroy(b); return fail(CCS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)); }
+    ce = cudaGraphInstantiate(&b->gexec, b->graph, 0);
+    if (ce != cudaSuccess) { ccs_batch_destroy(b); return fail(CCS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce)); }
+    *out = b;
+    return CCS_OK;
+}
+
+ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
+                         ccs_range_result* results, ccs_survivor* surv_host, ccs_chain* chains_host,
+                         void* stream) {
+    if (!b || (n_ranges && !ranges)) return fail(CCS_ERR_INVALID, "null argument");
+    if (n_ranges > b->max_ranges) return fail(CCS_ERR_INVALID, "too many ranges for this batch");
+    CU(cudaSetDevice(b->device));
+    (void)stream;
+    uint64_t total = 0;
+    uint32_t* cnt = b->d_counts.p;
+    for (uint32_t i = 0; i < n_ranges; i++) {
+        const ccs_range& rg = ranges[i];
+        if (rg.profile >= b->prof.size()) return fail(CCS_ERR_INVALID, "bad profile index");
+        if (rg.n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
+        ccs_engine* E = b->prof[rg.profile];
+        unsigned __int128 ts = mk128(rg.tile_start_lo, rg.tile_start_hi);
+        RangeDev& R = b->h_ranges[i];
+        memset(&R, 0, sizeof(R));
+        fill_J0(R.J0, ts / 6);
+        R.e0 = (uint32_t)(ts % 6);
+        R.n_tiles = (uint32_t)rg.n_tiles;
+        R.n_words = rg.n_tiles ? words_for(R.e0, rg.n_tiles) : 0;
+        R.unit_words = choose_unit_words(E, R.n_words);
+        R.profile = (uint32_t)E->slot;
+        R.prime_base = b->prime_base[rg.profile];
+        R.n_range_primes = (uint32_t)E->hp.range_primes.size();
+        R.surv_cap = (uint32_t)b->surv_cap;
+        R.surv_count = cnt;
+        R.surv = b->d_surv.p;
+        R.range_count = cnt + 4 + 3 * i;
+        R.range_id = i;
+        R.tile_bias = 0;
+        ProveRange& P = b->h_pranges[i];
+        memset(&P, 0, sizeof(P));
+        fill_J0(P.T0, ts);
+        P.bits = rg.bits ? rg.bits : E->hp.bits;
+        P.profile = (uint32_t)E->slot;
+        P.target = E->hp.target;
+        P.chain_count = cnt + 4 + 3 * i + 1;
+        P.prime_count = cnt + 4 + 3 * i + 2;
+        b->h_prefix[i] = total;
+        total += R.n_words ? units_of(E, R.n_words, R.unit_words) : 0;
+    }
+    b->h_prefix[n_ranges] = total;
+    for (uint32_t i = n_ranges + 1; i <= b->max_ranges; i++) b->h_prefix[i] = total;
+    b->h_hdr->n_ranges = n_ranges;
+    b->h_hdr->total_units = total;
+    CU(cudaEventRecord(b->ev0, b->stream));
+    CU(cudaGraphLaunch(b->gexec, b->stream));
+    CU(cudaEventRecord(b->ev1, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    CU(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    const uint32_t* hc = b->h_counts;
+    ccs_status st = CCS_OK;
+    if (hc[1] > b->cq_cap) st = fail(CCS_OVERFLOW, "deferred-stage queue overflow in batch");
+    uint64_t ns = hc[0], nch = hc[2];
+    // per-range offsets follow the order records were written; results report
+    // counts, and offsets are recovered from the flat arrays on the host
+    std::vector<uint64_t> soff(n_ranges + 1, 0), coff(n_ranges + 1, 0);
+    for (uint32_t i = 0; i < n_ranges; i++) {
+        ccs_range_result& r = results[i];
+        memset(&r, 0, sizeof(r));
+        r.n_survivors = hc[4 + 3 * i];
+        r.n_chains = hc[4 + 3 * i + 1];
+        r.n_primes = hc[4 + 3 * i + 2];
+        ccs_engine* E = b->prof[ranges[i].profile];
+        uint64_t cpt = 0;
+        for (uint32_t w : E->hp.wheel_total) cpt += w;
+        // exact candidate count: lines of each tile class times their blocks
+        uint32_t e0 = (uint32_t)(mk128(ranges[i].tile_start_lo, ranges[i].tile_start_hi) % 6);
+        uint64_t cand = 0;
+        for (uint32_t c6 = 0; c6 < 6; c6++) {
+            uint64_t endc = (uint64_t)e0 + ranges[i].n_tiles;
+            uint64_t jhi = endc > c6 ? (endc - c6 + 5) / 6 : 0;
+            uint64_t jlo = c6 < e0 ? 1 : 0;
+            if (jhi > jlo) cand += (jhi - jlo) * E->hp.lines_per_class[c6];
+        }
+        r.candidates = cand;
+        r.status = (ns > b->surv_cap || nch > b->chain_cap) ? CCS_OVERFLOW : CCS_OK;
+    }
+    uint64_t ncopy = std::min<uint64_t>(ns, b->surv_cap);
+    uint64_t ccopy = std::min<uint64_t>(nch, b->chain_cap);
+    if (surv_host && ncopy) CU(cudaMemcpy(surv_host, b->d_surv.p, 16 * ncopy, cudaMemcpyDeviceToHost));
+    if (chains_host && ccopy) CU(cudaMemcpy(chains_host, b->d_chains.p, 48 * ccopy, cudaMemcpyDeviceToHost));
+    if (ns > b->surv_cap || nch > b->chain_cap) st = fail(CCS_OVERFLOW, "batch capacity exceeded");
+    return st;
+}
+
+ccs_status ccs_batch_last_ms(const ccs_batch* b, float* ms) {
+    if (!b || !ms) return fail(CCS_ERR_INVALID, "null argument");
+    *ms = b->last_ms;
+    return CCS_OK;
+}
+
+}  // extern "C"

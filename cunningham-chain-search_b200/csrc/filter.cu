@@ -1,0 +1,372 @@
+// Depth-filter kernels for sm_100a.
+//
+// Reference behaviour replaced: cc18_filter_kernel (v13:1551-1714, v15:1753-1929)
+// and the host residue preparation prepare_batch (v13:1232-1259).
+//
+// Design (see ccs_internal.h for the line / phase model):
+//   * one warp owns 32 lines (residues r mod W) and sweeps them along the
+//     block index J, 64 blocks ("a word") per step;
+//   * level A: every filter prime q < 128 is bit-sliced.  Its 64-position kill
+//     word is a window of the q-periodic phase pattern, held in 2-4 registers
+//     and advanced by two shifts and an OR per word -- no table lookups, no
+//     per-candidate arithmetic;
+//   * level B: surviving positions are tested one by one against the primes in
+//     [128, split) using per-lane phases cached in shared memory and the G_q
+//     bitmaps (early exit, ascending q);
+//   * level C: the rare level-B survivors are queued in global memory and a
+//     warp-cooperative kernel tests all primes >= split (32 primes per round,
+//     ballot early exit);
+//   * survivors are written as the reference's 16-byte Survivor records.
+#include "ccs_kernels.cuh"
+
+namespace ccs {
+
+__constant__ ProfileConst c_prof[kMaxProfiles];
+
+// x mod q for x < 2^32 with magic = floor(2^32 / q)
+__device__ __forceinline__ uint32_t mod_magic(uint32_t x, uint32_t q, uint32_t magic) {
+    uint32_t t = x - __umulhi(x, magic) * q;
+    return t >= q ? t - q : t;
+}
+
+// x mod q for x < 2^64 with magic64 = floor(2^64 / q)
+__device__ __forceinline__ uint32_t mod_magic64(uint64_t x, uint32_t q, uint64_t magic64) {
+    uint64_t t = x - __umul64hi(x, magic64) * (uint64_t)q;
+    while (t >= q) t -= q;
+    return (uint32_t)t;
+}
+
+__device__ __forceinline__ uint32_t sel8(const uint32_t (&e)[8], uint32_t idx) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int x = 0; x < 8; x++) v = (idx == (uint32_t)x) ? e[x] : v;
+    return v;
+}
+
+// Phase of line residue r for slot prime q at block offset j (relative to J0):
+// (r*winv + J0 mod q + j) mod q.  Init-time only.
+__device__ __forceinline__ uint32_t phase_of(uint64_t r, uint32_t q, uint32_t winv, uint32_t j0q,
+                                             uint64_t j) {
+    uint64_t rm = r % q;
+    uint64_t v = rm * winv + j0q + (j % q);
+    return (uint32_t)(v % q);
+}
+
+// ---------------------------------------------------------------------------
+// per-range J0 mod q tables (replaces the host u128 prepare_batch)
+// ---------------------------------------------------------------------------
+__global__ void range_setup_kernel(const RangeDev* __restrict__ ranges,
+                                   const SweepHeader* __restrict__ hdr,
+                                   const uint32_t* __restrict__ primes, uint32_t n_primes,
+                                   uint32_t* __restrict__ jmod, uint32_t jmod_stride) {
+    const uint32_t n_ranges = hdr->n_ranges;
+    for (uint32_t r = blockIdx.y; r < n_ranges; r += gridDim.y) {
+    const RangeDev& R = ranges[r];
+    const uint32_t* pr = primes + R.prime_base;
+    uint32_t np = R.n_range_primes;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+        uint32_t q = pr[i];
+        uint64_t acc = 0;
+#pragma unroll
+        for (int w = 3; w >= 0; w--) acc = ((acc << 32) | R.J0[w]) % q;
+        jmod[(uint64_t)r * jmod_stride + i] = (uint32_t)acc;
+    }
+    }
+    (void)n_primes;
+}
+
+// ---------------------------------------------------------------------------
+// survivor emission
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void emit_survivor(const RangeDev& R, const Line& ln, uint32_t j) {
+    uint32_t c = ln.bc >> 16;
+    uint32_t slot = atomicAdd(R.surv_count, 1u);
+    if (R.range_count) atomicAdd(R.range_count, 1u);
+    if (slot < R.surv_cap) {
+        uint4 rec;
+        rec.x = ln.bc & 0xFFFFu;
+        rec.y = ln.k;
+        rec.z = 6u * j + c - R.e0 + R.tile_bias;
+        rec.w = R.range_id;
+        reinterpret_cast<uint4*>(R.surv)[slot] = rec;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sweep kernel (levels A and B)
+// ---------------------------------------------------------------------------
+struct SweepArgs {
+    const RangeDev* ranges;
+    const uint64_t* unit_prefix;   // [n_ranges + 1] exclusive prefix of units
+    const SweepHeader* hdr;
+    const uint32_t* jmod;          // [n_ranges][jmod_stride]
+    uint32_t jmod_stride;
+    CQueue cq;                     // level-C queue
+    uint32_t b_stride;             // level-B primes per lane column in shared memory
+};
+
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_kernel(SweepArgs a) {
+    extern __shared__ uint16_t s_phase[];                 // [warps][kMaxLevelB][32]
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp_in_block = threadIdx.x >> 5;
+    uint16_t* S = s_phase + (size_t)warp_in_block * a.b_stride * 32;
+    const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+
+    const uint32_t n_ranges = a.hdr->n_ranges;
+    const uint64_t total_units = a.hdr->total_units;
+    uint32_t cur_range = 0;
+    for (uint64_t u = gwarp; u < total_units; u += nwarps) {
+        // locate the range of unit u: units grow monotonically per warp, so a
+        // forward scan from the previous range suffices after one binary search
+        if (u >= a.unit_prefix[cur_range + 1] || u < a.unit_prefix[cur_range]) {
+            uint32_t lo = 0, hi = n_ranges;                 // find last prefix <= u
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (a.unit_prefix[mid] <= u) lo = mid; else hi = mid;
+            }
+            cur_range = lo;
+        }
+        const RangeDev& R = a.ranges[cur_range];
+        const ProfileConst& P = c_prof[R.profile];
+        const uint32_t* jm = a.jmod + (uint64_t)cur_range * a.jmod_stride;
+        const uint64_t local = u - a.unit_prefix[cur_range];
+        const uint32_t n_groups = (P.n_lines + 31) >> 5;
+        const uint32_t g = (uint32_t)(local % n_groups);
+        const uint32_t wc = (uint32_t)(local / n_groups);
+        const uint32_t w0 = wc * R.unit_words;
+        const uint32_t w1 = min(w0 + R.unit_words, R.n_words);
+
+        const uint32_t li = g * 32 + lane;
+        const bool has_line = li < P.n_lines;
+        Line ln = has_line ? P.lines[li] : Line{0, 0, 0, 0};
+        const uint64_t r = ((uint64_t)ln.r_hi << 32) | ln.r_lo;
+        const uint32_t c = ln.bc >> 16;
+        const uint32_t jlo = (c < R.e0) ? 1u : 0u;
+        const uint32_t end = R.e0 + R.n_tiles;          // < 2^32 + 6 handled as u64 below
+        const uint64_t endc = (uint64_t)R.e0 + R.n_tiles;
+        const uint32_t jhi = has_line && endc > c ? (uint32_t)((endc - c + 5) / 6) : 0u;
+        (void)end;
+        const uint64_t jbase = (uint64_t)w0 * 64;
+
+        // ---- level A windows at block jbase ----
+        uint64_t A1w[kNumA1];
+        uint32_t A2w[kNumA2][3];
+        uint32_t A3w[kNumA3][4];
+#pragma unroll
+        for (int i = 0; i < kNumA; i++) {
+            const LevelA& la = P.A[i];
+            uint32_t e[8];
+#pragma unroll
+            for (int m = 0; m < 8; m++) e[m] = la.ext[m];
+            uint32_t ph = (la.q > 1) ? phase_of(r, la.q, la.winv, jm[i], jbase) : 0u;
+            uint32_t aw = ph >> 5, b = ph & 31;
+            uint32_t wds[5];
+#pragma unroll
+            for (int m = 0; m < 5; m++)
+                wds[m] = __funnelshift_r(sel8(e, aw + m), sel8(e, aw + m + 1), b);
+            if (i < kNumA1) {
+                A1w[i] = ((uint64_t)wds[1] << 32) | wds[0];
+            } else if (i < kNumA1 + kNumA2) {
+#pragma unroll
+                for (int m = 0; m < 3; m++) A2w[i - kNumA1][m] = wds[m];
+            } else {
+#pragma unroll
+                for (int m = 0; m < 4; m++) A3w[i - kNumA1 - kNumA2][m] = wds[m];
+            }
+        }
+        // ---- level B phases at block jbase (lane-private shared column) ----
+        const uint32_t nB = P.nB;
+        for (uint32_t p = 0; p < nB; p++) {
+            const PrimeC pc = P.primesB[p];
+            S[p * 32 + lane] = (uint16_t)phase_of(r, pc.q, pc.winv, jm[kNumA + p], jbase);
+        }
+
+        for (uint32_t w = w0; w < w1; w++) {
+            uint64_t kill = 0;
+#pragma unroll
+            for (int i = 0; i < kNumA1; i++) {
+                const uint32_t s = P.A[i].s, t = P.A[i].t;
+                uint64_t W = A1w[i];
+                kill |= W;
+                A1w[i] = (W >> s) | (W << t);
+            }
+#pragma unroll
+            for (int i = 0; i < kNumA2; i++) {
+                const uint32_t t = P.A[kNumA1 + i].t;
+                uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
+                kill |= ((uint64_t)o1 << 32) | o0;
+                A2w[i][0] = o2 | (o0 << t);
+                A2w[i][1] = __funnelshift_l(o0, o1, t);
+                A2w[i][2] = __funnelshift_l(o1, o2, t);
+            }
+#pragma unroll
+            for (int i = 0; i < kNumA3; i++) {
+                const uint32_t t = P.A[kNumA1 + kNumA2 + i].t;
+                uint32_t o0 = A3w[i][0], o1 = A3w[i][1], o2 = A3w[i][2], o3 = A3w[i][3];
+                kill |= ((uint64_t)o1 << 32) | o0;
+                A3w[i][0] = o2;
+                A3w[i][1] = o3 | (o0 << t);
+                A3w[i][2] = __funnelshift_l(o0, o1, t);
+                A3w[i][3] = __funnelshift_l(o1, o2, t);
+            }
+            // positions of this word inside [jlo, jhi)
+            const uint32_t wb = w * 64;
+            uint64_t valid = 0;
+            if (jhi > wb && jlo < wb + 64) {
+                uint32_t lo = jlo > wb ? jlo - wb : 0;
+                uint32_t hi = jhi - wb < 64 ? jhi - wb : 64;
+                valid = (hi >= 64 ? ~0ull : ((1ull << hi) - 1)) & ~((1ull << lo) - 1);
+            }
+            uint64_t surv = ~kill & valid;
+            while (surv) {
+                const uint32_t bit = __ffsll((long long)surv) - 1;
+                surv &= surv - 1;
+                const uint32_t j = wb + bit;
+                const uint32_t jrel = j - (uint32_t)jbase;
+                bool ok = true;
+                for (uint32_t p = 0; p < nB; p++) {
+                    const PrimeC pc = P.primesB[p];
+                    uint32_t uph = mod_magic((uint32_t)S[p * 32 + lane] + jrel, pc.q, pc.magic);
+                    uint32_t wv = __ldg(P.bitmapB + pc.off + (uph >> 5));
+                    if ((wv >> (uph & 31)) & 1u) { ok = false; break; }
+                }
+                if (!ok) continue;
+                if (P.nC == 0) {
+                    emit_survivor(R, ln, j);
+                } else {
+                    uint32_t slot = atomicAdd(a.cq.count, 1u);
+                    if (slot < a.cq.cap) {
+                        uint4 e; e.x = li; e.y = j; e.z = cur_range; e.w = 0;
+                        a.cq.items[slot] = e;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// level C: warp-cooperative test of queued candidates against primes >= split
+// ---------------------------------------------------------------------------
+struct LevelCArgs {
+    const RangeDev* ranges;
+    const uint32_t* jmod;
+    uint32_t jmod_stride;
+    CQueue cq;
+};
+
+__global__ void __launch_bounds__(256)
+levelc_kernel(LevelCArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = min(*a.cq.count, a.cq.cap);
+    for (uint64_t e = gwarp; e < n; e += nwarps) {
+        const uint4 it = a.cq.items[e];
+        const RangeDev& R = a.ranges[it.z];
+        const ProfileConst& P = c_prof[R.profile];
+        const Line ln = P.lines[it.x];
+        const uint64_t r = ((uint64_t)ln.r_hi << 32) | ln.r_lo;
+        const uint32_t j = it.y;
+        const uint32_t* jm = a.jmod + (uint64_t)it.z * a.jmod_stride + kNumA + P.nB;
+        bool killed = false;
+        for (uint32_t base = 0; base < P.nC && !killed; base += 32) {
+            const uint32_t p = base + lane;
+            bool kill = false;
+            if (p < P.nC) {
+                const PrimeC pc = P.primesC[p];
+                uint32_t rm = mod_magic64(r, pc.q, pc.magic64);
+                uint32_t rw = mod_magic64((uint64_t)rm * pc.winv, pc.q, pc.magic64);
+                uint32_t jq = mod_magic64(j, pc.q, pc.magic64);
+                uint32_t uph = mod_magic64((uint64_t)rw + jm[p] + jq, pc.q, pc.magic64);
+                const uint32_t* lst = P.listC + pc.off;
+                // sorted list: binary search
+                uint32_t lo = 0, hi = pc.cnt;
+                while (lo < hi) {
+                    uint32_t mid = (lo + hi) >> 1;
+                    uint32_t v = __ldg(lst + mid);
+                    if (v < uph) lo = mid + 1; else hi = mid;
+                }
+                kill = lo < pc.cnt && __ldg(lst + lo) == uph;
+            }
+            killed = __any_sync(0xFFFFFFFFu, kill);
+        }
+        if (!killed && lane == 0) emit_survivor(R, ln, j);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch helpers
+// ---------------------------------------------------------------------------
+cudaError_t upload_profile_const(int slot, const ProfileConst& pc, cudaStream_t st) {
+    return cudaMemcpyToSymbolAsync(c_prof, &pc, sizeof(ProfileConst), slot * sizeof(ProfileConst),
+                                   cudaMemcpyHostToDevice, st);
+}
+
+cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, uint32_t max_ranges,
+                               const uint32_t* primes, uint32_t max_primes, uint32_t* jmod,
+                               uint32_t stride, cudaStream_t st) {
+    dim3 grid((max_primes + 255) / 256, max_ranges < 65535 ? max_ranges : 65535);
+    if (grid.x == 0) grid.x = 1;
+    if (grid.x > 64) grid.x = 64;
+    if (grid.y == 0) grid.y = 1;
+    range_setup_kernel<<<grid, 256, 0, st>>>(ranges, hdr, primes, max_primes, jmod, stride);
+    return cudaGetLastError();
+}
+
+size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride) {
+    return (size_t)(block_threads / 32) * b_stride * 32 * sizeof(uint16_t);
+}
+
+static bool g_sweep_attr_set = false;
+
+// raise the dynamic shared-memory limit of the sweep kernel once (never
+// during stream capture: callers invoke this before capturing)
+static cudaError_t ensure_sweep_attr() {
+    if (g_sweep_attr_set) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sweep_smem_bytes(kSweepThreads, kMaxLevelB));
+    if (e == cudaSuccess) g_sweep_attr_set = true;
+    return e;
+}
+
+int sweep_blocks_per_sm(uint32_t b_stride) {
+    int nb = 0;
+    if (ensure_sweep_attr() != cudaSuccess) return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel, kSweepThreads,
+                                                  sweep_smem_bytes(kSweepThreads, b_stride));
+    return nb;
+}
+
+cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
+                         const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride, CQueue cq,
+                         uint32_t b_stride, uint32_t grid, cudaStream_t st) {
+    size_t smem = sweep_smem_bytes(kSweepThreads, b_stride);
+    cudaError_t e = ensure_sweep_attr();
+    if (e != cudaSuccess) return e;
+    SweepArgs a;
+    a.ranges = ranges;
+    a.unit_prefix = unit_prefix;
+    a.hdr = hdr;
+    a.jmod = jmod;
+    a.jmod_stride = stride;
+    a.cq = cq;
+    a.b_stride = b_stride;
+    sweep_kernel<<<grid, kSweepThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_levelc(const RangeDev* ranges, const uint32_t* jmod, uint32_t stride, CQueue cq,
+                          uint32_t grid, cudaStream_t st) {
+    LevelCArgs a;
+    a.ranges = ranges;
+    a.jmod = jmod;
+    a.jmod_stride = stride;
+    a.cq = cq;
+    levelc_kernel<<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace ccs

@@ -1,0 +1,247 @@
+// Host-side lattice and filter-table builder.
+//
+// Replaces the reference's one-time table construction: forbidden residues
+// (v13:771-787, v33:585-609), CRT bases with mod-6 buckets (v13:907-1059,
+// v33:636-793) and the per-stage filter tables (v13:793-901, v15:871-1011).
+// Everything is parametric: any CRT / wheel / stage prime lists, depth up to
+// 32, filter primes up to 2^24.
+#include "ccs_internal.h"
+
+#include <algorithm>
+#include <map>
+#include <set>
+#include <cstring>
+
+namespace ccs {
+
+bool is_prime_u32(uint32_t n) {
+    if (n < 2) return false;
+    if (n % 2 == 0) return n == 2;
+    for (uint32_t d = 3; (uint64_t)d * d <= n; d += 2)
+        if (n % d == 0) return false;
+    return true;
+}
+
+static uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t m) {
+    return (uint64_t)((unsigned __int128)a * b % m);
+}
+
+static uint64_t powmod64(uint64_t b, uint64_t e, uint64_t m) {
+    uint64_t r = 1 % m;
+    b %= m;
+    while (e) {
+        if (e & 1) r = mulmod64(r, b, m);
+        b = mulmod64(b, b, m);
+        e >>= 1;
+    }
+    return r;
+}
+
+uint32_t mod_inverse_u32(uint32_t a, uint32_t q) {
+    // extended Euclid
+    int64_t t = 0, nt = 1, r = q, nr = a % q;
+    while (nr) {
+        int64_t qq = r / nr;
+        int64_t tmp = t - qq * nt; t = nt; nt = tmp;
+        tmp = r - qq * nr; r = nr; nr = tmp;
+    }
+    if (t < 0) t += q;
+    return (uint32_t)t;
+}
+
+// Residues n mod q with q | p_i = 2^i (n+1) - 1 for some i in [pos_lo, min(L, q)):
+// n = 2^{-i} - 1.  Walk x = 2^{-i} by repeated multiplication with 2^{-1}.
+static std::vector<uint32_t> forbidden_set(uint32_t q, uint32_t L, uint32_t pos_lo) {
+    std::set<uint32_t> s;
+    uint64_t inv2 = (q + 1) / 2;                 // 2^{-1} mod odd q
+    uint64_t x = 1;                               // 2^{-0}
+    uint32_t hi = std::min<uint32_t>(L, q);
+    for (uint32_t i = 0; i < hi; i++) {
+        if (i >= pos_lo) s.insert((uint32_t)((x + q - 1) % q));
+        x = x * inv2 % q;
+    }
+    return std::vector<uint32_t>(s.begin(), s.end());
+}
+
+std::string build_profile(HostProfile& hp, uint32_t split_prime) {
+    // ---- validation -------------------------------------------------------
+    if (hp.crt.empty() || hp.wheel.empty()) return "crt and wheel prime lists must be non-empty";
+    if (hp.target < 1 || hp.target > (uint32_t)kMaxChain) return "target out of range [1, 64]";
+    if (hp.depth < 1) hp.depth = 1;
+    if (hp.depth > (uint32_t)kMaxDepth) hp.depth = kMaxDepth;
+    if (hp.depth > hp.target) hp.depth = hp.target;     // v13:3248-3252
+    if (hp.bits < 21 || hp.bits > 160) return "bits out of range [21, 160]";
+    std::set<uint32_t> lattice_primes;
+    unsigned __int128 M = 1, WP = 1;
+    for (uint32_t p : hp.crt) {
+        if (!is_prime_u32(p) || p < 5) return "crt primes must be primes >= 5";
+        if (!lattice_primes.insert(p).second) return "duplicate lattice prime";
+        M *= p;
+    }
+    for (uint32_t p : hp.wheel) {
+        if (!is_prime_u32(p) || p < 5) return "wheel primes must be primes >= 5";
+        if (!lattice_primes.insert(p).second) return "duplicate lattice prime";
+        WP *= p;
+    }
+    if (M >= ((unsigned __int128)1 << 32)) return "product of crt primes must be < 2^32";
+    if (WP >= ((unsigned __int128)1 << 24)) return "wheel period must be < 2^24";
+    unsigned __int128 W = M * WP * 6;
+    if (W >= ((unsigned __int128)1 << 62)) return "lattice modulus 6*M*WP must be < 2^62";
+    hp.M = (uint64_t)M;
+    hp.WP = (uint32_t)WP;
+    hp.W = (uint64_t)W;
+    if (hp.stages.empty() || hp.stages.size() > (size_t)kMaxStages) return "1..4 filter stages required";
+
+    // ---- CRT bases: combine admissible residues of every CRT prime --------
+    std::vector<uint64_t> combos = {0};
+    uint64_t mod = 1;
+    for (uint32_t q : hp.crt) {
+        std::vector<uint32_t> f = forbidden_set(q, hp.target, 0);
+        std::vector<uint64_t> next;
+        uint64_t inv = mod_inverse_u32((uint32_t)(mod % q), q);   // mod^{-1} mod q
+        for (uint64_t a : combos) {
+            for (uint32_t v = 0; v < q; v++) {
+                if (std::binary_search(f.begin(), f.end(), v)) continue;
+                // x == a (mod mod), x == v (mod q)
+                uint64_t d = (v + q - a % q) % q;
+                uint64_t t = d * inv % q;
+                next.push_back(a + mod * t);
+            }
+        }
+        combos.swap(next);
+        mod *= q;
+    }
+    std::sort(combos.begin(), combos.end());
+
+    // ---- wheels and mod-6 classes -----------------------------------------
+    const uint32_t m6 = (uint32_t)(hp.M % 6);
+    const uint32_t inv_m6 = (m6 == 1) ? 1 : 5;             // units mod 6 are self-inverse
+    const uint32_t wp6 = hp.WP % 6;
+    std::vector<std::vector<uint32_t>> wf;
+    for (uint32_t q : hp.wheel) wf.push_back(forbidden_set(q, hp.target, 0));
+    hp.bases.clear(); hp.tkm6.clear(); hp.wheel_total.clear(); hp.lines.clear();
+    for (int c = 0; c < 6; c++) hp.lines_per_class[c] = 0;
+    for (uint64_t base : combos) {
+        if (hp.max_bases && hp.bases.size() >= hp.max_bases) break;
+        std::vector<uint32_t> rq(hp.wheel.size()), step(hp.wheel.size());
+        for (size_t i = 0; i < hp.wheel.size(); i++) {
+            rq[i] = (uint32_t)(base % hp.wheel[i]);
+            step[i] = (uint32_t)(hp.M % hp.wheel[i]);
+        }
+        std::vector<uint32_t> ks;
+        for (uint32_t k = 0; k < hp.WP; k++) {
+            bool ok = true;
+            for (size_t i = 0; i < hp.wheel.size() && ok; i++)
+                if (std::binary_search(wf[i].begin(), wf[i].end(), rq[i])) ok = false;
+            if (ok) ks.push_back(k);
+            for (size_t i = 0; i < hp.wheel.size(); i++) {
+                rq[i] += step[i];
+                if (rq[i] >= hp.wheel[i]) rq[i] -= hp.wheel[i];
+            }
+        }
+        if (ks.empty()) continue;
+        uint32_t bidx = (uint32_t)hp.bases.size();
+        if (bidx >= 65536) return "too many bases (> 65535)";
+        uint32_t t6 = (uint32_t)(((5 + 6 - base % 6) % 6) * inv_m6 % 6);
+        hp.bases.push_back(base);
+        hp.tkm6.push_back(t6);
+        hp.wheel_total.push_back((uint32_t)ks.size());
+        for (uint32_t k : ks) {
+            // tile class c with k == t6 - c*WP (mod 6)
+            uint32_t c = (uint32_t)(((t6 + 6 - k % 6) % 6) * wp6 % 6);
+            unsigned __int128 r = ((unsigned __int128)c * hp.WP + k) * hp.M + base;
+            Line ln;
+            ln.r_lo = (uint32_t)r;
+            ln.r_hi = (uint32_t)(r >> 32);
+            ln.k = k;
+            ln.bc = bidx | (c << 16);
+            hp.lines.push_back(ln);
+            hp.lines_per_class[c]++;
+        }
+    }
+    if (hp.bases.empty()) return "no admissible bases";
+    if (hp.lines.size() >= (1ull << 31)) return "too many lines";
+
+    // ---- filter primes ----------------------------------------------------
+    std::map<uint32_t, std::set<uint32_t>> fmap;
+    hp.expected_tests = 0;
+    double surv = 1.0;
+    for (auto& st : hp.stages) {
+        if (st.pos_lo > 1) return "stage pos_lo must be 0 or 1";
+        for (uint32_t q : st.primes) {
+            if (!is_prime_u32(q) || q < 5) return "filter primes must be primes >= 5";
+            if (lattice_primes.count(q)) return "filter prime divides the lattice modulus";
+            if (q >= (1u << 24)) return "filter primes must be < 2^24";
+            std::vector<uint32_t> f = forbidden_set(q, hp.depth, st.pos_lo);
+            // reference test order: stage by stage, prime by prime
+            hp.expected_tests += surv;
+            surv *= 1.0 - (double)f.size() / q;
+            fmap[q].insert(f.begin(), f.end());
+        }
+    }
+    hp.pass_rate = surv;
+    hp.fprimes.clear();
+    for (auto& kv : fmap) {
+        HostProfile::FPrime fp;
+        fp.q = kv.first;
+        fp.forb.assign(kv.second.begin(), kv.second.end());
+        hp.fprimes.push_back(fp);
+    }
+
+    // ---- level classification ----------------------------------------------
+    memset(hp.A, 0, sizeof(hp.A));
+    for (int i = 0; i < kNumA; i++) hp.A[i].q = 1;      // dummy: no kills
+    int nA1 = 0, nA2 = 0, nA3 = 0;
+    hp.primesB.clear(); hp.primesC.clear(); hp.bitmapB.clear(); hp.listC.clear();
+    const uint64_t Wm = hp.W;
+    for (auto& fp : hp.fprimes) {
+        uint32_t q = fp.q;
+        uint32_t winv = mod_inverse_u32((uint32_t)(Wm % q), q);
+        std::vector<uint32_t> g;
+        for (uint32_t f : fp.forb) g.push_back((uint32_t)((uint64_t)f * winv % q));
+        std::sort(g.begin(), g.end());
+        int slot = -1;
+        if (q < 64 && nA1 < kNumA1) slot = nA1++;
+        else if (q > 64 && q < 96 && nA2 < kNumA2) slot = kNumA1 + nA2++;
+        else if (q > 96 && q < 128 && nA3 < kNumA3) slot = kNumA1 + kNumA2 + nA3++;
+        if (slot >= 0) {
+            LevelA& a = hp.A[slot];
+            a.q = q;
+            a.winv = winv;
+            if (slot < kNumA1) { a.s = 64 % q; a.t = q - a.s; }
+            else if (slot < kNumA1 + kNumA2) { a.s = 0; a.t = q - 64; }
+            else { a.s = 0; a.t = q - 96; }
+            for (uint32_t x = 0; x < 256; x++)
+                if (std::binary_search(g.begin(), g.end(), x % q)) a.ext[x >> 5] |= 1u << (x & 31);
+            continue;
+        }
+        PrimeC pc;
+        memset(&pc, 0, sizeof(pc));
+        pc.q = q;
+        pc.magic = 0xFFFFFFFFu / q;
+        pc.winv = winv;
+        pc.c32 = (uint32_t)((1ull << 32) % q);
+        pc.magic64 = ~0ull / q;
+        if (q < split_prime && q < 65536 && hp.primesB.size() < (size_t)kMaxLevelB) {
+            pc.off = (uint32_t)hp.bitmapB.size();
+            pc.cnt = (uint32_t)g.size();
+            std::vector<uint32_t> bm((q + 31) / 32, 0);
+            for (uint32_t u : g) bm[u >> 5] |= 1u << (u & 31);
+            hp.bitmapB.insert(hp.bitmapB.end(), bm.begin(), bm.end());
+            hp.primesB.push_back(pc);
+        } else {
+            pc.off = (uint32_t)hp.listC.size();
+            pc.cnt = (uint32_t)g.size();
+            hp.listC.insert(hp.listC.end(), g.begin(), g.end());
+            hp.primesC.push_back(pc);
+        }
+    }
+    hp.range_primes.clear();
+    for (int i = 0; i < kNumA; i++) hp.range_primes.push_back(hp.A[i].q);
+    for (auto& p : hp.primesB) hp.range_primes.push_back(p.q);
+    for (auto& p : hp.primesC) hp.range_primes.push_back(p.q);
+    (void)powmod64;
+    return "";
+}
+
+}  // namespace ccs

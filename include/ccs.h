@@ -1,0 +1,248 @@
+/*
+ * ccs.h -- C ABI of the B200 Cunningham-chain search engine.
+ *
+ * The engine replaces the data-parallel hot path of nmicic/cunningham-chain-search
+ * (first-kind chains p, 2p+1, 4p+3, ...): CRT-lattice/wheel candidate
+ * enumeration, the three-stage forbidden-residue depth filter, and the
+ * Miller-Rabin prove / chain walk.  Reference paths below are relative to the
+ * reference repository; "v13" is src/cuda/cc18_filter_cuda_CpC_v13.cu, "v33"
+ * is src/cpu/cc_gmp_v33_03.c.
+ *
+ * Conventions
+ *   - every entry point returns a ccs_status; nothing calls exit() (the
+ *     reference's CUDA_CHECK exits, v13:142-149);
+ *   - a ccs_engine owns all of its device memory; caller buffers are passed as
+ *     plain pointers plus capacities; the *_dev arguments are device pointers,
+ *     the *_host arguments host pointers;
+ *   - "stream" is a cudaStream_t passed as void* (NULL = legacy default);
+ *   - an engine is not thread-safe: use one engine per host thread;
+ *   - capacity overflow returns CCS_OVERFLOW together with the true count;
+ *     records beyond the capacity are not written (the reference truncates
+ *     with a warning, v13:3846-3863).
+ */
+#ifndef CCS_H
+#define CCS_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCS_ABI_VERSION 1
+
+typedef enum {
+    CCS_OK = 0,
+    CCS_ERR_INVALID = 1,      /* bad argument or parameter set */
+    CCS_ERR_CUDA = 2,         /* a CUDA call failed; see ccs_last_error() */
+    CCS_OVERFLOW = 3,         /* output capacity exceeded; count is exact */
+    CCS_ERR_NOMEM = 4,        /* device or host allocation failed */
+    CCS_ERR_TIMEOUT = 5,      /* a bounded device wait gave up */
+    CCS_ERR_BUSY = 6,         /* admission refused: no slot or memory free */
+    CCS_ERR_NOT_FOUND = 7,    /* unknown request id */
+    CCS_ERR_CANCELLED = 8,    /* request was cancelled */
+    CCS_PENDING = 9           /* request still running */
+} ccs_status;
+
+/* One filter stage: the listed primes are tested at chain positions
+ * [pos_lo, min(depth, q)).  The reference's L2 and ext-L2 stages use
+ * pos_lo = 0 (v13:799-828); its line sieve uses pos_lo = 1 (v13:834-846). */
+typedef struct {
+    const uint32_t* primes;
+    uint32_t n_primes;
+    uint32_t pos_lo;
+} ccs_stage;
+
+enum { CCS_KIND_FIRST = 1 };
+
+/* Primality predicate used by the prover. */
+enum {
+    CCS_PRIME_MR = 0,      /* strong-PRP for every witness (v13 gpu_is_prime, v13:1428-1452) */
+    CCS_PRIME_BPSW = 1     /* Baillie-PSW: GMP 6.3 mpz_probab_prime_p(n, 1) (v13:1841) */
+};
+
+/* Prove semantics. */
+enum {
+    CCS_PROVE_ROOTS = 0,   /* reference K2: 132-prime trial division, non-roots dropped (v13:1462-1538) */
+    CCS_PROVE_FULL = 1     /* reference CPU prover: 62-prime trial division, backward walk
+                              to the true root, forward walk (v13:1814-1881) */
+};
+
+/* Engine parameters.  Zero / NULL fields take the reference's values
+ * (v13:155-201): CRT {5..19}, wheel {23,29,31}, stages 37..61 / 67..97 /
+ * 101..863 (line sieve from position 1), target 18, depth = target, bits 89,
+ * v13's 20 witnesses {2..71}, BPSW, full prove. */
+typedef struct {
+    uint32_t kind;                 /* CCS_KIND_FIRST */
+    uint32_t target;               /* chain length for CRT/wheel admissibility (v13 generate_bases) */
+    uint32_t depth;                /* filter depth, clamped to [1, min(target, 32)] (v13:3238-3252) */
+    uint32_t bits;                 /* bit width gate of the prover (v13:1495, 1828) */
+    const uint32_t* crt_primes;    /* lattice modulus M = product */
+    uint32_t n_crt;
+    const uint32_t* wheel_primes;  /* wheel period WP = product */
+    uint32_t n_wheel;
+    const ccs_stage* stages;       /* up to 4 filter stages */
+    uint32_t n_stages;
+    uint32_t max_bases;            /* 0 = every admissible base (v33); 64 = v13's MAX_BASES cap */
+    const uint64_t* witnesses;     /* CCS_PRIME_MR witnesses */
+    uint32_t n_witnesses;
+    uint32_t primality;            /* CCS_PRIME_MR | CCS_PRIME_BPSW */
+    uint32_t prove_mode;           /* CCS_PROVE_ROOTS | CCS_PROVE_FULL */
+    uint32_t flags;                /* reserved, 0 */
+} ccs_params;
+
+/* Filter output: the reference's Survivor record (v13:207-212), 16 bytes.
+ * tile_idx is relative to the tile_start of the call. */
+typedef struct {
+    uint32_t base_idx;
+    uint32_t k_offset;
+    uint32_t tile_idx;
+    uint32_t _pad;         /* written as 0 */
+} ccs_survivor;
+
+/* Prove output.  The first four words are the reference's ChainResult
+ * (v13:218-223); the rest carries the chain root (the reference CPU prover
+ * prints it, v13:1895-1896).  48 bytes. */
+typedef struct {
+    uint32_t base_idx;
+    uint32_t k_offset;
+    uint32_t tile_idx;
+    uint32_t chain_len;
+    uint32_t root[6];      /* true root, little-endian 32-bit limbs (<= 192 bits) */
+    uint32_t flags;        /* bit0: survivor is the root; bit1: chain_len >= target */
+    uint32_t survivor;     /* index of the survivor this record came from */
+} ccs_chain;
+
+enum { CCS_CHAIN_IS_ROOT = 1u, CCS_CHAIN_TARGET = 2u };
+
+typedef struct ccs_engine ccs_engine;
+
+/* Lattice facts of an engine (host copy). */
+typedef struct {
+    uint64_t lattice_m;            /* M */
+    uint32_t wheel_period;         /* WP */
+    uint32_t n_bases;
+    uint64_t n_lines;              /* admissible residues mod W = 6*M*WP */
+    uint64_t candidates_per_tile;  /* sum of wheel sizes / 6 (v13:3980-3987) */
+    uint32_t target, depth, bits;
+    uint32_t n_filter_primes;
+    double expected_tests;         /* E[residue tests per candidate] of the
+                                      reference's stage-ordered early-exit test */
+    double pass_rate;              /* product of per-prime pass fractions */
+    uint64_t launches;             /* kernels this engine has launched so far */
+} ccs_info;
+
+/* ---- engine ---------------------------------------------------------------- */
+
+/* Host-only: build the lattice and filter tables for params and report them
+ * without touching a GPU.  bases (optional) receives up to cap base values. */
+ccs_status ccs_describe(const ccs_params* params, ccs_info* out, uint64_t* bases, uint32_t cap);
+
+/* Builds the lattice, filter tables and device state (replaces v13's
+ * init_filter_tables / generate_bases / gpu_upload_tables, v13:793-1222).
+ * device = CUDA ordinal. */
+ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out);
+ccs_status ccs_destroy(ccs_engine* eng);
+ccs_status ccs_get_info(const ccs_engine* eng, ccs_info* out);
+/* host copies of the lattice: bases[n_bases] */
+ccs_status ccs_get_bases(const ccs_engine* eng, uint64_t* bases, uint32_t cap);
+const char* ccs_last_error(void);
+int ccs_abi_version(void);
+
+/* ---- plain per-range path ------------------------------------------------ */
+
+/* Filter tiles [tile_start, tile_start + n_tiles) (tile_start a u128 given as
+ * lo/hi words) and write survivors to out_dev (device, capacity cap).  The
+ * survivor SET equals the reference K1's for the same range (v13:1551-1714,
+ * launched as v13:3764-3795); order is unspecified.  n_tiles < 2^32.
+ * Replaces prepare_batch + cc18_filter_kernel (v13:1232-1259, 1551-1714). */
+ccs_status ccs_filter_range(ccs_engine* eng, uint64_t tile_start_lo, uint64_t tile_start_hi,
+                            uint64_t n_tiles, ccs_survivor* out_dev, uint64_t cap,
+                            uint64_t* n_out, void* stream);
+
+/* Prove survivors (device array) of the range that started at tile_start.
+ * Replaces cc18_prove_kernel (v13:1462-1538) and prove_survivors_mt
+ * (v13:1967-2068), per params.prove_mode / params.primality.
+ * primes_out (optional) counts survivors whose n tested prime. */
+ccs_status ccs_prove(ccs_engine* eng, const ccs_survivor* surv_dev, uint64_t n_surv,
+                     uint64_t tile_start_lo, uint64_t tile_start_hi, ccs_chain* out_dev,
+                     uint64_t cap, uint64_t* n_out, uint64_t* primes_out, void* stream);
+
+/* Same two steps on HOST buffers, copies included (the reference's per-batch
+ * H2D/D2H boundary, v13:3769-3830). */
+ccs_status ccs_search_range_host(ccs_engine* eng, uint64_t tile_start_lo, uint64_t tile_start_hi,
+                                 uint64_t n_tiles, ccs_survivor* surv_host, uint64_t surv_cap,
+                                 uint64_t* n_surv, ccs_chain* chains_host, uint64_t chain_cap,
+                                 uint64_t* n_chains, uint64_t* primes_out);
+
+/* Walk given numbers forward (p -> 2p+1 while prime) and write each chain
+ * length (0 when the number itself is not prime).  numbers_dev holds n
+ * numbers of limbs x 32-bit little-endian limbs (limbs <= 6).  Same
+ * predicate as the prover. */
+ccs_status ccs_walk_numbers(ccs_engine* eng, const uint32_t* numbers_dev, uint64_t n, uint32_t limbs,
+                            uint32_t* lengths_dev, void* stream);
+
+/* ---- batched path -------------------------------------------------------- */
+
+/* One lattice range of a batch.  profile selects one of the engines passed to
+ * ccs_batch_create (ranges may differ in depth, width and lattice). */
+typedef struct {
+    uint64_t tile_start_lo, tile_start_hi;
+    uint64_t n_tiles;
+    uint32_t profile;
+    uint32_t bits;          /* prover bit gate for this range */
+} ccs_range;
+
+/* Per-range result of a batch. */
+typedef struct {
+    uint64_t n_survivors;   /* exact count (may exceed the slice given) */
+    uint64_t n_chains;
+    uint64_t n_primes;
+    uint64_t candidates;
+    uint64_t surv_offset;   /* first survivor of this range in the batch survivor array */
+    uint64_t chain_offset;
+    uint32_t status;        /* ccs_status of this range */
+    uint32_t _pad;
+} ccs_range_result;
+
+typedef struct ccs_batch ccs_batch;
+
+/* A batch executor over n_profiles engines (all on one device).  Runs every
+ * range of a submission in one persistent filter launch and one prove launch,
+ * recorded once into a CUDA graph and replayed. max_ranges bounds a
+ * submission; surv_cap / chain_cap bound the whole batch. */
+ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, uint32_t max_ranges,
+                            uint64_t surv_cap, uint64_t chain_cap, ccs_batch** out);
+ccs_status ccs_batch_destroy(ccs_batch* b);
+/* ranges are host records; results / survivors / chains are copied back to the
+ * host arrays (surv_host / chains_host may be NULL). */
+ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
+                         ccs_range_result* results, ccs_survivor* surv_host, ccs_chain* chains_host,
+                         void* stream);
+/* device-side timing of the last ccs_batch_run: filter+prove milliseconds */
+ccs_status ccs_batch_last_ms(const ccs_batch* b, float* ms);
+
+/* ---- tuning -------------------------------------------------------------- */
+
+typedef struct {
+    uint32_t block_threads;   /* threads per block of the filter sweep */
+    uint32_t blocks_per_sm;   /* resident blocks requested per SM */
+    uint32_t unit_words;      /* 64-candidate words per lane per work unit */
+    uint32_t split_prime;     /* first prime tested by the deferred warp-cooperative stage */
+} ccs_tuning;
+
+ccs_status ccs_get_tuning(const ccs_engine* eng, ccs_tuning* out);
+ccs_status ccs_set_tuning(ccs_engine* eng, const ccs_tuning* t);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+
+/* Measured INT32 ALU issue rate of the device (tera ops/s): eight independent
+ * IADD3/LOP3 chains per thread, all SMs.  The roofline denominator of the
+ * integer filter kernels. */
+ccs_status ccs_measure_int32_peak(int device, double* tops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CCS_H */

@@ -1,0 +1,190 @@
+"""Generates the committed golden fixtures under tests/golden/ from the
+reference itself (run in the container that holds the reference tree):
+
+  * known_roots.json   -- the reference self-test vectors (v13:2089-2101,
+                          v33:2401, v33:2735) with chain lengths from GMP's
+                          mpz_probab_prime_p walk of the CPU prover
+                          (v13:1870-1881) and from v33's screened walker
+  * cc10_sample.json   -- roots from the reference data sample
+                          (data/sample/cc10plus_roots_sample_1000.txt) with
+                          their GMP chain lengths
+  * gmp_primality.json -- GMP 6.3.0 mpz_probab_prime_p(n, 1) verdicts on
+                          seeded primes, composites, base-2 strong
+                          pseudoprimes and Carmichael numbers
+  * v33_counts.json    -- survivor / stage counters of the reference CPU
+                          engine (cc_gmp_v33 --sieve-only) on seeded
+                          sequential prefix ranges
+  * v13_prover.json    -- output lines of the reference CPU GMP prover pool
+                          (prove_survivors_mt) on survivors of seeded ranges
+  * walk_roots.json    -- seeded 80..110-bit odd roots with GMP forward chain
+                          lengths (the prove-batch workload)
+
+Usage: python tests/golden/make_golden.py   (needs oracle/_ref built by
+`make -C oracle`).
+"""
+import json
+import os
+import random
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+import oracle_bind as ob  # noqa: E402
+
+REF = "/root/reference"
+
+
+def dump(name, obj):
+    with open(os.path.join(HERE, name), "w") as f:
+        json.dump(obj, f, indent=1)
+    print("wrote", name)
+
+
+def main():
+    r33 = ob.ref33()
+    r13 = ob.ref13()
+    assert r33 is not None and r13 is not None, "build oracle/_ref first (make -C oracle)"
+
+    # ---- known roots -----------------------------------------------------
+    vecs = ["2", "89", "1122659", "19099919", "85864769", "26089808579", "665043081119",
+            "554688278429", "4090932431513069", "95405042230542329", "2759832934171386593519",
+            str(int("3d3aa382c918303b5470bad", 16)), str(int("5062b474874cd337fe0f061aaef7c442d1", 16))]
+    known = []
+    for v in vecs:
+        n = int(v)
+        buf = C_buf()
+        full = r33.ref33_full_chain(hex(n)[2:].encode(), buf)
+        fwd = r33.ref_gmp_forward_chain(hex(n)[2:].encode())
+        scr = r33.ref33_forward_chain(hex(n)[2:].encode())
+        known.append({"root": v, "forward": fwd, "v33_screened": scr, "full": full,
+                      "full_root": str(int(buf.value, 16))})
+    q7 = ["0x140ECDB88F050428006DE301E959", "0x1F4FFB48D6888D03552C06F4F1ED",
+          "0x1FEC88EDDD75548569E35D0B2871", "0x1FB44BE8961B14B6BCA70B0059B1"]
+    dump("known_roots.json", {"source": "v13:2089-2101, v33:2401, v33:2735, v13:2816-2821",
+                              "chains": known, "q7_roots": q7})
+
+    # ---- data sample -----------------------------------------------------
+    rows = []
+    with open(os.path.join(REF, "data/sample/cc10plus_roots_sample_1000.txt")) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[1].startswith("0x"):
+                rows.append((parts[0], parts[1]))
+    sample = []
+    for tag, hx in rows:
+        n = int(hx, 16)
+        fwd = r33.ref_gmp_forward_chain(hx[2:].encode())
+        sample.append({"tag": tag, "root": hx, "forward": fwd})
+    dump("cc10_sample.json", {"source": "data/sample/cc10plus_roots_sample_1000.txt",
+                              "roots": sample})
+
+    # ---- GMP primality ---------------------------------------------------
+    rnd = random.Random(20261203)
+    nums = set()
+    for bits in (8, 16, 31, 32, 33, 63, 64, 65, 80, 89, 96, 110, 127, 128, 129, 150, 180):
+        for _ in range(40):
+            nums.add(rnd.getrandbits(bits) | (1 << (bits - 1)) | 1)
+    # primes by search
+    for bits in (40, 64, 89, 110, 128, 160, 190):
+        found = 0
+        while found < 25:
+            n = rnd.getrandbits(bits) | (1 << (bits - 1)) | 1
+            if r33.ref33_gmp_probab_prime(hex(n)[2:].encode(), 25) > 0:
+                nums.add(n)
+                found += 1
+    # strong pseudoprimes to base 2, Carmichael numbers, Wieferich squares
+    spsp2 = [2047, 3277, 4033, 4681, 8321, 15841, 29341, 42799, 49141, 52633, 65281, 74665,
+             80581, 85489, 88357, 90751, 3215031751, 2152302898747, 3474749660383,
+             341550071728321, 3825123056546413051]
+    carm = [561, 1105, 1729, 2465, 2821, 6601, 8911, 10585, 15841, 29341, 41041, 46657, 52633]
+    for v in spsp2 + carm + [1093 ** 2, 3511 ** 2, 1093 * 3511, 2, 3, 5, 7, 9, 15, 25, 49, 97 * 97]:
+        nums.add(v)
+    nums.add(18446744073709551557)  # largest 64-bit prime
+    prim = []
+    for n in sorted(nums):
+        prim.append([str(n), r33.ref33_gmp_probab_prime(hex(n)[2:].encode(), 1)])
+    dump("gmp_primality.json", {"source": "GMP 6.3.0 mpz_probab_prime_p(n, 1) via oracle/_ref",
+                                "cases": prim})
+
+    # ---- v33 sieve-only counts on sequential prefix ranges ----------------
+    counts = []
+    for (bits, target, pbits, seed) in [(89, 18, 47, 1), (89, 18, 47, 2), (89, 18, 46, 3),
+                                        (61, 18, 21, 4), (100, 18, 58, 5), (89, 16, 47, 6),
+                                        (89, 14, 48, 7)]:
+        rr = random.Random(seed)
+        prefix = (1 << (pbits - 1)) | rr.getrandbits(pbits - 1)
+        pstr = "0b" + bin(prefix)[2:]
+        out = subprocess.run([os.path.join(ob.REF_DIR, "cc_gmp_v33"), "--sieve-only", "--prefix", pstr,
+                              "--sequential", "--bits", str(bits), "--target", str(target),
+                              "--threads", "1"], capture_output=True, text=True).stdout
+        wc = int(re.search(r"Wheel candidates \(L1\):\s+(\d+)", out).group(1))
+        l2 = int(re.search(r"Passed L2 bitmask:\s+(\d+)", out).group(1))
+        ext = int(re.search(r"Passed ext L2 \(OPT-7\):\s+(\d+)", out).group(1))
+        lp = int(re.search(r"Line-sieve \(OPT-17\):\s+(\d+) passed", out).group(1))
+        counts.append({"bits": bits, "target": target, "prefix": pstr, "candidates": wc,
+                       "pass_l2": l2, "pass_ext": ext, "survivors": lp})
+    dump("v33_counts.json", {"source": "cc_gmp_v33 --sieve-only --sequential (v33:1690-1960)",
+                             "runs": counts})
+
+    # ---- v13 CPU prover on oracle survivors --------------------------------
+    prover = []
+    for (target, bits, ts, nt) in [(18, 61, (1 << 60) // (20677 * 1616615) + 12345, 600),
+                                   (18, 64, (1 << 63) // (20677 * 1616615) + 777, 400),
+                                   (16, 61, (1 << 60) // (20677 * 1616615) + 4242, 300)]:
+        r13.ref13_setup(target, target)
+        lat = ob.Lattice(lattice_len=target, depth=target)
+        surv = lat.filter_range(ts, nt)
+        lat13_n = r13.ref13_num_bases()
+        if target < 18:
+            # v13 caps the base list at MAX_BASES = 64 (v13:966): keep the
+            # survivors its CPU prover can address
+            surv = surv[surv[:, 0] < lat13_n]
+        s = np.ascontiguousarray(surv.astype(np.uint32))
+        path = tempfile.mktemp(suffix=".txt")
+        import ctypes as C
+        pr, ch = C.c_ulonglong(0), C.c_ulonglong(0)
+        r13.ref13_prove_cpu(s.reshape(-1), len(s), ts & (2**64 - 1), ts >> 64, target, bits,
+                            path.encode(), C.byref(pr), C.byref(ch))
+        lines = [ln.strip() for ln in open(path) if ln.strip()]
+        os.unlink(path)
+        prover.append({"target": target, "depth": target, "bits": bits, "tile_start": str(ts),
+                       "n_tiles": nt, "n_survivors": int(len(surv)), "primes": pr.value,
+                       "chains": ch.value, "lines": sorted(lines),
+                       "survivors": surv.astype(np.int64).tolist()})
+    dump("v13_prover.json", {"source": "prove_survivors_mt (v13:1967-2068) via oracle/_ref",
+                             "runs": prover})
+
+    # ---- walk roots (prove-batch workload) ---------------------------------
+    # odd roots drawn from seeded 80..110-bit tile windows of the 31# lattice at
+    # depth 16, pre-filtered by primes 37..1021 at chain positions 0..15 (the
+    # first filter stage of the prove-batch configuration)
+    rw = random.Random(424242)
+    lat = ob.Lattice(lattice_len=16, depth=16, stages=[(ob.primes_between(37, 1024), 0)])
+    M, WP = lat.M, lat.WP
+    bases = lat.bases()
+    walks = []
+    while len(walks) < 400:
+        bits = rw.randint(80, 110)
+        lo = (1 << (bits - 1)) // (M * WP)
+        hi = (1 << bits) // (M * WP)
+        ts = rw.randint(lo, hi - 20)
+        surv = lat.filter_range(ts, 6)
+        for b, k, t, _ in surv[:4]:
+            n = ((ts + int(t)) * WP + int(k)) * M + bases[int(b)]
+            walks.append({"n": str(n), "forward": r33.ref_gmp_forward_chain(hex(n)[2:].encode())})
+    dump("walk_roots.json", {"source": "GMP mpz_probab_prime_p(., 1) forward walk (v13:1870-1881)",
+                             "roots": walks})
+
+
+def C_buf():
+    import ctypes as C
+    return C.create_string_buffer(256)
+
+
+if __name__ == "__main__":
+    main()

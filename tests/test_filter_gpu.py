@@ -1,0 +1,157 @@
+"""Filter parity on the GPU: the engine's survivor sets equal the oracle's
+(and, where oracle/_ref was built, the reference v13 kernel's own output) on
+seeded windows, plus exact size-independent properties at larger sizes."""
+import os
+import random
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REF13 = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                     "libref13.so")
+
+
+def as_set(arr):
+    a = np.asarray(arr.cpu().numpy() if hasattr(arr, "cpu") else arr).astype(np.int64) & 0xFFFFFFFF
+    return sorted(map(tuple, a[:, :3].tolist()))
+
+
+@pytest.fixture(scope="module")
+def eng18(ccs):
+    e = ccs.Engine()
+    yield e
+    e.close()
+
+
+def windows(ccs, bits, seed, sizes):
+    bases = ccs.describe()[1]
+    t0, t1 = ccs.bit_tile_range(bits, bases, 1616615, 20677)
+    r = random.Random(seed)
+    return [(r.randint(t0, t1 - 10000), n) for n in sizes]
+
+
+def test_reference_params_match_oracle(ccs, ob, eng18):
+    lat = ob.Lattice()
+    for ts, n in windows(ccs, 89, 1, [1, 2, 5, 6, 7, 11, 64, 385, 1000, 2500]):
+        want = as_set(lat.filter_range(ts, n))
+        got = as_set(eng18.filter_range(ts, n, cap=1 << 16))
+        assert got == want, (ts, n)
+
+
+def test_every_start_phase(ccs, ob, eng18):
+    # tile_start mod 6 selects the mod-6 bucket (v13:1589-1590): cover all six
+    lat = ob.Lattice()
+    base = windows(ccs, 89, 2, [1])[0][0]
+    base -= base % 6
+    for e0 in range(6):
+        for n in (1, 4, 13, 389):
+            ts = base + e0 + 1000 * n
+            assert as_set(eng18.filter_range(ts, n)) == as_set(lat.filter_range(ts, n))
+
+
+def test_wide_tile_starts(ccs, ob, eng18):
+    lat = ob.Lattice()
+    for ts in (0, 1, 12345, (1 << 64) - 7, (1 << 64) + 3, (1 << 100) + 17, (1 << 127) // 20677):
+        assert as_set(eng18.filter_range(ts, 97)) == as_set(lat.filter_range(ts, 97)), ts
+
+
+def test_empty_range(eng18):
+    assert eng18.filter_range(123456789, 0).shape[0] == 0
+
+
+def test_overflow_reports_exact_count(ccs, eng18):
+    ts, n = windows(ccs, 89, 3, [3000])[0]
+    full = eng18.filter_range(ts, n, cap=1 << 16)
+    assert full.shape[0] > 10
+    with pytest.raises(ccs.CCSError) as e:
+        eng18.filter_range(ts, n, cap=5)
+    assert e.value.status == ccs.OVERFLOW and str(full.shape[0]) in str(e.value)
+
+
+def test_cc16_scale_params_match_oracle(ccs, ob):
+    """depth 16, stage primes to 2^17: levels A, B and the deferred
+    warp-cooperative stage all take part."""
+    cfg = ccs.config_cc16_scale()
+    eng = ccs.Engine(**cfg)
+    lat = ob.Lattice(lattice_len=16, depth=16, stages=cfg["stages"])
+    info, bases = ccs.describe(**cfg)
+    t0, t1 = ccs.bit_tile_range(88, bases, 1616615, 20677)
+    r = random.Random(9)
+    for n in (1, 7, 200):
+        ts = r.randint(t0, t1 - 1000)
+        assert as_set(eng.filter_range(ts, n)) == as_set(lat.filter_range(ts, n))
+    eng.close()
+
+
+@pytest.mark.parametrize("primes", [
+    "levelA",      # only bit-sliced primes (< 128)
+    "levelB",      # only per-lane primes (128 .. 1023)
+    "levelC",      # only deferred primes (>= 1024): every candidate reaches the last stage
+])
+def test_each_filter_level_alone(ccs, ob, primes):
+    sel = {"levelA": ccs.primes_in(37, 128), "levelB": ccs.primes_in(131, 1024),
+           "levelC": ccs.primes_in(1031, 40000)}[primes]
+    stages = [(sel, 0)]
+    eng = ccs.Engine(target=16, depth=16, stages=stages)
+    lat = ob.Lattice(lattice_len=16, depth=16, stages=stages)
+    r = random.Random(len(sel))
+    for n in (1, 3, 7) if primes == "levelC" else (1, 3, 70):
+        ts = r.randint(1 << 40, 1 << 60)
+        want = as_set(lat.filter_range(ts, n))
+        got = as_set(eng.filter_range(ts, n, cap=1 << 22))
+        assert got == want, (primes, ts, n)
+    eng.close()
+
+
+def test_cpu_method_lattice_matches_oracle(ccs, ob):
+    cfg = ccs.config_cpu_method()
+    eng = ccs.Engine(**cfg)
+    lat = ob.Lattice(wheel=[23], lattice_len=8, depth=8, stages=cfg["stages"])
+    r = random.Random(5)
+    for n in (1, 5, 6, 50, 301):
+        ts = r.randint(1 << 30, 1 << 50)
+        assert as_set(eng.filter_range(ts, n, cap=1 << 20)) == as_set(lat.filter_range(ts, n))
+    eng.close()
+
+
+def test_split_range_additivity_at_scale(ccs):
+    """Filtering [T, T+N) equals filtering [T, T+a) and [T+a, T+N) with tile
+    offsets shifted: an exact property checked at ~1.5e10 candidates."""
+    eng = ccs.Engine(**ccs.config_cc16_scale())
+    ts = (1 << 87) // (1616615 * 20677) + 987654321
+    n = 200_000
+    a = 77_777
+    whole = as_set(eng.filter_range(ts, n, cap=1 << 18))
+    left = as_set(eng.filter_range(ts, a, cap=1 << 18))
+    right = [(b, k, t + a) for b, k, t in as_set(eng.filter_range(ts + a, n - a, cap=1 << 18))]
+    assert whole == sorted(left + right)
+    # survivor rate is within statistical bounds of the predicted pass rate
+    info = eng.info
+    expect = n * info["candidates_per_tile"] * info["pass_rate"]
+    assert abs(len(whole) - expect) < 6 * expect ** 0.5 + 5
+    eng.close()
+
+
+@pytest.mark.skipif(not os.path.exists(REF13), reason="reference harness not built")
+@pytest.mark.parametrize("target,max_bases", [(18, 0), (16, 64)])
+def test_matches_reference_v13_kernel(ccs, ob, target, max_bases):
+    """Bit-identical survivor sets versus the reference's own
+    cc18_filter_kernel, launched as its main loop launches it.  At target 16
+    the reference keeps only its first 64 bases (MAX_BASES); max_bases=64
+    reproduces that."""
+    r13 = ob.ref13()
+    r13.ref13_setup(target, target)
+    r13.ref13_upload(target, 89)
+    eng = ccs.Engine(target=target, max_bases=max_bases)
+    r = random.Random(target)
+    for n in (1, 6, 97, 1000, 16384):
+        ts = r.randint(1 << 50, 1 << 60)
+        cap = 1 << 20
+        out = np.zeros(4 * cap, dtype=np.uint32)
+        cnt = r13.ref13_filter(ts & (2**64 - 1), ts >> 64, n, 12, out, cap)
+        ref = as_set(out[: 4 * cnt].reshape(-1, 4))
+        got = as_set(eng.filter_range(ts, n, cap=cap))
+        assert got == ref, (target, ts, n)
+    eng.close()
