@@ -166,13 +166,16 @@ def run_ours(args):
 
     cfg = ccs.config_cc16_scale()
     eng = ccs.Engine(device=local, **cfg)
+    TILES = args.tiles_per_step
+    if args.unit_words:
+        eng.set_tuning(unit_words=args.unit_words)
     info = eng.info
     cpt = info["candidates_per_tile"]
     bases = eng.bases()
     t_lo, t_hi = ccs.bit_tile_range(BITS, bases, info["lattice_m"], info["wheel_period"])
     import random
     rnd = random.Random(SEED)
-    total_tiles = (args.warmup + args.steps) * TILES_PER_STEP
+    total_tiles = (args.warmup + args.steps + 8) * TILES
     start = rnd.randint(t_lo, t_hi - total_tiles * max(ws, 1) - 1)
     lane0, _ = ccs.lane_range(start, start + total_tiles * ws, ws, rank)
 
@@ -182,7 +185,7 @@ def run_ours(args):
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
 
     def step(ts):
-        surv = eng.filter_range(ts, TILES_PER_STEP, out=surv_buf, stream=stream)
+        surv = eng.filter_range(ts, TILES, out=surv_buf, stream=stream)
         chains, primes = eng.prove(surv, ts, out=chain_buf, stream=stream)
         return surv.shape[0], chains.shape[0], primes
 
@@ -190,7 +193,7 @@ def run_ours(args):
     ts = lane0
     for _ in range(args.warmup):
         step(ts)
-        ts += TILES_PER_STEP
+        ts += TILES
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
@@ -212,7 +215,7 @@ def run_ours(args):
         n_surv += s
         n_chain += c
         n_prime += p
-        ts += TILES_PER_STEP
+        ts += TILES
     torch.cuda.synchronize()
     t_wall = time.time() - t_wall
     step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -224,13 +227,13 @@ def run_ours(args):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms_total = float(t.item())
         pg.barrier()
-    cand_step = TILES_PER_STEP * cpt
+    cand_step = TILES * cpt
     value = ws * args.steps * cand_step / (ms_total * 1e-3)
 
     # dominant kernel: time one filter launch alone on its stream
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    eng.filter_range(ts, TILES_PER_STEP, out=surv_buf, stream=stream)
+    eng.filter_range(ts, TILES, out=surv_buf, stream=stream)
     ev1.record(stream)
     torch.cuda.synchronize()
     filt_ms = ev0.elapsed_time(ev1)
@@ -244,11 +247,11 @@ def run_ours(args):
     t0 = time.time()
     h2d = d2h = 0
     for _ in range(e2e_steps):
-        surv, chains, primes = eng.search_range_host(ts, TILES_PER_STEP, surv_cap=1 << 20,
+        surv, chains, primes = eng.search_range_host(ts, TILES, surv_cap=1 << 20,
                                                      chain_cap=1 << 16)
         h2d += 80 + 16 + 16 + 64                       # range, prefix, header, prove descriptors
         d2h += 16 * len(surv) + 48 * len(chains) + 16  # records + counters
-        ts += TILES_PER_STEP
+        ts += TILES
     e2e_s = time.time() - t0
     e2e_value = ws * e2e_steps * cand_step / e2e_s
 
@@ -267,10 +270,10 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "tiles_per_step": TILES_PER_STEP,
+            "config": {"workload": WORKLOAD, "tiles_per_step": TILES,
                        "candidates_per_step": cand_step, "bits": BITS, "seed": SEED,
                        "start_tile": start, "l2": "flushed (512 MB write) between timed steps",
-                       "parallelism": f"lanes{ws}"},
+                       "parallelism": f"lanes{ws}", "tuning": eng.tuning()},
             "survivors": n_surv, "chains": n_chain, "primes": n_prime,
             "survivor_rate": n_surv / (args.steps * cand_step),
             "roofline": {"bound": "int32", "achieved": achieved, "peak": int_peak, "unit": "TOPS",
@@ -301,6 +304,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tiles-per-step", type=int, default=TILES_PER_STEP,
+                    help="tiles per step (smaller values: profiling cases)")
+    ap.add_argument("--unit-words", type=int, default=0, help="sweep work-unit length (0: tuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3")

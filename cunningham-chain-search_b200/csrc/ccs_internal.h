@@ -36,7 +36,17 @@ struct LevelA {
     uint32_t s;          // A1: 64 mod q          A2/A3: unused
     uint32_t t;          // A1: q - s             A2: q - 64   A3: q - 96
     uint32_t winv;       // W^{-1} mod q
+    uint32_t magic;      // floor(2^32 / q)
+    uint32_t c32;        // 2^32 mod q
+    uint32_t _pad[2];
     uint32_t ext[8];     // 256 bits: bit x = [x mod q in G_q]; all zero = dummy
+};
+
+// Level-B prime record read per candidate test: x = floor(2^32/q),
+// y = q | (bitmap word offset << 16).
+struct PrimeB {
+    uint32_t magic;
+    uint32_t q_off;
 };
 
 // Per-prime constants for the per-candidate stages.
@@ -66,7 +76,9 @@ struct ProfileConst {
     LevelA A[kNumA];
     const Line* lines;
     const PrimeC* primesB;           // level B primes (ascending)
+    const PrimeB* packB;             // compact level B records for the per-candidate test
     const uint32_t* bitmapB;         // G_q bitmaps of level B primes
+    uint32_t std_a;                  // 1: level-A slots hold the standard set 37..127
     const PrimeC* primesC;           // level C primes (ascending)
     const uint32_t* listC;           // sorted G_q lists of level C primes
 };
@@ -99,6 +111,8 @@ struct HostProfile {
     // device-facing tables
     LevelA A[kNumA];
     std::vector<PrimeC> primesB, primesC;
+    std::vector<PrimeB> packB;
+    uint32_t std_a = 0;
     std::vector<uint32_t> bitmapB, listC;
     // index of every level-A/B prime for the per-range J0 mod q table
     std::vector<uint32_t> range_primes;   // A slots (kNumA, dummies as 1) then B then C

@@ -84,12 +84,12 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride);
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride, CQueue cq,
-                         uint32_t b_stride, uint32_t grid, cudaStream_t st);
+                         uint32_t b_stride, uint32_t grid, bool std_a, cudaStream_t st);
 cudaError_t launch_levelc(const RangeDev* ranges, const uint32_t* jmod, uint32_t stride, CQueue cq,
                           uint32_t grid, cudaStream_t st);
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_walk(const uint32_t* numbers, uint64_t n, uint32_t limbs, uint32_t* lengths,
                         int profile, cudaStream_t st);
-int sweep_blocks_per_sm(uint32_t b_stride);
+int sweep_blocks_per_sm(uint32_t b_stride, bool std_a);
 
 }  // namespace ccs

@@ -87,6 +87,7 @@ struct ccs_engine {
     // profile tables
     DevBuf<Line> lines;
     DevBuf<PrimeC> primesB, primesC;
+    DevBuf<PrimeB> packB;
     DevBuf<uint32_t> bitmapB, listC, range_primes;
     DevBuf<uint64_t> bases;
 
@@ -172,6 +173,9 @@ ccs_status upload_profile(ccs_engine* E, cudaStream_t st) {
     CU(E->primesC.alloc(hp.primesC.size()));
     if (!hp.primesC.empty())
         CU(cudaMemcpy(E->primesC.p, hp.primesC.data(), sizeof(PrimeC) * hp.primesC.size(), cudaMemcpyHostToDevice));
+    CU(E->packB.alloc(hp.packB.size()));
+    if (!hp.packB.empty())
+        CU(cudaMemcpy(E->packB.p, hp.packB.data(), sizeof(PrimeB) * hp.packB.size(), cudaMemcpyHostToDevice));
     CU(E->bitmapB.alloc(hp.bitmapB.size()));
     if (!hp.bitmapB.empty())
         CU(cudaMemcpy(E->bitmapB.p, hp.bitmapB.data(), 4 * hp.bitmapB.size(), cudaMemcpyHostToDevice));
@@ -192,7 +196,9 @@ ccs_status upload_profile(ccs_engine* E, cudaStream_t st) {
     memcpy(pc.A, hp.A, sizeof(pc.A));
     pc.lines = E->lines.p;
     pc.primesB = E->primesB.p;
+    pc.packB = E->packB.p;
     pc.bitmapB = E->bitmapB.p;
+    pc.std_a = hp.std_a;
     pc.primesC = E->primesC.p;
     pc.listC = E->listC.p;
     CU(upload_profile_const(E->slot, pc, st));
@@ -224,8 +230,17 @@ uint64_t units_of(const ccs_engine* E, uint32_t n_words, uint32_t unit_words) {
     return groups * chunks;
 }
 
+// words per work unit: the tuned length, shortened when the range is too
+// small to give every resident warp several units
 uint32_t choose_unit_words(const ccs_engine* E, uint32_t n_words) {
-    uint32_t uw = E->tune.unit_words ? E->tune.unit_words : 256;
+    uint32_t uw = E->tune.unit_words ? E->tune.unit_words : 1024;
+    uint64_t groups = (E->hp.lines.size() + 31) / 32;
+    uint64_t warps = (uint64_t)E->sms * std::max<uint32_t>(E->tune.blocks_per_sm, 1) * (kSweepThreads / 32);
+    uint64_t chunks_wanted = (4 * warps + groups - 1) / groups;
+    if (chunks_wanted > 1) {
+        uint64_t fit = (n_words + chunks_wanted - 1) / chunks_wanted;
+        if (fit < uw) uw = (uint32_t)std::max<uint64_t>(fit, 32);
+    }
     if (uw > n_words) uw = n_words ? n_words : 1;
     return uw;
 }
@@ -337,7 +352,7 @@ ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out) {
         if (s != CCS_OK) { delete E; return s; }
     }
     E->tune.block_threads = kSweepThreads;
-    E->tune.unit_words = 256;
+    E->tune.unit_words = 1024;
     E->tune.split_prime = 1024;
     // fraction of candidates that reach level C
     double f = 1.0;
@@ -353,7 +368,7 @@ ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out) {
     CU(cudaStreamCreateWithFlags(&E->own_stream, cudaStreamNonBlocking));
     ccs_status st = upload_profile(E, E->own_stream);
     if (st != CCS_OK) { ccs_destroy(E); return st; }
-    int bps = sweep_blocks_per_sm(b_stride_of((uint32_t)hp.primesB.size()));
+    int bps = sweep_blocks_per_sm(b_stride_of((uint32_t)hp.primesB.size()), hp.std_a != 0);
     E->tune.blocks_per_sm = bps > 0 ? (uint32_t)bps : 1;
 
     // plain-path state
@@ -376,7 +391,7 @@ ccs_status ccs_destroy(ccs_engine* E) {
     if (!E) return CCS_OK;
     cudaSetDevice(E->device);
     if (E->own_stream) cudaStreamSynchronize(E->own_stream);
-    E->lines.free_(); E->primesB.free_(); E->primesC.free_(); E->bitmapB.free_();
+    E->lines.free_(); E->primesB.free_(); E->primesC.free_(); E->bitmapB.free_(); E->packB.free_();
     E->listC.free_(); E->range_primes.free_(); E->bases.free_();
     E->d_range.free_(); E->d_prange.free_(); E->d_prefix.free_(); E->d_hdr.free_();
     E->d_jmod.free_(); E->d_counters.free_(); E->d_cq.free_();
@@ -464,7 +479,7 @@ static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_t
     if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
     CU(launch_sweep(E->d_range.p, E->d_prefix.p, E->d_hdr.p, E->d_jmod.p,
                     (uint32_t)hp.range_primes.size(), cq, b_stride_of((uint32_t)hp.primesB.size()),
-                    grid, st));
+                    grid, hp.std_a != 0, st));
     if (!hp.primesC.empty()) {
         CU(launch_levelc(E->d_range.p, E->d_jmod.p, (uint32_t)hp.range_primes.size(), cq,
                          (uint32_t)E->sms * 8, st));
@@ -674,7 +689,9 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     CU(cudaEventCreate(&b->ev0));
     CU(cudaEventCreate(&b->ev1));
-    int bps = sweep_blocks_per_sm(b->b_stride);
+    bool all_std = true;
+    for (auto* E : b->prof) all_std &= E->hp.std_a != 0;
+    int bps = sweep_blocks_per_sm(b->b_stride, all_std);
     b->grid = (uint32_t)b->prof[0]->sms * (uint32_t)std::max(bps, 1);
 
     // record the whole batch once: H2D descriptors, setup, sweep, level C,
@@ -690,7 +707,7 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
                        b->d_jmod.p, b->jstride, st);
     CQueue cq{b->d_counts.p + 1, b->cq_cap, b->d_cq.p};
     launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, cq, b->b_stride,
-                 b->grid, st);
+                 b->grid, all_std, st);
     if (any_c) launch_levelc(b->d_ranges.p, b->d_jmod.p, b->jstride, cq, (uint32_t)b->prof[0]->sms * 8, st);
     ProveArgs pa;
     pa.ranges = b->d_pranges.p;

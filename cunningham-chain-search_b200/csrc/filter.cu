@@ -43,15 +43,6 @@ __device__ __forceinline__ uint32_t sel8(const uint32_t (&e)[8], uint32_t idx) {
     return v;
 }
 
-// Phase of line residue r for slot prime q at block offset j (relative to J0):
-// (r*winv + J0 mod q + j) mod q.  Init-time only.
-__device__ __forceinline__ uint32_t phase_of(uint64_t r, uint32_t q, uint32_t winv, uint32_t j0q,
-                                             uint64_t j) {
-    uint64_t rm = r % q;
-    uint64_t v = rm * winv + j0q + (j % q);
-    return (uint32_t)(v % q);
-}
-
 // ---------------------------------------------------------------------------
 // per-range J0 mod q tables (replaces the host u128 prepare_batch)
 // ---------------------------------------------------------------------------
@@ -105,12 +96,98 @@ struct SweepArgs {
     uint32_t b_stride;             // level-B primes per lane column in shared memory
 };
 
+// standard level-A set (every prime 37..127): slots 0..6, 9..14, 15..21
+__device__ constexpr uint32_t kStdQ[kNumA] = {37, 41, 43, 47, 53, 59, 61, 1, 1,
+                                              67, 71, 73, 79, 83, 89,
+                                              97, 101, 103, 107, 109, 113, 127};
+
+constexpr int kQCap = 256;               // per-warp level-B queue (entries)
+constexpr uint32_t kNone = 0xFFFFFFFFu;  // empty lane slot
+
+// x mod q for x < 2^32 via the profile's magic (fast init-time reductions)
+__device__ __forceinline__ uint32_t phase_fast(uint32_t rl, uint32_t rh, uint32_t q, uint32_t magic,
+                                               uint32_t c32, uint32_t winv, uint32_t j0q,
+                                               uint32_t jb) {
+    uint32_t a = mod_magic(rh, q, magic) * c32 + mod_magic(rl, q, magic);   // < q^2 + q
+    a = mod_magic(a, q, magic);
+    a = mod_magic(a * winv, q, magic);                                     // r * W^-1 mod q
+    uint32_t v = a + j0q + mod_magic(jb, q, magic);                        // < 3q
+    v = v >= q ? v - q : v;
+    return v >= q ? v - q : v;
+}
+
+// Per-warp level-B machinery: a queue of (lane line, block offset) entries in
+// shared memory and one candidate per lane, refilled whenever a lane's
+// candidate is decided, so lanes stay busy whichever line produced the work.
+struct LevelB {
+    uint32_t* Q;                   // kQCap entries: (jrel << 5) | line lane
+    const uint16_t* S;             // [nB][32] phases of the unit's 32 lines at jbase
+    const PrimeB* pb;
+    const uint32_t* bm;
+    uint32_t nB;
+    uint32_t head, tail;           // warp-uniform
+    uint32_t cur, pi;              // this lane's candidate and next prime index
+};
+
+__device__ __forceinline__ void b_emit(const SweepArgs& a, const RangeDev& R, const ProfileConst& P,
+                                       uint32_t cur_range, uint32_t g, uint32_t jbase, uint32_t e) {
+    const uint32_t L = e & 31u;
+    const uint32_t j = jbase + (e >> 5);
+    const uint32_t li = g * 32 + L;
+    const Line ln = P.lines[li];
+    if (P.nC == 0) {
+        emit_survivor(R, ln, j);
+    } else {
+        uint32_t slot = atomicAdd(a.cq.count, 1u);
+        if (slot < a.cq.cap) {
+            uint4 it; it.x = li; it.y = j; it.z = cur_range; it.w = 0;
+            a.cq.items[slot] = it;
+        }
+    }
+}
+
+// one round: refill empty lanes from the queue, then test two primes
+__device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const RangeDev& R,
+                                        const ProfileConst& P, uint32_t cur_range, uint32_t g,
+                                        uint32_t jbase, uint32_t lane_lt) {
+    const bool needy = B.cur == kNone;
+    const uint32_t nm = __ballot_sync(0xFFFFFFFFu, needy);
+    const uint32_t avail = B.tail - B.head;
+    if (needy) {
+        const uint32_t rk = __popc(nm & lane_lt);
+        if (rk < avail) { B.cur = B.Q[(B.head + rk) & (kQCap - 1)]; B.pi = 0; }
+    }
+    B.head += min((uint32_t)__popc(nm), avail);
+    if (B.cur != kNone) {
+        const uint32_t L = B.cur & 31u, jrel = B.cur >> 5;
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            if (B.cur != kNone && B.pi < B.nB) {
+                const uint2 pr2 = __ldg(reinterpret_cast<const uint2*>(B.pb) + B.pi);
+                const PrimeB pr{pr2.x, pr2.y};
+                const uint32_t q = pr.q_off & 0xFFFFu;
+                const uint32_t u = mod_magic((uint32_t)B.S[B.pi * 32 + L] + jrel, q, pr.magic);
+                const uint32_t wv = __ldg(B.bm + (pr.q_off >> 16) + (u >> 5));
+                if ((wv >> (u & 31)) & 1u) B.cur = kNone; else B.pi++;
+            }
+        }
+        if (B.cur != kNone && B.pi >= B.nB) {
+            b_emit(a, R, P, cur_range, g, jbase, B.cur);
+            B.cur = kNone;
+        }
+    }
+}
+
+template <bool STD>
 __global__ void __launch_bounds__(kSweepThreads)
 sweep_kernel(SweepArgs a) {
-    extern __shared__ uint16_t s_phase[];                 // [warps][kMaxLevelB][32]
+    extern __shared__ uint32_t s_mem[];
     const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lane_lt = (1u << lane) - 1u;
     const uint32_t warp_in_block = threadIdx.x >> 5;
-    uint16_t* S = s_phase + (size_t)warp_in_block * a.b_stride * 32;
+    // per warp: queue (kQCap u32) then phases (b_stride * 32 u16)
+    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + a.b_stride * 16);
+    uint16_t* S = reinterpret_cast<uint16_t*>(Qw + kQCap);
     const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
@@ -118,10 +195,8 @@ sweep_kernel(SweepArgs a) {
     const uint64_t total_units = a.hdr->total_units;
     uint32_t cur_range = 0;
     for (uint64_t u = gwarp; u < total_units; u += nwarps) {
-        // locate the range of unit u: units grow monotonically per warp, so a
-        // forward scan from the previous range suffices after one binary search
         if (u >= a.unit_prefix[cur_range + 1] || u < a.unit_prefix[cur_range]) {
-            uint32_t lo = 0, hi = n_ranges;                 // find last prefix <= u
+            uint32_t lo = 0, hi = n_ranges;                 // last prefix <= u
             while (hi - lo > 1) {
                 uint32_t mid = (lo + hi) >> 1;
                 if (a.unit_prefix[mid] <= u) lo = mid; else hi = mid;
@@ -140,15 +215,12 @@ sweep_kernel(SweepArgs a) {
 
         const uint32_t li = g * 32 + lane;
         const bool has_line = li < P.n_lines;
-        Line ln = has_line ? P.lines[li] : Line{0, 0, 0, 0};
-        const uint64_t r = ((uint64_t)ln.r_hi << 32) | ln.r_lo;
+        const Line ln = has_line ? P.lines[li] : Line{0, 0, 0, 0};
         const uint32_t c = ln.bc >> 16;
         const uint32_t jlo = (c < R.e0) ? 1u : 0u;
-        const uint32_t end = R.e0 + R.n_tiles;          // < 2^32 + 6 handled as u64 below
         const uint64_t endc = (uint64_t)R.e0 + R.n_tiles;
         const uint32_t jhi = has_line && endc > c ? (uint32_t)((endc - c + 5) / 6) : 0u;
-        (void)end;
-        const uint64_t jbase = (uint64_t)w0 * 64;
+        const uint32_t jbase = w0 * 64;
 
         // ---- level A windows at block jbase ----
         uint64_t A1w[kNumA1];
@@ -157,14 +229,16 @@ sweep_kernel(SweepArgs a) {
 #pragma unroll
         for (int i = 0; i < kNumA; i++) {
             const LevelA& la = P.A[i];
+            const uint32_t q = STD ? kStdQ[i] : la.q;
+            uint32_t ph = 0;
+            if (q > 1) ph = phase_fast(ln.r_lo, ln.r_hi, q, la.magic, la.c32, la.winv, jm[i], jbase);
             uint32_t e[8];
 #pragma unroll
             for (int m = 0; m < 8; m++) e[m] = la.ext[m];
-            uint32_t ph = (la.q > 1) ? phase_of(r, la.q, la.winv, jm[i], jbase) : 0u;
-            uint32_t aw = ph >> 5, b = ph & 31;
-            uint32_t wds[5];
+            const uint32_t aw = ph >> 5, b = ph & 31;
+            uint32_t wds[4];
 #pragma unroll
-            for (int m = 0; m < 5; m++)
+            for (int m = 0; m < 4; m++)
                 wds[m] = __funnelshift_r(sel8(e, aw + m), sel8(e, aw + m + 1), b);
             if (i < kNumA1) {
                 A1w[i] = ((uint64_t)wds[1] << 32) | wds[0];
@@ -176,26 +250,40 @@ sweep_kernel(SweepArgs a) {
                 for (int m = 0; m < 4; m++) A3w[i - kNumA1 - kNumA2][m] = wds[m];
             }
         }
-        // ---- level B phases at block jbase (lane-private shared column) ----
-        const uint32_t nB = P.nB;
-        for (uint32_t p = 0; p < nB; p++) {
+        // ---- level B phases at block jbase, one column per line ----
+        LevelB B;
+        B.Q = Qw;
+        B.S = S;
+        B.pb = P.packB;
+        B.bm = P.bitmapB;
+        B.nB = P.nB;
+        B.head = 0;
+        B.tail = 0;
+        B.cur = kNone;
+        B.pi = 0;
+        for (uint32_t p = 0; p < B.nB; p++) {
             const PrimeC pc = P.primesB[p];
-            S[p * 32 + lane] = (uint16_t)phase_of(r, pc.q, pc.winv, jm[kNumA + p], jbase);
+            S[p * 32 + lane] = (uint16_t)phase_fast(ln.r_lo, ln.r_hi, pc.q, pc.magic, pc.c32, pc.winv,
+                                                    jm[kNumA + p], jbase);
         }
+        __syncwarp();
 
         for (uint32_t w = w0; w < w1; w++) {
             uint64_t kill = 0;
 #pragma unroll
             for (int i = 0; i < kNumA1; i++) {
-                const uint32_t s = P.A[i].s, t = P.A[i].t;
-                uint64_t W = A1w[i];
+                if (STD && i >= 7) continue;                 // dummy slots of the standard set
+                const uint32_t q = STD ? kStdQ[i] : P.A[i].q;
+                const uint32_t s = STD ? (64u % q) : P.A[i].s;
+                const uint32_t t = STD ? (q - 64u % q) : P.A[i].t;
+                const uint64_t W = A1w[i];
                 kill |= W;
                 A1w[i] = (W >> s) | (W << t);
             }
 #pragma unroll
             for (int i = 0; i < kNumA2; i++) {
-                const uint32_t t = P.A[kNumA1 + i].t;
-                uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
+                const uint32_t t = STD ? (kStdQ[kNumA1 + i] - 64u) : P.A[kNumA1 + i].t;
+                const uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
                 kill |= ((uint64_t)o1 << 32) | o0;
                 A2w[i][0] = o2 | (o0 << t);
                 A2w[i][1] = __funnelshift_l(o0, o1, t);
@@ -203,8 +291,8 @@ sweep_kernel(SweepArgs a) {
             }
 #pragma unroll
             for (int i = 0; i < kNumA3; i++) {
-                const uint32_t t = P.A[kNumA1 + kNumA2 + i].t;
-                uint32_t o0 = A3w[i][0], o1 = A3w[i][1], o2 = A3w[i][2], o3 = A3w[i][3];
+                const uint32_t t = STD ? (kStdQ[kNumA1 + kNumA2 + i] - 96u) : P.A[kNumA1 + kNumA2 + i].t;
+                const uint32_t o0 = A3w[i][0], o1 = A3w[i][1], o2 = A3w[i][2], o3 = A3w[i][3];
                 kill |= ((uint64_t)o1 << 32) | o0;
                 A3w[i][0] = o2;
                 A3w[i][1] = o3 | (o0 << t);
@@ -215,35 +303,37 @@ sweep_kernel(SweepArgs a) {
             const uint32_t wb = w * 64;
             uint64_t valid = 0;
             if (jhi > wb && jlo < wb + 64) {
-                uint32_t lo = jlo > wb ? jlo - wb : 0;
-                uint32_t hi = jhi - wb < 64 ? jhi - wb : 64;
+                const uint32_t lo = jlo > wb ? jlo - wb : 0;
+                const uint32_t hi = jhi - wb < 64 ? jhi - wb : 64;
                 valid = (hi >= 64 ? ~0ull : ((1ull << hi) - 1)) & ~((1ull << lo) - 1);
             }
-            uint64_t surv = ~kill & valid;
-            while (surv) {
-                const uint32_t bit = __ffsll((long long)surv) - 1;
-                surv &= surv - 1;
-                const uint32_t j = wb + bit;
-                const uint32_t jrel = j - (uint32_t)jbase;
-                bool ok = true;
-                for (uint32_t p = 0; p < nB; p++) {
-                    const PrimeC pc = P.primesB[p];
-                    uint32_t uph = mod_magic((uint32_t)S[p * 32 + lane] + jrel, pc.q, pc.magic);
-                    uint32_t wv = __ldg(P.bitmapB + pc.off + (uph >> 5));
-                    if ((wv >> (uph & 31)) & 1u) { ok = false; break; }
+            uint64_t m = ~kill & valid;
+            // push this lane's survivors into the warp queue
+            for (;;) {
+                const bool has = m != 0;
+                const uint32_t bmask = __ballot_sync(0xFFFFFFFFu, has);
+                if (!bmask) break;
+                const uint32_t n = __popc(bmask);
+                if (n > (uint32_t)kQCap - (B.tail - B.head)) {
+                    __syncwarp();
+                    b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
+                    continue;
                 }
-                if (!ok) continue;
-                if (P.nC == 0) {
-                    emit_survivor(R, ln, j);
-                } else {
-                    uint32_t slot = atomicAdd(a.cq.count, 1u);
-                    if (slot < a.cq.cap) {
-                        uint4 e; e.x = li; e.y = j; e.z = cur_range; e.w = 0;
-                        a.cq.items[slot] = e;
-                    }
+                if (has) {
+                    const uint32_t rk = __popc(bmask & lane_lt);
+                    const uint32_t bit = __ffsll((long long)m) - 1;
+                    m &= m - 1;
+                    B.Q[(B.tail + rk) & (kQCap - 1)] = ((wb + bit - jbase) << 5) | lane;
                 }
+                B.tail += n;
             }
+            __syncwarp();
+            while (B.tail - B.head >= 32) b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
         }
+        // drain before the unit's phases are replaced
+        while (__any_sync(0xFFFFFFFFu, B.cur != kNone) || B.tail != B.head)
+            b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
+        __syncwarp();
     }
 }
 
@@ -317,32 +407,38 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
 }
 
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride) {
-    return (size_t)(block_threads / 32) * b_stride * 32 * sizeof(uint16_t);
+    return (size_t)(block_threads / 32) * (kQCap + (size_t)b_stride * 16) * sizeof(uint32_t);
 }
 
 static bool g_sweep_attr_set = false;
 
-// raise the dynamic shared-memory limit of the sweep kernel once (never
+// raise the dynamic shared-memory limit of the sweep kernels once (never
 // during stream capture: callers invoke this before capturing)
 static cudaError_t ensure_sweep_attr() {
     if (g_sweep_attr_set) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sweep_smem_bytes(kSweepThreads, kMaxLevelB));
+    const int lim = (int)sweep_smem_bytes(kSweepThreads, kMaxLevelB);
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     if (e == cudaSuccess) g_sweep_attr_set = true;
     return e;
 }
 
-int sweep_blocks_per_sm(uint32_t b_stride) {
+int sweep_blocks_per_sm(uint32_t b_stride, bool std_a) {
     int nb = 0;
     if (ensure_sweep_attr() != cudaSuccess) return 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel, kSweepThreads,
-                                                  sweep_smem_bytes(kSweepThreads, b_stride));
+    if (std_a)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<true>, kSweepThreads,
+                                                      sweep_smem_bytes(kSweepThreads, b_stride));
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<false>, kSweepThreads,
+                                                      sweep_smem_bytes(kSweepThreads, b_stride));
     return nb;
 }
 
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride, CQueue cq,
-                         uint32_t b_stride, uint32_t grid, cudaStream_t st) {
+                         uint32_t b_stride, uint32_t grid, bool std_a, cudaStream_t st) {
     size_t smem = sweep_smem_bytes(kSweepThreads, b_stride);
     cudaError_t e = ensure_sweep_attr();
     if (e != cudaSuccess) return e;
@@ -354,7 +450,8 @@ cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
     a.jmod_stride = stride;
     a.cq = cq;
     a.b_stride = b_stride;
-    sweep_kernel<<<grid, kSweepThreads, smem, st>>>(a);
+    if (std_a) sweep_kernel<true><<<grid, kSweepThreads, smem, st>>>(a);
+    else sweep_kernel<false><<<grid, kSweepThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -192,7 +192,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime) {
     memset(hp.A, 0, sizeof(hp.A));
     for (int i = 0; i < kNumA; i++) hp.A[i].q = 1;      // dummy: no kills
     int nA1 = 0, nA2 = 0, nA3 = 0;
-    hp.primesB.clear(); hp.primesC.clear(); hp.bitmapB.clear(); hp.listC.clear();
+    hp.primesB.clear(); hp.primesC.clear(); hp.bitmapB.clear(); hp.listC.clear(); hp.packB.clear();
     const uint64_t Wm = hp.W;
     for (auto& fp : hp.fprimes) {
         uint32_t q = fp.q;
@@ -208,6 +208,8 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime) {
             LevelA& a = hp.A[slot];
             a.q = q;
             a.winv = winv;
+            a.magic = 0xFFFFFFFFu / q;
+            a.c32 = (uint32_t)((1ull << 32) % q);
             if (slot < kNumA1) { a.s = 64 % q; a.t = q - a.s; }
             else if (slot < kNumA1 + kNumA2) { a.s = 0; a.t = q - 64; }
             else { a.s = 0; a.t = q - 96; }
@@ -222,19 +224,34 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime) {
         pc.winv = winv;
         pc.c32 = (uint32_t)((1ull << 32) % q);
         pc.magic64 = ~0ull / q;
-        if (q < split_prime && q < 65536 && hp.primesB.size() < (size_t)kMaxLevelB) {
+        if (q < split_prime && q < 65536 && hp.primesB.size() < (size_t)kMaxLevelB &&
+            hp.bitmapB.size() + (q + 31) / 32 < 65536) {
             pc.off = (uint32_t)hp.bitmapB.size();
             pc.cnt = (uint32_t)g.size();
             std::vector<uint32_t> bm((q + 31) / 32, 0);
             for (uint32_t u : g) bm[u >> 5] |= 1u << (u & 31);
             hp.bitmapB.insert(hp.bitmapB.end(), bm.begin(), bm.end());
             hp.primesB.push_back(pc);
+            PrimeB pb;
+            pb.magic = pc.magic;
+            pb.q_off = q | (pc.off << 16);
+            hp.packB.push_back(pb);
         } else {
             pc.off = (uint32_t)hp.listC.size();
             pc.cnt = (uint32_t)g.size();
             hp.listC.insert(hp.listC.end(), g.begin(), g.end());
             hp.primesC.push_back(pc);
         }
+    }
+    // the standard level-A set (every prime 37..127) has a kernel with
+    // compile-time shift amounts
+    {
+        static const uint32_t std_q[kNumA] = {37, 41, 43, 47, 53, 59, 61, 1, 1,
+                                              67, 71, 73, 79, 83, 89,
+                                              97, 101, 103, 107, 109, 113, 127};
+        hp.std_a = 1;
+        for (int i = 0; i < kNumA; i++)
+            if (hp.A[i].q != std_q[i]) hp.std_a = 0;
     }
     hp.range_primes.clear();
     for (int i = 0; i < kNumA; i++) hp.range_primes.push_back(hp.A[i].q);
