@@ -132,6 +132,7 @@ _SIGS = {
     "ccs_last_error": (C.c_char_p, []),
     "ccs_abi_version": (C.c_int, []),
     "ccs_filter_range": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
+    "ccs_filter_range_noalloc": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
     "ccs_prove": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64),
                             C.POINTER(_u64), _vp]),
     "ccs_search_range_host": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp,
@@ -354,6 +355,22 @@ class Engine:
         if st == OVERFLOW:
             raise CCSError(st, f"{n.value} survivors > cap {cap}")
         _check(st, "ccs_filter_range")
+        return out[: n.value]
+
+    def filter_range_noalloc(self, tile_start, n_tiles, out, stream=None):
+        """filter_range through the entry point that allocates no device
+        memory (ccs_filter_range_noalloc); out is a caller-owned int32 CUDA
+        tensor [cap, 4].  For callers that cannot allocate at call time
+        (inside stream capture, fixed-footprint embedders); calls that overlap
+        on one GPU race on its shared working array."""
+        lo, hi = _split128(tile_start)
+        n = _u64(0)
+        s = stream.cuda_stream if stream is not None else None
+        st = load_library().ccs_filter_range_noalloc(self.h, lo, hi, int(n_tiles), out.data_ptr(),
+                                                     out.shape[0], C.byref(n), s)
+        if st == OVERFLOW:
+            raise CCSError(st, f"{n.value} survivors > cap {out.shape[0]}")
+        _check(st, "ccs_filter_range_noalloc")
         return out[: n.value]
 
     def prove(self, survivors, tile_start, cap=1 << 16, out=None, stream=None):

@@ -618,6 +618,141 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
 }
 
 // ---------------------------------------------------------------------------
+// filter without allocation
+//
+// For callers that cannot allocate device memory at the point of the call:
+// code running inside a CUDA stream capture or a host callback (where
+// cudaMalloc is not allowed), allocators that forbid growth after start-up,
+// and embedders that pre-size their GPU footprint.  The engine's tables were
+// allocated by ccs_create; this entry point uses only a fixed scratch area
+// that lives in the library image itself.
+// ---------------------------------------------------------------------------
+
+// Scratch layout (bytes):
+//   [0, 1024)            range descriptor, unit prefix, sweep header, counters
+//   [1024, +64 KiB)      per-range residues J0 mod q (kNoAllocMaxPrimes x u32)
+//   [.., +4 MiB)         deferred-stage queue (kNoAllocQueue x 16 B)
+constexpr uint32_t kNoAllocMaxPrimes = 16384;
+constexpr uint32_t kNoAllocQueue = 1u << 18;
+constexpr size_t kNoAllocJmodOff = 1024;
+constexpr size_t kNoAllocQueueOff = kNoAllocJmodOff + 4ull * kNoAllocMaxPrimes;
+constexpr size_t kNoAllocBytes = kNoAllocQueueOff + 16ull * kNoAllocQueue;   // 4,260,864 B
+
+// One copy per device that loads the library, held until process exit.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on `device` (which must be current).
+// Resolved once per device; the host-side name of the array is not a device
+// address and is never passed to a kernel.
+ccs_status noalloc_scratch(int device, unsigned char** out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return fail(CCS_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = (unsigned char*)p;
+    }
+    *out = g_noalloc_ptr[device];
+    return CCS_OK;
+}
+}  // namespace
+
+ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint64_t n_tiles,
+                                    ccs_survivor* out_dev, uint64_t cap, uint64_t* n_out, void* stream) {
+    if (!E || !n_out) return fail(CCS_ERR_INVALID, "null argument");
+    if (cap && !out_dev) return fail(CCS_ERR_INVALID, "out_dev is null");
+    if (n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
+    const HostProfile& hp = E->hp;
+    const uint32_t np = (uint32_t)hp.range_primes.size();
+    if (np > kNoAllocMaxPrimes)
+        return fail(CCS_ERR_INVALID, "ccs_filter_range_noalloc supports at most " +
+                                         std::to_string(kNoAllocMaxPrimes - kNumA) +
+                                         " filter primes per engine (this engine has " +
+                                         std::to_string(np - kNumA) + ")");
+    unsigned __int128 ts = mk128(ts_lo, ts_hi);
+    if (ts + n_tiles < ts) return fail(CCS_ERR_INVALID, "tile range wraps 2^128");
+    CU(cudaSetDevice(E->device));
+    unsigned char* base = nullptr;
+    {
+        ccs_status s = noalloc_scratch(E->device, &base);
+        if (s != CCS_OK) return s;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : E->own_stream;
+    RangeDev* d_range = (RangeDev*)(base + 0);
+    uint64_t* d_prefix = (uint64_t*)(base + 256);
+    SweepHeader* d_hdr = (SweepHeader*)(base + 512);
+    uint32_t* d_cnt = (uint32_t*)(base + 768);                 // [0] survivors, [1] queue
+    uint32_t* d_jmod = (uint32_t*)(base + kNoAllocJmodOff);
+    uint4* d_queue = (uint4*)(base + kNoAllocQueueOff);
+    // the array keeps the previous call's contents: zero the counters
+    CU(cudaMemsetAsync(d_cnt, 0, 8, st));
+    uint64_t max_tiles = n_tiles ? n_tiles : 1;
+    if (!hp.primesC.empty() && E->levelc_rate > 0) {
+        uint64_t cpt = 0;
+        for (uint32_t w : hp.wheel_total) cpt += w;
+        cpt = cpt / 6 + 1;
+        double tiles = (double)kNoAllocQueue / (4.0 * E->levelc_rate * (double)cpt);
+        if (tiles < 6) tiles = 6;
+        if (tiles < (double)max_tiles) max_tiles = (uint64_t)tiles / 6 * 6;
+    }
+    for (uint64_t off = 0; off < n_tiles; off += max_tiles) {
+        const uint64_t nt = std::min<uint64_t>(max_tiles, n_tiles - off);
+        const unsigned __int128 cts = ts + off;
+        RangeDev hr;
+        memset(&hr, 0, sizeof(hr));
+        fill_J0(hr.J0, cts / 6);
+        hr.e0 = (uint32_t)(cts % 6);
+        hr.n_tiles = (uint32_t)nt;
+        hr.n_words = words_for(hr.e0, nt);
+        hr.unit_words = choose_unit_words(E, hr.n_words);
+        hr.profile = (uint32_t)E->slot;
+        hr.n_range_primes = np;
+        hr.surv_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
+        hr.surv_count = d_cnt;
+        hr.surv = (uint32_t*)out_dev;
+        hr.tile_bias = (uint32_t)off;
+        const uint64_t units = units_of(E, hr.n_words, hr.unit_words);
+        uint64_t hpre[2] = {0, units};
+        SweepHeader hh;
+        memset(&hh, 0, sizeof(hh));
+        hh.n_ranges = 1;
+        hh.total_units = units;
+        CU(cudaMemcpyAsync(d_range, &hr, sizeof(hr), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_prefix, hpre, sizeof(hpre), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_hdr, &hh, sizeof(hh), cudaMemcpyHostToDevice, st));
+        CU(cudaMemsetAsync(d_cnt + 1, 0, 4, st));
+        CU(launch_range_setup(d_range, d_hdr, 1, E->range_primes.p, np, d_jmod, np, st));
+        CQueue cq{d_cnt + 1, kNoAllocQueue, d_queue};
+        uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
+        const uint64_t need = (units + (kSweepThreads / 32) - 1) / (kSweepThreads / 32);
+        if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
+        CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, cq, b_stride_of((uint32_t)hp.primesB.size()),
+                        grid, hp.std_a != 0, st));
+        E->launches += 2;
+        if (!hp.primesC.empty()) {
+            CU(launch_levelc(d_range, d_jmod, np, cq, (uint32_t)E->sms * 8, st));
+            E->launches += 1;
+            uint32_t qn = 0;
+            CU(cudaMemcpyAsync(&qn, d_cnt + 1, 4, cudaMemcpyDeviceToHost, st));
+            CU(cudaStreamSynchronize(st));
+            if (qn > kNoAllocQueue)
+                return fail(CCS_OVERFLOW, "deferred-stage queue of the no-allocation path overflowed");
+        }
+    }
+    uint32_t cnt = 0;
+    CU(cudaMemcpyAsync(&cnt, d_cnt, 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    *n_out = cnt;
+    if (cnt > cap) return fail(CCS_OVERFLOW, "survivor capacity exceeded");
+    return CCS_OK;
+}
+
+// ---------------------------------------------------------------------------
 // batched executor
 // ---------------------------------------------------------------------------
 ccs_status ccs_batch_destroy(ccs_batch* b) {

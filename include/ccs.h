@@ -161,6 +161,23 @@ ccs_status ccs_filter_range(ccs_engine* eng, uint64_t tile_start_lo, uint64_t ti
                             uint64_t n_tiles, ccs_survivor* out_dev, uint64_t cap,
                             uint64_t* n_out, void* stream);
 
+/* ccs_filter_range without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory when they
+ * filter: code inside a CUDA stream capture or a host callback, where
+ * cudaMalloc is not allowed, and embedders that must fix their GPU footprint
+ * at start-up.  The working memory is a 4,260,864-byte array compiled into
+ * the library; every GPU that loads the library holds one copy until the
+ * process exits.  Limit: engines with at most 16362 filter primes (larger
+ * ones return CCS_ERR_INVALID); any n_tiles < 2^32.  The first call on a
+ * device looks up the array's device address, so make that first call
+ * before any stream capture.  Every call on a device shares the one array:
+ * calls that overlap on the GPU (other streams, other threads, other
+ * engines on the same device) race and must be serialised by the caller.
+ * Results equal ccs_filter_range's. */
+ccs_status ccs_filter_range_noalloc(ccs_engine* eng, uint64_t tile_start_lo, uint64_t tile_start_hi,
+                                    uint64_t n_tiles, ccs_survivor* out_dev, uint64_t cap,
+                                    uint64_t* n_out, void* stream);
+
 /* Prove survivors (device array) of the range that started at tile_start.
  * Replaces cc18_prove_kernel (v13:1462-1538) and prove_survivors_mt
  * (v13:1967-2068), per params.prove_mode / params.primality.
