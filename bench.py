@@ -151,6 +151,200 @@ def run_reference(args):
     return 0
 
 
+def _gmp_walk_worker(hexes):
+    """Reference GMP chain walk (v13:1870-1881 via oracle/_ref) on a list of
+    hex numbers; runs in a spawned process."""
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref33.so"))
+    lib.ref_gmp_forward_chain.argtypes = [ctypes.c_char_p]
+    return [lib.ref_gmp_forward_chain(h.encode()) for h in hexes]
+
+
+def gmp_walk_baseline(roots, seconds_goal=10.0):
+    """Proofs/s of the reference GMP prover walk on all host cores over a
+    bounded sample of the prove-batch roots."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref33.so")):
+        return None
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    hexes = [format(int(n), "x") for n in roots]
+    # calibrate on one core
+    t0 = time.time()
+    _gmp_walk_worker(hexes[:200])
+    per = (time.time() - t0) / 200
+    n = int(min(len(hexes), max(cores * 200, seconds_goal * cores / max(per, 1e-7))))
+    chunks = [hexes[i::cores] for i in range(cores)]
+    chunks = [c[: n // cores + 1] for c in chunks]
+    with ctx.Pool(cores) as pool:
+        t0 = time.time()
+        res = pool.map(_gmp_walk_worker, chunks)
+        dt = time.time() - t0
+    done = sum(len(c) for c in chunks)
+    return {"value": done / dt, "unit": "roots/s", "cores": cores, "kind": "reference",
+            "sample": f"{done} prove-batch roots walked with GMP mpz_probab_prime_p(.,1) "
+                      f"(the reference CPU prover's walk, v13:1870-1881) in {dt:.1f} s",
+            "lengths": [x for r in res for x in r][:0]}
+
+
+def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
+    """Prove batch: 2^24 roots of 80..110 bits pre-filtered by every prime
+    < 2^17 at chain positions 0..15 (survivors of the cc16 filter at seeded
+    widths), walked p -> 2p+1 until the first composite (BPSW)."""
+    import random
+    r = random.Random(SEED + 3)
+    info = eng.info
+    bases = eng.bases()
+    M, WP = info["lattice_m"], info["wheel_period"]
+    roots = []
+    t_gen = time.time()
+    out = torch.empty((1 << 20, 4), dtype=torch.int32, device=dev)
+    while len(roots) < n_unique:
+        bits = r.randint(80, 110)
+        t0, t1 = ccs.bit_tile_range(bits, bases, M, WP)
+        ts = r.randint(t0, t1 - (1 << 22) - 1)
+        surv = eng.filter_range(ts, 1 << 22, out=out).cpu().numpy().astype("int64") & 0xFFFFFFFF
+        for b, k, t, _ in surv:
+            n = ((ts + int(t)) * WP + int(k)) * M + bases[int(b)]
+            if n.bit_length() == bits:
+                roots.append(n)
+    roots = roots[:n_unique]
+    t_gen = time.time() - t_gen
+    import numpy as np
+    arr = np.zeros((n_unique, 4), dtype=np.uint32)
+    for i, v in enumerate(roots):
+        for w in range(4):
+            arr[i, w] = (v >> (32 * w)) & 0xFFFFFFFF
+    uniq = torch.from_numpy(arr.view(np.int32)).to(dev)
+    nums = uniq.repeat(copies, 1).contiguous()
+    total = nums.shape[0]
+    lengths = torch.zeros(total, dtype=torch.int32, device=dev)
+    eng.walk_numbers_dev(nums[: 1 << 16], 4, lengths[: 1 << 16])       # warm-up
+    torch.cuda.synchronize()
+    eng.walk_modmuls(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    eng.walk_numbers_dev(nums, 4, lengths)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    mm = eng.walk_modmuls(reset=True)
+    L = lengths[:n_unique].cpu().numpy()
+    tests = int(((L + 1).clip(max=64)).sum()) * copies           # numbers tested
+    primes = int(L.sum()) * copies
+    imad = ccs.measure_imad_peak(local)
+    # IMAD ops per Montgomery product: 2 NL^2 + NL lo/hi pairs, NL from the width
+    nl = np.array([3 if v.bit_length() <= 96 else 4 for v in roots], dtype=np.float64)
+    ops_per_mm = float((2 * (2 * nl * nl + nl)).mean())
+    achieved = mm * ops_per_mm / (ms * 1e-3) / 1e12
+    cpu = gmp_walk_baseline(roots[:20000])
+    return {"workload": f"{total} roots (= {copies} x {n_unique} distinct), 80..110-bit, pre-filtered "
+                        "by all primes < 2^17 at positions 0..15, BPSW walk",
+            "roots_per_s": total / (ms * 1e-3), "primality_tests_per_s": tests / (ms * 1e-3),
+            "prime_verdicts_per_s": primes / (ms * 1e-3), "modmuls_per_s": mm / (ms * 1e-3),
+            "ms": ms, "mean_chain_len": float(L.mean()), "max_chain_len": int(L.max()),
+            "root_generation_s": t_gen,
+            "roofline": {"bound": "imad", "achieved": achieved, "peak": imad, "unit": "TOPS",
+                         "frac": achieved / imad,
+                         "work": f"{ops_per_mm:.1f} IMAD ops per Montgomery product (2 x (2NL^2+NL))",
+                         "peak_source": "measured: ccs_measure_imad_peak"},
+            "cpu_baseline": cpu}
+
+
+def section_batched(ccs, engines, n_ranges=4096):
+    """Uneven ranges: one batched graph replay versus per-range plain calls."""
+    ranges = ccs.mixed_ranges(engines, n_ranges, SEED + 11)
+    batch = ccs.Batch(engines, n_ranges, surv_cap=1 << 22, chain_cap=1 << 20)
+    batch.run(ranges[:32], want_records=False)
+    t0 = time.time()
+    res, surv, ch = batch.run(ranges)
+    tb = time.time() - t0
+    dev_ms = batch.last_ms()
+    cand = sum(x["candidates"] for x in res)
+    nsurv = sum(x["n_survivors"] for x in res)
+    nprimes = sum(x["n_primes"] for x in res)
+    batch.close()
+    t0 = time.time()
+    psurv = pprimes = 0
+    for ts, nt, p, bits in ranges:
+        e = engines[p]
+        s = e.filter_range(ts, nt, cap=1 << 20)
+        c, pr = e.prove(s, ts)
+        psurv += s.shape[0]
+        pprimes += pr
+    tp = time.time() - t0
+    return {"workload": f"{n_ranges} ranges, log-uniform 2^20..2^34 candidates, depth 14..19, "
+                        "width 64..110 bits",
+            "candidates": cand, "batched_candidates_per_s": cand / tb,
+            "batched_device_ms": dev_ms, "plain_candidates_per_s": cand / tp,
+            "speedup": tp / tb, "survivors": nsurv, "plain_survivors": psurv,
+            "primes": nprimes, "plain_primes": pprimes,
+            "batched_proofs_per_s": nprimes / tb, "plain_proofs_per_s": pprimes / tp}
+
+
+def section_served(ccs, engines, n_req=2048, lam=2000.0):
+    """Poisson arrivals of uneven range requests: continuous-batching server
+    versus a plain first-come-first-served loop; p50/p99 request latency."""
+    import random
+    import numpy as np
+    ranges = ccs.mixed_ranges(engines, n_req, SEED + 23)
+    rr = random.Random(SEED + 29)
+    arr = []
+    t = 0.0
+    for _ in range(n_req):
+        t += rr.expovariate(lam)
+        arr.append(t)
+    cand_total = 0
+
+    # served
+    srv = ccs.Server(engines, max_active=256, chunk_tiles=1 << 19, mem_cap_bytes=120 << 30)
+    ids = [None] * n_req
+    base = time.monotonic() + 0.05
+
+    def submitter():
+        for i, (ts, nt, p, bits) in enumerate(ranges):
+            d = base + arr[i] - time.monotonic()
+            if d > 0:
+                time.sleep(d)
+            ids[i] = srv.submit(ts, nt, p, bits)
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    lat = []
+    first, last = 1e30, 0
+    for rid in ids:
+        srv.wait(rid)
+        st, res, _, _ = srv.poll(rid, surv_cap=1 << 16, chain_cap=1 << 12)
+        lat.append(res["done_s"] - res["submit_s"])
+        first = min(first, res["submit_s"])
+        last = max(last, res["done_s"])
+        cand_total += res["candidates"]
+    stats = srv.stats()
+    srv.close()
+    served = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+              "candidates_per_s": cand_total / (last - first), "makespan_s": last - first,
+              "ticks": stats["ticks"]}
+
+    # plain: one request at a time in arrival order
+    lat_p = []
+    base = time.monotonic() + 0.05
+    t_first = base + arr[0]
+    for i, (ts, nt, p, bits) in enumerate(ranges):
+        d = base + arr[i] - time.monotonic()
+        if d > 0:
+            time.sleep(d)
+        e = engines[p]
+        s = e.filter_range(ts, nt, cap=1 << 20)
+        e.prove(s, ts)
+        lat_p.append(time.monotonic() - (base + arr[i]))
+    t_last = time.monotonic()
+    plain = {"p50_s": float(np.percentile(lat_p, 50)), "p99_s": float(np.percentile(lat_p, 99)),
+             "candidates_per_s": cand_total / (t_last - t_first), "makespan_s": t_last - t_first}
+    return {"workload": f"{n_req} requests, Poisson arrivals {lam:.0f}/s, log-uniform 2^20..2^34 "
+                        "candidates, depth 14..19, width 64..110 bits, admission cap 120 GB",
+            "offered_candidates_per_s": cand_total / arr[-1], "served": served, "plain": plain}
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     import torch
@@ -264,6 +458,23 @@ def run_ours(args):
                               f"--target 16 --threads {s['cores']}: {s['candidates']} candidates in "
                               f"{s['seconds']:.1f} s (reference stage primes 37..863 on the same "
                               f"W=31# depth-16 lattice)")}
+    extra = {}
+    if rank == 0 and not args.headline_only:
+        try:
+            extra["prove"] = section_prove(ccs, torch, eng, dev, local)
+        except Exception as ex:                       # report, keep the headline
+            extra["prove"] = {"error": repr(ex)}
+        depth_engines = [ccs.Engine(device=local, **ccs.config_depth_profile(d)) for d in range(14, 20)]
+        try:
+            extra["batched"] = section_batched(ccs, depth_engines, args.batch_ranges)
+        except Exception as ex:
+            extra["batched"] = {"error": repr(ex)}
+        try:
+            extra["served"] = section_served(ccs, depth_engines, args.served_requests)
+        except Exception as ex:
+            extra["served"] = {"error": repr(ex)}
+        for e in depth_engines:
+            e.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "candidates/s", "n_gpus": ws,
@@ -289,6 +500,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "wall_s_timed": t_wall,
         }
+        line.update(extra)
         print(json.dumps(line))
     if pg:
         pg.barrier()
@@ -307,6 +519,10 @@ def main():
     ap.add_argument("--tiles-per-step", type=int, default=TILES_PER_STEP,
                     help="tiles per step (smaller values: profiling cases)")
     ap.add_argument("--unit-words", type=int, default=0, help="sweep work-unit length (0: tuned)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the prove-batch, batched and served sections")
+    ap.add_argument("--batch-ranges", type=int, default=4096)
+    ap.add_argument("--served-requests", type=int, default=2048)
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3")

@@ -115,6 +115,17 @@ class _RangeResult(C.Structure):
                 ("chain_offset", C.c_uint64), ("status", C.c_uint32), ("_pad", C.c_uint32)]
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("max_active", C.c_uint32), ("chunk_tiles", C.c_uint32), ("mem_cap_bytes", C.c_uint64),
+                ("max_pending", C.c_uint32), ("_pad", C.c_uint32)]
+
+
+class _RequestResult(C.Structure):
+    _fields_ = [("n_survivors", C.c_uint64), ("n_chains", C.c_uint64), ("n_primes", C.c_uint64),
+                ("candidates", C.c_uint64), ("submit_s", C.c_double), ("admit_s", C.c_double),
+                ("done_s", C.c_double), ("status", C.c_uint32), ("ticks", C.c_uint32)]
+
+
 class _Tuning(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("unit_words", C.c_uint32), ("split_prime", C.c_uint32)]
@@ -145,7 +156,16 @@ _SIGS = {
                                 _vp, _vp, _vp]),
     "ccs_batch_last_ms": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "ccs_get_tuning": (C.c_int, [_vp, C.POINTER(_Tuning)]),
+    "ccs_server_create": (C.c_int, [C.POINTER(_vp), C.c_uint32, C.POINTER(_ServerConfig), C.POINTER(_vp)]),
+    "ccs_server_destroy": (C.c_int, [_vp]),
+    "ccs_submit": (C.c_int, [_vp, C.POINTER(_Range), C.POINTER(_u64)]),
+    "ccs_poll": (C.c_int, [_vp, _u64, C.POINTER(_RequestResult), _vp, _u64, _vp, _u64]),
+    "ccs_wait": (C.c_int, [_vp, _u64, C.c_uint32]),
+    "ccs_cancel": (C.c_int, [_vp, _u64]),
+    "ccs_server_stats": (C.c_int, [_vp, C.POINTER(_u64)]),
     "ccs_measure_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "ccs_measure_imad_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "ccs_walk_modmuls": (C.c_int, [_vp, C.POINTER(_u64), C.c_int]),
     "ccs_set_tuning": (C.c_int, [_vp, C.POINTER(_Tuning)]),
 }
 
@@ -408,6 +428,12 @@ class Engine:
                                                out.data_ptr(), None), "ccs_walk_numbers")
         return out.cpu().numpy().astype(np.int64)
 
+    def walk_modmuls(self, reset=True):
+        """Montgomery products spent by walk launches since the last reset."""
+        v = _u64(0)
+        _check(load_library().ccs_walk_modmuls(self.h, C.byref(v), 1 if reset else 0))
+        return v.value
+
     def walk_numbers_dev(self, numbers_dev, limbs, lengths_dev):
         _check(load_library().ccs_walk_numbers(self.h, numbers_dev.data_ptr(), numbers_dev.shape[0],
                                                limbs, lengths_dev.data_ptr(), None))
@@ -547,8 +573,105 @@ def lane_range(tile_min, tile_max, lanes, lane_id):
     return start, end
 
 
+def measure_imad_peak(device=0):
+    """Measured 32-bit multiply-add issue rate in tera-ops/s."""
+    t = C.c_double(0)
+    _check(load_library().ccs_measure_imad_peak(device, C.byref(t)), "ccs_measure_imad_peak")
+    return t.value
+
+
 def measure_int32_peak(device=0):
     """Measured INT32 ALU issue rate in tera-ops/s (ccs_measure_int32_peak)."""
     t = C.c_double(0)
     _check(load_library().ccs_measure_int32_peak(device, C.byref(t)), "ccs_measure_int32_peak")
     return t.value
+
+
+class Server:
+    """Continuous-batching request server (ccs_server_*): submit ranges at any
+    time; admitted requests share every scheduling tick on the GPU."""
+
+    def __init__(self, engines, max_active=256, chunk_tiles=1 << 20, mem_cap_bytes=120 << 30,
+                 max_pending=1 << 20):
+        lib = load_library()
+        arr = (_vp * len(engines))(*[e.h for e in engines])
+        cfg = _ServerConfig(max_active, chunk_tiles, mem_cap_bytes, max_pending, 0)
+        h = _vp()
+        _check(lib.ccs_server_create(arr, len(engines), C.byref(cfg), C.byref(h)), "ccs_server_create")
+        self.h = h
+        self.engines = engines
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().ccs_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, tile_start, n_tiles, profile=0, bits=None):
+        lo, hi = _split128(tile_start)
+        rg = _Range(lo, hi, int(n_tiles), profile, bits or self.engines[profile].bits)
+        rid = _u64(0)
+        _check(load_library().ccs_submit(self.h, C.byref(rg), C.byref(rid)), "ccs_submit")
+        return rid.value
+
+    def wait(self, rid, timeout_ms=600000):
+        st = load_library().ccs_wait(self.h, rid, timeout_ms)
+        _check(st, "ccs_wait")
+
+    def poll(self, rid, surv_cap=1 << 20, chain_cap=1 << 16):
+        """None while running, else (status, result dict, survivors, chains)."""
+        res = _RequestResult()
+        surv = np.zeros(surv_cap, dtype=SURVIVOR_DTYPE)
+        ch = np.zeros(chain_cap, dtype=CHAIN_DTYPE)
+        st = load_library().ccs_poll(self.h, rid, C.byref(res), surv.ctypes.data, surv_cap,
+                                     ch.ctypes.data, chain_cap)
+        if st == PENDING:
+            return None
+        if st not in (OK, OVERFLOW, ERR_CANCELLED):
+            _check(st, "ccs_poll")
+        r = {f: getattr(res, f) for f, _ in _RequestResult._fields_}
+        return st, r, surv[: min(r["n_survivors"], surv_cap)], ch[: min(r["n_chains"], chain_cap)]
+
+    def cancel(self, rid):
+        _check(load_library().ccs_cancel(self.h, rid), "ccs_cancel")
+
+    def stats(self):
+        out = (_u64 * 6)()
+        _check(load_library().ccs_server_stats(self.h, out))
+        return dict(zip(["submitted", "admitted", "completed", "cancelled", "ticks", "pending"],
+                        [int(x) for x in out]))
+
+
+def config_depth_profile(depth):
+    """One profile of the mixed-depth workloads: W = 31#, the given depth,
+    stage primes 37..2^10 / 2^10..2^14 / 2^14..2^17 at positions [0, depth)."""
+    return dict(target=depth, depth=depth, bits=89,
+                stages=[(primes_in(37, 1 << 10), 0), (primes_in(1 << 10, 1 << 14), 0),
+                        (primes_in(1 << 14, 1 << 17), 0)])
+
+
+def mixed_ranges(engines, n, seed, min_log2=20, max_log2=34, width_lo=64, width_hi=110):
+    """Seeded uneven ranges: length log-uniform in [2^min_log2, 2^max_log2]
+    candidates, profile (depth) uniform over engines, root width uniform in
+    [width_lo, width_hi], start drawn inside that width's tile range.
+    Returns [(tile_start, n_tiles, profile, bits)]."""
+    import random
+    r = random.Random(seed)
+    info = [(e.info["candidates_per_tile"], e.bases(), e.info["lattice_m"], e.info["wheel_period"])
+            for e in engines]
+    out = []
+    for _ in range(n):
+        p = r.randrange(len(engines))
+        cpt, bases, M, WP = info[p]
+        cands = 2.0 ** r.uniform(min_log2, max_log2)
+        nt = max(1, int(round(cands / cpt)))
+        bits = r.randint(width_lo, width_hi)
+        t0, t1 = bit_tile_range(bits, bases, M, WP)
+        ts = r.randint(t0, max(t0, t1 - nt - 1))
+        out.append((ts, nt, p, bits))
+    return out

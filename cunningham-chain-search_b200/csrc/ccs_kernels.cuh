@@ -91,5 +91,6 @@ cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_walk(const uint32_t* numbers, uint64_t n, uint32_t limbs, uint32_t* lengths,
                         int profile, cudaStream_t st);
 int sweep_blocks_per_sm(uint32_t b_stride, bool std_a);
+cudaError_t modmul_count(uint64_t* out, bool reset);
 
 }  // namespace ccs

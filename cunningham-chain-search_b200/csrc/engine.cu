@@ -617,6 +617,13 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
     return CCS_OK;
 }
 
+ccs_status ccs_walk_modmuls(ccs_engine* E, uint64_t* count, int reset) {
+    if (!E || !count) return fail(CCS_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(E->device));
+    CU(modmul_count(count, reset != 0));
+    return CCS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // filter without allocation
 //

@@ -19,6 +19,9 @@ namespace ccs {
 
 __constant__ ProveConst c_prove[kMaxProfiles];
 
+// Montgomery products executed by walk launches (one atomic per number)
+__device__ unsigned long long g_modmul_count = 0;
+
 cudaError_t upload_prove_const(int slot, const ProveConst& pc, cudaStream_t st) {
     return cudaMemcpyToSymbolAsync(c_prove, &pc, sizeof(ProveConst), slot * sizeof(ProveConst),
                                    cudaMemcpyHostToDevice, st);
@@ -82,6 +85,7 @@ struct Mont {
     uint32_t ninv;        // -n^{-1} mod 2^32
     uint32_t one[NL];     // R mod n
     uint32_t mone[NL];    // n - (R mod n)  (Montgomery form of -1)
+    uint32_t count;       // Montgomery products executed with this context
 };
 
 template <int NL>
@@ -258,7 +262,7 @@ __device__ __forceinline__ void to_mont_small(uint32_t (&r)[NL], uint32_t a, con
 
 // strong probable-prime test to base a (n odd, n > a)
 template <int NL>
-__device__ bool strong_prp(const Mont<NL>& M, const Big& nb, uint32_t a) {
+__device__ bool strong_prp(Mont<NL>& M, const Big& nb, uint32_t a) {
     // n - 1 = d 2^s
     Big d = nb;
     d.w[0] -= 1;                              // n odd: no borrow
@@ -287,14 +291,16 @@ __device__ bool strong_prp(const Mont<NL>& M, const Big& nb, uint32_t a) {
     const int top = big_bits(d) - 1;
     for (int b = top - 1; b >= 0; b--) {
         montmul<NL>(x, x, x, M.n, M.ninv);
+        M.count++;
         if ((d.w[b >> 5] >> (b & 31)) & 1u) {
             if (a == 2) dblmod<NL>(x, x, M.n);
-            else montmul<NL>(x, x, am, M.n, M.ninv);
+            else { montmul<NL>(x, x, am, M.n, M.ninv); M.count++; }
         }
     }
     if (eq<NL>(x, M.one) || eq<NL>(x, M.mone)) return true;
     for (int r = 1; r < s; r++) {
         montmul<NL>(x, x, x, M.n, M.ninv);
+        M.count++;
         if (eq<NL>(x, M.mone)) return true;
         if (eq<NL>(x, M.one)) return false;
     }
@@ -334,7 +340,7 @@ __device__ int jacobi_small(int D, const Big& nb) {
 
 // strong Lucas probable-prime test, Selfridge method A (P = 1, Q = (1 - D)/4)
 template <int NL>
-__device__ bool strong_lucas(const Mont<NL>& M, const Big& nb) {
+__device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
     int D = 5;
     int tries = 0;
     for (;;) {
@@ -387,6 +393,7 @@ __device__ bool strong_lucas(const Mont<NL>& M, const Big& nb) {
         addmod<NL>(t2, Qk, Qk, M.n);
         submod<NL>(V, t1, t2, M.n);
         montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
+        M.count += 3;
         if ((d.w[b >> 5] >> (b & 31)) & 1u) {
             uint32_t nu[NL], nv[NL];
             addmod<NL>(nu, U, V, M.n);
@@ -397,6 +404,7 @@ __device__ bool strong_lucas(const Mont<NL>& M, const Big& nb) {
 #pragma unroll
             for (int i = 0; i < NL; i++) { U[i] = nu[i]; V[i] = nv[i]; }
             montmul<NL>(Qk, Qk, Qm, M.n, M.ninv);
+            M.count += 2;
         }
     }
     if (is_zero<NL>(U) || is_zero<NL>(V)) return true;
@@ -406,28 +414,33 @@ __device__ bool strong_lucas(const Mont<NL>& M, const Big& nb) {
         submod<NL>(V, t1, t2, M.n);
         if (is_zero<NL>(V)) return true;
         montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
+        M.count += 2;
     }
     return false;
 }
 
 template <int NL>
-__device__ bool prp_suite(const Big& nb, int nbits, uint32_t primality, const ProveConst& pc) {
+__device__ bool prp_suite(const Big& nb, int nbits, uint32_t primality, const ProveConst& pc,
+                          uint32_t& mm) {
     Mont<NL> M;
     mont_setup<NL>(M, nb, nbits);
+    M.count = 0;
+    bool r = true;
     if (primality == CCS_PRIME_BPSW) {
-        if (!strong_prp<NL>(M, nb, 2)) return false;
-        return strong_lucas<NL>(M, nb);
+        r = strong_prp<NL>(M, nb, 2) && strong_lucas<NL>(M, nb);
+    } else {
+        for (uint32_t i = 0; i < pc.n_wit && r; i++) r = strong_prp<NL>(M, nb, pc.wit[i]);
     }
-    for (uint32_t i = 0; i < pc.n_wit; i++)
-        if (!strong_prp<NL>(M, nb, pc.wit[i])) return false;
-    return true;
+    mm += M.count;
+    return r;
 }
 
 __constant__ uint32_t c_small_primes[27] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47,
                                             53, 59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 1093, 3511};
 
-// primality predicate of the profile for any n < 2^192
-__device__ bool is_prime_dev(const Big& nb, const ProveConst& pc) {
+// primality predicate of the profile for any n < 2^192; mm counts the
+// Montgomery products spent
+__device__ bool is_prime_dev(const Big& nb, const ProveConst& pc, uint32_t& mm) {
     const int nbits = big_bits(nb);
     if (nbits <= 1) return false;
     const uint32_t lo = nb.w[0];
@@ -456,22 +469,22 @@ __device__ bool is_prime_dev(const Big& nb, const ProveConst& pc) {
     }
     const int nl = (nbits + 31) >> 5;
     switch (nl <= 2 ? 2 : nl) {
-        case 2: return prp_suite<2>(nb, nbits, pc.primality, pc);
-        case 3: return prp_suite<3>(nb, nbits, pc.primality, pc);
-        case 4: return prp_suite<4>(nb, nbits, pc.primality, pc);
-        case 5: return prp_suite<5>(nb, nbits, pc.primality, pc);
-        default: return prp_suite<6>(nb, nbits, pc.primality, pc);
+        case 2: return prp_suite<2>(nb, nbits, pc.primality, pc, mm);
+        case 3: return prp_suite<3>(nb, nbits, pc.primality, pc, mm);
+        case 4: return prp_suite<4>(nb, nbits, pc.primality, pc, mm);
+        case 5: return prp_suite<5>(nb, nbits, pc.primality, pc, mm);
+        default: return prp_suite<6>(nb, nbits, pc.primality, pc, mm);
     }
 }
 
 // forward walk p -> 2p + 1 while prime, counting p (v13:1519-1528, 1873-1881)
-__device__ int walk_forward(Big cur, const ProveConst& pc) {
+__device__ int walk_forward(Big cur, const ProveConst& pc, uint32_t& mm) {
     int len = 1;
     while (len < kMaxChain) {
         if (big_bits(cur) >= 32 * kMaxLimbs) break;   // next member would exceed 192 bits
         Big nx = cur;
         big_shl1_inc(nx);
-        if (!is_prime_dev(nx, pc)) break;
+        if (!is_prime_dev(nx, pc, mm)) break;
         len++;
         cur = nx;
     }
@@ -531,13 +544,14 @@ prove_kernel(ProveArgs a) {
         bool comp = false;
         for (int t = 0; t < ntd && !comp; t++) comp = big_mod_small(nb, c_screen[t]) == 0;
         if (comp) continue;
-        if (!is_prime_dev(nb, pc)) continue;
+        uint32_t mm = 0;
+        if (!is_prime_dev(nb, pc, mm)) continue;
         if (R.prime_count) atomicAdd(R.prime_count, 1u);
         Big root = nb;
         bool is_root = true;
         Big pred = nb;
         big_pred(pred);
-        if (!big_lt_u32(pred, 2) && is_prime_dev(pred, pc)) {
+        if (!big_lt_u32(pred, 2) && is_prime_dev(pred, pc, mm)) {
             is_root = false;
             if (pc.prove_mode == CCS_PROVE_ROOTS) continue;              // v13:1513-1516
             root = pred;
@@ -545,11 +559,11 @@ prove_kernel(ProveArgs a) {
                 Big p2 = root;
                 big_pred(p2);
                 if (big_lt_u32(p2, 2)) break;
-                if (!is_prime_dev(p2, pc)) break;
+                if (!is_prime_dev(p2, pc, mm)) break;
                 root = p2;
             }
         }
-        const int len = walk_forward(root, pc);
+        const int len = walk_forward(root, pc, mm);
         if (R.chain_count) atomicAdd(R.chain_count, 1u);
         const uint32_t slot = atomicAdd(a.chain_count, 1u);
         if (slot < a.chain_cap) {
@@ -576,8 +590,22 @@ walk_kernel(const uint32_t* __restrict__ numbers, uint64_t n, uint32_t limbs,
         Big x;
 #pragma unroll
         for (int w = 0; w < kMaxLimbs; w++) x.w[w] = (w < (int)limbs) ? numbers[i * limbs + w] : 0u;
-        lengths[i] = is_prime_dev(x, pc) ? (uint32_t)walk_forward(x, pc) : 0u;
+        uint32_t mm = 0;
+        lengths[i] = is_prime_dev(x, pc, mm) ? (uint32_t)walk_forward(x, pc, mm) : 0u;
+        atomicAdd(&g_modmul_count, (unsigned long long)mm);
     }
+}
+
+cudaError_t modmul_count(uint64_t* out, bool reset) {
+    unsigned long long v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_modmul_count, sizeof(v));
+    if (e != cudaSuccess) return e;
+    *out = v;
+    if (reset) {
+        v = 0;
+        e = cudaMemcpyToSymbol(g_modmul_count, &v, sizeof(v));
+    }
+    return e;
 }
 
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st) {

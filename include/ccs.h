@@ -240,6 +240,46 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
 /* device-side timing of the last ccs_batch_run: filter+prove milliseconds */
 ccs_status ccs_batch_last_ms(const ccs_batch* b, float* ms);
 
+/* ---- served path ------------------------------------------------------------ */
+
+/* A request server with continuous batching: requests (lattice ranges) are
+ * admitted as slots and memory free up; every scheduling tick runs one chunk
+ * of every admitted request together in one batched graph replay, so new
+ * arrivals overlap with long-running requests on the device.  Results are
+ * identical to a plain ccs_filter_range + ccs_prove of the whole range. */
+typedef struct ccs_server ccs_server;
+
+typedef struct {
+    uint32_t max_active;      /* admitted requests per tick (batch slots) */
+    uint32_t chunk_tiles;     /* tiles of one request per tick */
+    uint64_t mem_cap_bytes;   /* admission budget for result buffers */
+    uint32_t max_pending;     /* submitted-but-not-admitted queue bound */
+    uint32_t _pad;
+} ccs_server_config;
+
+typedef struct {
+    uint64_t n_survivors, n_chains, n_primes, candidates;
+    double submit_s, admit_s, done_s;   /* monotonic seconds */
+    uint32_t status;                    /* CCS_OK / CCS_PENDING / CCS_ERR_CANCELLED / CCS_OVERFLOW */
+    uint32_t ticks;                     /* scheduling ticks the request took part in */
+} ccs_request_result;
+
+ccs_status ccs_server_create(ccs_engine* const* profiles, uint32_t n_profiles,
+                             const ccs_server_config* cfg, ccs_server** out);
+ccs_status ccs_server_destroy(ccs_server* s);
+/* queue a range; CCS_ERR_BUSY when the pending queue is full */
+ccs_status ccs_submit(ccs_server* s, const ccs_range* range, uint64_t* id);
+/* CCS_PENDING while running; otherwise fills res and copies up to the given
+ * capacities of survivors / chains (tile_idx relative to the range start)
+ * and forgets the request */
+ccs_status ccs_poll(ccs_server* s, uint64_t id, ccs_request_result* res, ccs_survivor* surv_host,
+                    uint64_t surv_cap, ccs_chain* chains_host, uint64_t chain_cap);
+/* block until the request is done (or timeout_ms passes: CCS_ERR_TIMEOUT) */
+ccs_status ccs_wait(ccs_server* s, uint64_t id, uint32_t timeout_ms);
+ccs_status ccs_cancel(ccs_server* s, uint64_t id);
+/* counters: [0] submitted [1] admitted [2] completed [3] cancelled [4] ticks [5] pending now */
+ccs_status ccs_server_stats(ccs_server* s, uint64_t* out6);
+
 /* ---- tuning -------------------------------------------------------------- */
 
 typedef struct {
@@ -258,6 +298,14 @@ ccs_status ccs_set_tuning(ccs_engine* eng, const ccs_tuning* t);
  * IADD3/LOP3 chains per thread, all SMs.  The roofline denominator of the
  * integer filter kernels. */
 ccs_status ccs_measure_int32_peak(int device, double* tops);
+
+/* Measured 32-bit multiply-add issue rate (IMAD / IMAD.HI chains), tera
+ * ops/s: the roofline denominator of the Montgomery prover. */
+ccs_status ccs_measure_imad_peak(int device, double* tops);
+
+/* Montgomery products executed by ccs_walk_numbers launches on this device
+ * since the last reset (reset != 0 clears after reading). */
+ccs_status ccs_walk_modmuls(ccs_engine* eng, uint64_t* count, int reset);
 
 #ifdef __cplusplus
 }
