@@ -174,6 +174,8 @@ def gmp_walk_baseline(roots, seconds_goal=10.0):
     _gmp_walk_worker(hexes[:200])
     per = (time.time() - t0) / 200
     n = int(min(len(hexes), max(cores * 200, seconds_goal * cores / max(per, 1e-7))))
+    if n > len(hexes):
+        n = len(hexes)
     chunks = [hexes[i::cores] for i in range(cores)]
     chunks = [c[: n // cores + 1] for c in chunks]
     with ctx.Pool(cores) as pool:
@@ -183,8 +185,7 @@ def gmp_walk_baseline(roots, seconds_goal=10.0):
     done = sum(len(c) for c in chunks)
     return {"value": done / dt, "unit": "roots/s", "cores": cores, "kind": "reference",
             "sample": f"{done} prove-batch roots walked with GMP mpz_probab_prime_p(.,1) "
-                      f"(the reference CPU prover's walk, v13:1870-1881) in {dt:.1f} s",
-            "lengths": [x for r in res for x in r][:0]}
+                      f"(the reference CPU prover's walk, v13:1870-1881) in {dt:.1f} s"}
 
 
 def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
@@ -268,6 +269,7 @@ def section_batched(ccs, engines, n_ranges=4096):
     psurv = pprimes = 0
     for ts, nt, p, bits in ranges:
         e = engines[p]
+        e.set_bits(bits)
         s = e.filter_range(ts, nt, cap=1 << 20)
         c, pr = e.prove(s, ts)
         psurv += s.shape[0]
@@ -334,6 +336,7 @@ def section_served(ccs, engines, n_req=2048, lam=2000.0):
         if d > 0:
             time.sleep(d)
         e = engines[p]
+        e.set_bits(bits)
         s = e.filter_range(ts, nt, cap=1 << 20)
         e.prove(s, ts)
         lat_p.append(time.monotonic() - (base + arr[i]))

@@ -146,6 +146,7 @@ _SIGS = {
     "ccs_filter_range_noalloc": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
     "ccs_prove": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64),
                             C.POINTER(_u64), _vp]),
+    "ccs_set_bits": (C.c_int, [_vp, C.c_uint32]),
     "ccs_search_range_host": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp,
                                         _u64, C.POINTER(_u64), C.POINTER(_u64)]),
     "ccs_walk_numbers": (C.c_int, [_vp, _vp, _u64, C.c_uint32, _vp, _vp]),
@@ -336,6 +337,11 @@ class Engine:
         a = (C.c_uint64 * n)()
         _check(load_library().ccs_get_bases(self.h, a, n))
         return [int(x) for x in a]
+
+    def set_bits(self, bits):
+        """Prover bit-width gate for subsequent prove calls (--bits)."""
+        _check(load_library().ccs_set_bits(self.h, int(bits)), "ccs_set_bits")
+        self.bits = int(bits)
 
     def launches(self):
         inf = _Info()

@@ -33,12 +33,6 @@ struct SweepHeader {
     uint64_t total_units;
 };
 
-// Level-C work queue.
-struct CQueue {
-    uint32_t* count;
-    uint32_t cap;
-    uint4* items;            // {line, j, range, 0}
-};
 
 // Prove-side description of one range.
 struct ProveRange {
@@ -83,10 +77,8 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
                                uint32_t stride, cudaStream_t st);
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride);
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
-                         const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride, CQueue cq,
+                         const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
                          uint32_t b_stride, uint32_t grid, bool std_a, cudaStream_t st);
-cudaError_t launch_levelc(const RangeDev* ranges, const uint32_t* jmod, uint32_t stride, CQueue cq,
-                          uint32_t grid, cudaStream_t st);
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_walk(const uint32_t* numbers, uint64_t n, uint32_t limbs, uint32_t* lengths,
                         int profile, cudaStream_t st);

@@ -97,15 +97,12 @@ struct ccs_engine {
     DevBuf<uint64_t> d_prefix;
     DevBuf<SweepHeader> d_hdr;
     DevBuf<uint32_t> d_jmod;
-    DevBuf<uint32_t> d_counters;     // [0] surv, [1] cq, [2] chains, [3] primes
-    DevBuf<uint4> d_cq;
-    uint32_t cq_cap = 0;
+    DevBuf<uint32_t> d_counters;     // [0] surv, [1] spare, [2] chains, [3] primes
     // host-path scratch
     DevBuf<uint32_t> d_surv_scratch, d_chain_scratch;
     // pinned staging
     void* h_stage = nullptr;
     size_t h_stage_bytes = 0;
-    double levelc_rate = 0;          // fraction of candidates entering level C
     uint64_t launches = 0;           // kernels launched by this engine
 };
 
@@ -121,9 +118,7 @@ struct ccs_batch {
     DevBuf<SweepHeader> d_hdr;
     DevBuf<uint32_t> d_jmod, d_primes;   // concatenated range-prime lists of all profiles
     DevBuf<uint32_t> d_surv, d_chains;
-    DevBuf<uint32_t> d_counts;           // [0] surv [1] cq [2] chains [3] spare, then 3 per range
-    DevBuf<uint4> d_cq;
-    uint32_t cq_cap = 0;
+    DevBuf<uint32_t> d_counts;           // [0] surv [1] spare [2] chains [3] spare, then 3 per range
     std::vector<uint32_t> prime_base;    // per profile offset into d_primes
     uint32_t max_range_primes = 0;
     uint32_t b_stride = 0;
@@ -354,12 +349,6 @@ ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out) {
     E->tune.block_threads = kSweepThreads;
     E->tune.unit_words = 1024;
     E->tune.split_prime = 1024;
-    // fraction of candidates that reach level C
-    double f = 1.0;
-    for (auto& fp : hp.fprimes)
-        if (fp.q < E->tune.split_prime) f *= 1.0 - (double)fp.forb.size() / fp.q;
-    E->levelc_rate = hp.primesC.empty() ? 0.0 : f;
-
     E->slot = alloc_slot(device);
     if (E->slot < 0) { delete E; return fail(CCS_ERR_BUSY, "all constant-memory profile slots in use (max 8 engines per device)"); }
     cudaDeviceProp prop;
@@ -372,9 +361,8 @@ ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out) {
     E->tune.blocks_per_sm = bps > 0 ? (uint32_t)bps : 1;
 
     // plain-path state
-    E->cq_cap = hp.primesC.empty() ? 1 : (1u << 24);
     if (E->d_range.alloc(1) || E->d_prange.alloc(1) || E->d_prefix.alloc(2) || E->d_hdr.alloc(1) ||
-        E->d_jmod.alloc(hp.range_primes.size()) || E->d_counters.alloc(8) || E->d_cq.alloc(E->cq_cap)) {
+        E->d_jmod.alloc(hp.range_primes.size()) || E->d_counters.alloc(8)) {
         ccs_destroy(E);
         return fail(CCS_ERR_NOMEM, "device allocation failed");
     }
@@ -394,7 +382,7 @@ ccs_status ccs_destroy(ccs_engine* E) {
     E->lines.free_(); E->primesB.free_(); E->primesC.free_(); E->bitmapB.free_(); E->packB.free_();
     E->listC.free_(); E->range_primes.free_(); E->bases.free_();
     E->d_range.free_(); E->d_prange.free_(); E->d_prefix.free_(); E->d_hdr.free_();
-    E->d_jmod.free_(); E->d_counters.free_(); E->d_cq.free_();
+    E->d_jmod.free_(); E->d_counters.free_();
     E->d_surv_scratch.free_(); E->d_chain_scratch.free_();
     if (E->h_stage) cudaFreeHost(E->h_stage);
     if (E->own_stream) cudaStreamDestroy(E->own_stream);
@@ -468,29 +456,16 @@ static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_t
     CU(cudaMemcpyAsync(E->d_range.p, hr, sizeof(RangeDev), cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(E->d_prefix.p, hpre, 16, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(E->d_hdr.p, hh, sizeof(SweepHeader), cudaMemcpyHostToDevice, st));
-    CU(cudaMemsetAsync(E->d_counters.p + 1, 0, 4, st));
-    E->launches += hp.primesC.empty() ? 2 : 3;
+    E->launches += 2;
     CU(launch_range_setup(E->d_range.p, E->d_hdr.p, 1, E->range_primes.p,
                           (uint32_t)hp.range_primes.size(), E->d_jmod.p,
                           (uint32_t)hp.range_primes.size(), st));
-    CQueue cq{E->d_counters.p + 1, E->cq_cap, E->d_cq.p};
     uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
     uint64_t need = (units + (kSweepThreads / 32) - 1) / (kSweepThreads / 32);
     if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
     CU(launch_sweep(E->d_range.p, E->d_prefix.p, E->d_hdr.p, E->d_jmod.p,
-                    (uint32_t)hp.range_primes.size(), cq, b_stride_of((uint32_t)hp.primesB.size()),
+                    (uint32_t)hp.range_primes.size(), b_stride_of((uint32_t)hp.primesB.size()),
                     grid, hp.std_a != 0, st));
-    if (!hp.primesC.empty()) {
-        CU(launch_levelc(E->d_range.p, E->d_jmod.p, (uint32_t)hp.range_primes.size(), cq,
-                         (uint32_t)E->sms * 8, st));
-        uint32_t cqn = 0;
-        CU(cudaMemcpyAsync(hh, E->d_counters.p + 1, 4, cudaMemcpyDeviceToHost, st));
-        CU(cudaStreamSynchronize(st));
-        cqn = *(uint32_t*)hh;
-        if (cqn > E->cq_cap)
-            return fail(CCS_OVERFLOW, "deferred-stage queue overflow (" + std::to_string(cqn) +
-                                          " > " + std::to_string(E->cq_cap) + "); use smaller ranges");
-    }
     return CCS_OK;
 }
 
@@ -506,21 +481,8 @@ ccs_status ccs_filter_range(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint6
     CU(cudaMemsetAsync(E->d_counters.p, 0, 4, st));
     *n_out = 0;
     if (n_tiles) {
-        // chunk so the deferred level-C queue cannot overflow (4x margin)
-        uint64_t cpt = 0;
-        for (uint32_t w : E->hp.wheel_total) cpt += w;
-        cpt = cpt / 6 + 1;
-        uint64_t max_tiles = n_tiles;
-        if (E->levelc_rate > 0) {
-            double tiles = (double)E->cq_cap / (4.0 * E->levelc_rate * (double)cpt);
-            if (tiles < 6) tiles = 6;
-            if (tiles < (double)max_tiles) max_tiles = (uint64_t)tiles / 6 * 6;
-        }
-        for (uint64_t off = 0; off < n_tiles; off += max_tiles) {
-            uint64_t nt = std::min<uint64_t>(max_tiles, n_tiles - off);
-            ccs_status s = filter_chunk(E, ts + off, nt, (uint32_t)off, out_dev, cap, st);
-            if (s != CCS_OK) return s;
-        }
+        ccs_status s = filter_chunk(E, ts, n_tiles, 0, out_dev, cap, st);
+        if (s != CCS_OK) return s;
     }
     uint32_t cnt = 0;
     CU(cudaMemcpyAsync(E->h_stage, E->d_counters.p, 4, cudaMemcpyDeviceToHost, st));
@@ -569,6 +531,13 @@ ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_sur
     *n_out = hc[0];
     if (primes_out) *primes_out = hc[1];
     if (hc[0] > cap) return fail(CCS_OVERFLOW, "chain capacity exceeded");
+    return CCS_OK;
+}
+
+ccs_status ccs_set_bits(ccs_engine* E, uint32_t bits) {
+    if (!E) return fail(CCS_ERR_INVALID, "null engine");
+    if (bits < 21 || bits > 160) return fail(CCS_ERR_INVALID, "bits out of range [21, 160]");
+    E->hp.bits = bits;
     return CCS_OK;
 }
 
@@ -638,12 +607,9 @@ ccs_status ccs_walk_modmuls(ccs_engine* E, uint64_t* count, int reset) {
 // Scratch layout (bytes):
 //   [0, 1024)            range descriptor, unit prefix, sweep header, counters
 //   [1024, +64 KiB)      per-range residues J0 mod q (kNoAllocMaxPrimes x u32)
-//   [.., +4 MiB)         deferred-stage queue (kNoAllocQueue x 16 B)
 constexpr uint32_t kNoAllocMaxPrimes = 16384;
-constexpr uint32_t kNoAllocQueue = 1u << 18;
 constexpr size_t kNoAllocJmodOff = 1024;
-constexpr size_t kNoAllocQueueOff = kNoAllocJmodOff + 4ull * kNoAllocMaxPrimes;
-constexpr size_t kNoAllocBytes = kNoAllocQueueOff + 16ull * kNoAllocQueue;   // 4,260,864 B
+constexpr size_t kNoAllocBytes = kNoAllocJmodOff + 4ull * kNoAllocMaxPrimes;   // 66,560 B
 
 // One copy per device that loads the library, held until process exit.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -693,23 +659,13 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
     RangeDev* d_range = (RangeDev*)(base + 0);
     uint64_t* d_prefix = (uint64_t*)(base + 256);
     SweepHeader* d_hdr = (SweepHeader*)(base + 512);
-    uint32_t* d_cnt = (uint32_t*)(base + 768);                 // [0] survivors, [1] queue
+    uint32_t* d_cnt = (uint32_t*)(base + 768);                 // [0] survivors
     uint32_t* d_jmod = (uint32_t*)(base + kNoAllocJmodOff);
-    uint4* d_queue = (uint4*)(base + kNoAllocQueueOff);
-    // the array keeps the previous call's contents: zero the counters
-    CU(cudaMemsetAsync(d_cnt, 0, 8, st));
-    uint64_t max_tiles = n_tiles ? n_tiles : 1;
-    if (!hp.primesC.empty() && E->levelc_rate > 0) {
-        uint64_t cpt = 0;
-        for (uint32_t w : hp.wheel_total) cpt += w;
-        cpt = cpt / 6 + 1;
-        double tiles = (double)kNoAllocQueue / (4.0 * E->levelc_rate * (double)cpt);
-        if (tiles < 6) tiles = 6;
-        if (tiles < (double)max_tiles) max_tiles = (uint64_t)tiles / 6 * 6;
-    }
-    for (uint64_t off = 0; off < n_tiles; off += max_tiles) {
-        const uint64_t nt = std::min<uint64_t>(max_tiles, n_tiles - off);
-        const unsigned __int128 cts = ts + off;
+    // the array keeps the previous call's contents: zero the counter
+    CU(cudaMemsetAsync(d_cnt, 0, 4, st));
+    if (n_tiles) {
+        const uint64_t nt = n_tiles, off = 0;
+        const unsigned __int128 cts = ts;
         RangeDev hr;
         memset(&hr, 0, sizeof(hr));
         fill_J0(hr.J0, cts / 6);
@@ -732,24 +688,13 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
         CU(cudaMemcpyAsync(d_range, &hr, sizeof(hr), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(d_prefix, hpre, sizeof(hpre), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(d_hdr, &hh, sizeof(hh), cudaMemcpyHostToDevice, st));
-        CU(cudaMemsetAsync(d_cnt + 1, 0, 4, st));
         CU(launch_range_setup(d_range, d_hdr, 1, E->range_primes.p, np, d_jmod, np, st));
-        CQueue cq{d_cnt + 1, kNoAllocQueue, d_queue};
         uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
         const uint64_t need = (units + (kSweepThreads / 32) - 1) / (kSweepThreads / 32);
         if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
-        CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, cq, b_stride_of((uint32_t)hp.primesB.size()),
+        CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, b_stride_of((uint32_t)hp.primesB.size()),
                         grid, hp.std_a != 0, st));
         E->launches += 2;
-        if (!hp.primesC.empty()) {
-            CU(launch_levelc(d_range, d_jmod, np, cq, (uint32_t)E->sms * 8, st));
-            E->launches += 1;
-            uint32_t qn = 0;
-            CU(cudaMemcpyAsync(&qn, d_cnt + 1, 4, cudaMemcpyDeviceToHost, st));
-            CU(cudaStreamSynchronize(st));
-            if (qn > kNoAllocQueue)
-                return fail(CCS_OVERFLOW, "deferred-stage queue of the no-allocation path overflowed");
-        }
     }
     uint32_t cnt = 0;
     CU(cudaMemcpyAsync(&cnt, d_cnt, 4, cudaMemcpyDeviceToHost, st));
@@ -770,7 +715,7 @@ ccs_status ccs_batch_destroy(ccs_batch* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     b->d_ranges.free_(); b->d_pranges.free_(); b->d_prefix.free_(); b->d_hdr.free_();
     b->d_jmod.free_(); b->d_primes.free_(); b->d_surv.free_(); b->d_chains.free_();
-    b->d_counts.free_(); b->d_cq.free_();
+    b->d_counts.free_();
     if (b->h_ranges) cudaFreeHost(b->h_ranges);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -796,23 +741,20 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     b->chain_cap = std::max<uint64_t>(chain_cap, 1);
     std::vector<uint32_t> allp;
     uint32_t maxnb = 0;
-    bool any_c = false;
     for (auto* E : b->prof) {
         b->prime_base.push_back((uint32_t)allp.size());
         allp.insert(allp.end(), E->hp.range_primes.begin(), E->hp.range_primes.end());
         b->max_range_primes = std::max<uint32_t>(b->max_range_primes, (uint32_t)E->hp.range_primes.size());
         maxnb = std::max<uint32_t>(maxnb, (uint32_t)E->hp.primesB.size());
-        any_c |= !E->hp.primesC.empty();
     }
     b->b_stride = b_stride_of(maxnb);
     b->jstride = b->max_range_primes;
-    b->cq_cap = any_c ? (1u << 24) : 1;
     size_t nc = 4 + 3 * (size_t)max_ranges;
     if (b->d_ranges.alloc(max_ranges) || b->d_pranges.alloc(max_ranges) ||
         b->d_prefix.alloc(max_ranges + 1) || b->d_hdr.alloc(1) ||
         b->d_jmod.alloc((size_t)max_ranges * b->jstride) || b->d_primes.alloc(allp.size()) ||
         b->d_surv.alloc(4 * b->surv_cap) || b->d_chains.alloc(12 * b->chain_cap) ||
-        b->d_counts.alloc(nc) || b->d_cq.alloc(b->cq_cap)) {
+        b->d_counts.alloc(nc)) {
         ccs_batch_destroy(b);
         return fail(CCS_ERR_NOMEM, "batch device allocation failed");
     }
@@ -847,10 +789,8 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     cudaMemsetAsync(b->d_counts.p, 0, 4 * nc, st);
     launch_range_setup(b->d_ranges.p, b->d_hdr.p, max_ranges, b->d_primes.p, b->max_range_primes,
                        b->d_jmod.p, b->jstride, st);
-    CQueue cq{b->d_counts.p + 1, b->cq_cap, b->d_cq.p};
-    launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, cq, b->b_stride,
+    launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, b->b_stride,
                  b->grid, all_std, st);
-    if (any_c) launch_levelc(b->d_ranges.p, b->d_jmod.p, b->jstride, cq, (uint32_t)b->prof[0]->sms * 8, st);
     ProveArgs pa;
     pa.ranges = b->d_pranges.p;
     pa.surv = b->d_surv.p;
@@ -924,7 +864,6 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
     CU(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
     const uint32_t* hc = b->h_counts;
     ccs_status st = CCS_OK;
-    if (hc[1] > b->cq_cap) st = fail(CCS_OVERFLOW, "deferred-stage queue overflow in batch");
     uint64_t ns = hc[0], nch = hc[2];
     // per-range offsets follow the order records were written; results report
     // counts, and offsets are recovered from the flat arrays on the host

@@ -13,9 +13,9 @@
 //   * level B: surviving positions are tested one by one against the primes in
 //     [128, split) using per-lane phases cached in shared memory and the G_q
 //     bitmaps (early exit, ascending q);
-//   * level C: the rare level-B survivors are queued in global memory and a
-//     warp-cooperative kernel tests all primes >= split (32 primes per round,
-//     ballot early exit);
+//   * level C: the rare level-B survivors collect in a per-warp list and the
+//     whole warp tests them against all primes >= split (32 primes per
+//     round, ballot early exit) inside the same kernel;
 //   * survivors are written as the reference's 16-byte Survivor records.
 #include "ccs_kernels.cuh"
 
@@ -92,7 +92,6 @@ struct SweepArgs {
     const SweepHeader* hdr;
     const uint32_t* jmod;          // [n_ranges][jmod_stride]
     uint32_t jmod_stride;
-    CQueue cq;                     // level-C queue
     uint32_t b_stride;             // level-B primes per lane column in shared memory
 };
 
@@ -102,6 +101,7 @@ __device__ constexpr uint32_t kStdQ[kNumA] = {37, 41, 43, 47, 53, 59, 61, 1, 1,
                                               97, 101, 103, 107, 109, 113, 127};
 
 constexpr int kQCap = 256;               // per-warp level-B queue (entries)
+constexpr int kCCap = 64;                // per-warp level-C list (entries)
 constexpr uint32_t kNone = 0xFFFFFFFFu;  // empty lane slot
 
 // x mod q for x < 2^32 via the profile's magic (fast init-time reductions)
@@ -121,6 +121,8 @@ __device__ __forceinline__ uint32_t phase_fast(uint32_t rl, uint32_t rh, uint32_
 // candidate is decided, so lanes stay busy whichever line produced the work.
 struct LevelB {
     uint32_t* Q;                   // kQCap entries: (jrel << 5) | line lane
+    uint32_t* Cl;                  // kCCap level-B survivors waiting for level C
+    uint32_t cnum;                 // entries in Cl (warp-uniform)
     const uint16_t* S;             // [nB][32] phases of the unit's 32 lines at jbase
     const PrimeB* pb;
     const uint32_t* bm;
@@ -129,21 +131,43 @@ struct LevelB {
     uint32_t cur, pi;              // this lane's candidate and next prime index
 };
 
-__device__ __forceinline__ void b_emit(const SweepArgs& a, const RangeDev& R, const ProfileConst& P,
-                                       uint32_t cur_range, uint32_t g, uint32_t jbase, uint32_t e) {
-    const uint32_t L = e & 31u;
-    const uint32_t j = jbase + (e >> 5);
-    const uint32_t li = g * 32 + L;
-    const Line ln = P.lines[li];
-    if (P.nC == 0) {
-        emit_survivor(R, ln, j);
-    } else {
-        uint32_t slot = atomicAdd(a.cq.count, 1u);
-        if (slot < a.cq.cap) {
-            uint4 it; it.x = li; it.y = j; it.z = cur_range; it.w = 0;
-            a.cq.items[slot] = it;
+// Level C, warp-cooperative: every lane takes 32 primes >= split per round
+// for each listed candidate (phase from scratch, binary search in the sorted
+// G_q list), ballot early exit; survivors are written by lane 0.
+__device__ __forceinline__ void c_process(LevelB& B, const SweepArgs& a, const RangeDev& R,
+                                       const ProfileConst& P, uint32_t cur_range, uint32_t g,
+                                       uint32_t jbase, uint32_t lane) {
+    __syncwarp();
+    const uint32_t* jm = a.jmod + (uint64_t)cur_range * a.jmod_stride + kNumA + P.nB;
+    for (uint32_t e = 0; e < B.cnum; e++) {
+        const uint32_t ent = B.Cl[e];
+        const uint32_t j = jbase + (ent >> 5);
+        const Line ln = P.lines[g * 32 + (ent & 31u)];
+        const uint64_t r = ((uint64_t)ln.r_hi << 32) | ln.r_lo;
+        bool killed = false;
+        for (uint32_t base = 0; base < P.nC && !killed; base += 32) {
+            const uint32_t p = base + lane;
+            bool kill = false;
+            if (p < P.nC) {
+                const PrimeC pc = P.primesC[p];
+                const uint32_t rm = mod_magic64(r, pc.q, pc.magic64);
+                const uint32_t rw = mod_magic64((uint64_t)rm * pc.winv, pc.q, pc.magic64);
+                const uint32_t jq = mod_magic64(j, pc.q, pc.magic64);
+                const uint32_t uph = mod_magic64((uint64_t)rw + jm[p] + jq, pc.q, pc.magic64);
+                const uint32_t* lst = P.listC + pc.off;
+                uint32_t lo = 0, hi = pc.cnt;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (__ldg(lst + mid) < uph) lo = mid + 1; else hi = mid;
+                }
+                kill = lo < pc.cnt && __ldg(lst + lo) == uph;
+            }
+            killed = __any_sync(0xFFFFFFFFu, kill);
         }
+        if (!killed && lane == 0) emit_survivor(R, ln, j);
     }
+    B.cnum = 0;
+    __syncwarp();
 }
 
 // one round: refill empty lanes from the queue, then test two primes
@@ -171,10 +195,22 @@ __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const Ran
                 if ((wv >> (u & 31)) & 1u) B.cur = kNone; else B.pi++;
             }
         }
-        if (B.cur != kNone && B.pi >= B.nB) {
-            b_emit(a, R, P, cur_range, g, jbase, B.cur);
+    }
+    // candidates that passed every level-B prime
+    const bool pass = B.cur != kNone && B.pi >= B.nB;
+    if (P.nC == 0) {
+        if (pass) {
+            emit_survivor(R, P.lines[g * 32 + (B.cur & 31u)], jbase + (B.cur >> 5));
             B.cur = kNone;
         }
+    } else {
+        const uint32_t pm = __ballot_sync(0xFFFFFFFFu, pass);
+        if (pass) {
+            B.Cl[B.cnum + __popc(pm & lane_lt)] = B.cur;
+            B.cur = kNone;
+        }
+        B.cnum += __popc(pm);
+        if (B.cnum > (uint32_t)(kCCap - 32)) c_process(B, a, R, P, cur_range, g, jbase, threadIdx.x & 31);
     }
 }
 
@@ -185,9 +221,10 @@ sweep_kernel(SweepArgs a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lane_lt = (1u << lane) - 1u;
     const uint32_t warp_in_block = threadIdx.x >> 5;
-    // per warp: queue (kQCap u32) then phases (b_stride * 32 u16)
-    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + a.b_stride * 16);
-    uint16_t* S = reinterpret_cast<uint16_t*>(Qw + kQCap);
+    // per warp: level-B queue (kQCap u32), level-C list (kCCap u32), phases (b_stride * 32 u16)
+    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + kCCap + a.b_stride * 16);
+    uint32_t* Cw = Qw + kQCap;
+    uint16_t* S = reinterpret_cast<uint16_t*>(Cw + kCCap);
     const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
@@ -253,6 +290,8 @@ sweep_kernel(SweepArgs a) {
         // ---- level B phases at block jbase, one column per line ----
         LevelB B;
         B.Q = Qw;
+        B.Cl = Cw;
+        B.cnum = 0;
         B.S = S;
         B.pb = P.packB;
         B.bm = P.bitmapB;
@@ -333,57 +372,8 @@ sweep_kernel(SweepArgs a) {
         // drain before the unit's phases are replaced
         while (__any_sync(0xFFFFFFFFu, B.cur != kNone) || B.tail != B.head)
             b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
+        if (B.cnum) c_process(B, a, R, P, cur_range, g, jbase, lane);
         __syncwarp();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// level C: warp-cooperative test of queued candidates against primes >= split
-// ---------------------------------------------------------------------------
-struct LevelCArgs {
-    const RangeDev* ranges;
-    const uint32_t* jmod;
-    uint32_t jmod_stride;
-    CQueue cq;
-};
-
-__global__ void __launch_bounds__(256)
-levelc_kernel(LevelCArgs a) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const uint32_t n = min(*a.cq.count, a.cq.cap);
-    for (uint64_t e = gwarp; e < n; e += nwarps) {
-        const uint4 it = a.cq.items[e];
-        const RangeDev& R = a.ranges[it.z];
-        const ProfileConst& P = c_prof[R.profile];
-        const Line ln = P.lines[it.x];
-        const uint64_t r = ((uint64_t)ln.r_hi << 32) | ln.r_lo;
-        const uint32_t j = it.y;
-        const uint32_t* jm = a.jmod + (uint64_t)it.z * a.jmod_stride + kNumA + P.nB;
-        bool killed = false;
-        for (uint32_t base = 0; base < P.nC && !killed; base += 32) {
-            const uint32_t p = base + lane;
-            bool kill = false;
-            if (p < P.nC) {
-                const PrimeC pc = P.primesC[p];
-                uint32_t rm = mod_magic64(r, pc.q, pc.magic64);
-                uint32_t rw = mod_magic64((uint64_t)rm * pc.winv, pc.q, pc.magic64);
-                uint32_t jq = mod_magic64(j, pc.q, pc.magic64);
-                uint32_t uph = mod_magic64((uint64_t)rw + jm[p] + jq, pc.q, pc.magic64);
-                const uint32_t* lst = P.listC + pc.off;
-                // sorted list: binary search
-                uint32_t lo = 0, hi = pc.cnt;
-                while (lo < hi) {
-                    uint32_t mid = (lo + hi) >> 1;
-                    uint32_t v = __ldg(lst + mid);
-                    if (v < uph) lo = mid + 1; else hi = mid;
-                }
-                kill = lo < pc.cnt && __ldg(lst + lo) == uph;
-            }
-            killed = __any_sync(0xFFFFFFFFu, kill);
-        }
-        if (!killed && lane == 0) emit_survivor(R, ln, j);
     }
 }
 
@@ -407,7 +397,7 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
 }
 
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride) {
-    return (size_t)(block_threads / 32) * (kQCap + (size_t)b_stride * 16) * sizeof(uint32_t);
+    return (size_t)(block_threads / 32) * (kQCap + kCCap + (size_t)b_stride * 16) * sizeof(uint32_t);
 }
 
 static bool g_sweep_attr_set = false;
@@ -437,7 +427,7 @@ int sweep_blocks_per_sm(uint32_t b_stride, bool std_a) {
 }
 
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
-                         const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride, CQueue cq,
+                         const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
                          uint32_t b_stride, uint32_t grid, bool std_a, cudaStream_t st) {
     size_t smem = sweep_smem_bytes(kSweepThreads, b_stride);
     cudaError_t e = ensure_sweep_attr();
@@ -448,22 +438,11 @@ cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
     a.hdr = hdr;
     a.jmod = jmod;
     a.jmod_stride = stride;
-    a.cq = cq;
     a.b_stride = b_stride;
     if (std_a) sweep_kernel<true><<<grid, kSweepThreads, smem, st>>>(a);
     else sweep_kernel<false><<<grid, kSweepThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_levelc(const RangeDev* ranges, const uint32_t* jmod, uint32_t stride, CQueue cq,
-                          uint32_t grid, cudaStream_t st) {
-    LevelCArgs a;
-    a.ranges = ranges;
-    a.jmod = jmod;
-    a.jmod_stride = stride;
-    a.cq = cq;
-    levelc_kernel<<<grid, 256, 0, st>>>(a);
-    return cudaGetLastError();
-}
 
 }  // namespace ccs

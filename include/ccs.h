@@ -165,7 +165,7 @@ ccs_status ccs_filter_range(ccs_engine* eng, uint64_t tile_start_lo, uint64_t ti
  * reference.  For callers that cannot allocate device memory when they
  * filter: code inside a CUDA stream capture or a host callback, where
  * cudaMalloc is not allowed, and embedders that must fix their GPU footprint
- * at start-up.  The working memory is a 4,260,864-byte array compiled into
+ * at start-up.  The working memory is a 66,560-byte array compiled into
  * the library; every GPU that loads the library holds one copy until the
  * process exits.  Limit: engines with at most 16362 filter primes (larger
  * ones return CCS_ERR_INVALID); any n_tiles < 2^32.  The first call on a
@@ -185,6 +185,10 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* eng, uint64_t tile_start_lo, uin
 ccs_status ccs_prove(ccs_engine* eng, const ccs_survivor* surv_dev, uint64_t n_surv,
                      uint64_t tile_start_lo, uint64_t tile_start_hi, ccs_chain* out_dev,
                      uint64_t cap, uint64_t* n_out, uint64_t* primes_out, void* stream);
+
+/* Sets the prover bit-width gate of this engine for subsequent ccs_prove /
+ * ccs_search_range_host calls (the reference's --bits, v13:3092). */
+ccs_status ccs_set_bits(ccs_engine* eng, uint32_t bits);
 
 /* Same two steps on HOST buffers, copies included (the reference's per-batch
  * H2D/D2H boundary, v13:3769-3830). */
