@@ -366,6 +366,8 @@ def run_ours(args):
     TILES = args.tiles_per_step
     if args.unit_words:
         eng.set_tuning(unit_words=args.unit_words)
+    if args.ext_min_words:
+        eng.set_tuning(ext_min_words=args.ext_min_words)
     info = eng.info
     cpt = info["candidates_per_tile"]
     bases = eng.bases()
@@ -522,6 +524,9 @@ def main():
     ap.add_argument("--tiles-per-step", type=int, default=TILES_PER_STEP,
                     help="tiles per step (smaller values: profiling cases)")
     ap.add_argument("--unit-words", type=int, default=0, help="sweep work-unit length (0: tuned)")
+    ap.add_argument("--ext-min-words", type=lambda v: int(v, 0), default=0,
+                    help="extended-lattice threshold in 64-position words (0: engine default, "
+                         "0xFFFFFFFF: plain lattice only)")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the prove-batch, batched and served sections")
     ap.add_argument("--batch-ranges", type=int, default=4096)

@@ -128,7 +128,8 @@ class _RequestResult(C.Structure):
 
 class _Tuning(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("unit_words", C.c_uint32), ("split_prime", C.c_uint32)]
+                ("unit_words", C.c_uint32), ("split_prime", C.c_uint32),
+                ("ext_min_words", C.c_uint32), ("_pad", C.c_uint32)]
 
 
 # exported symbols of include/ccs.h, with their ctypes signatures
@@ -355,7 +356,7 @@ class Engine:
     def tuning(self):
         t = _Tuning()
         _check(load_library().ccs_get_tuning(self.h, C.byref(t)))
-        return {f: getattr(t, f) for f, _ in _Tuning._fields_}
+        return {f: getattr(t, f) for f, _ in _Tuning._fields_ if not f.startswith("_")}
 
     def set_tuning(self, **kw):
         t = _Tuning()

@@ -26,7 +26,7 @@ constexpr int kNumA1 = 9;              // bit-sliced primes q < 64
 constexpr int kNumA2 = 6;              // bit-sliced primes 64 < q < 96 (96-bit windows)
 constexpr int kNumA3 = 7;              // bit-sliced primes 96 < q < 128 (128-bit windows)
 constexpr int kNumA = kNumA1 + kNumA2 + kNumA3;
-constexpr int kMaxProfiles = 8;
+constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
 
 // One bit-sliced ("level A") prime: the 64-candidate kill window is advanced
@@ -60,16 +60,20 @@ struct PrimeC {
     uint64_t magic64;    // floor(2^64 / q) (level C)
 };
 
-// Device line record: residue r mod W and its reference coordinates.
+// Device line record: residue r mod W and its reference coordinates.  On an
+// extended profile (a filter prime q0 absorbed into the modulus, W' = q0 W)
+// r is the residue mod W' and d = (r div W) < q0 selects the block class.
 struct Line {
     uint32_t r_lo, r_hi;
     uint32_t k;          // wheel offset (k_offset)
-    uint32_t bc;         // base_idx | (c << 16)   (c = tile mod 6 of the line)
+    uint32_t bc;         // base_idx | (c << 16) | (d << 19)   (c = tile mod 6)
 };
 
 // Constant-memory image of one profile (lattice + filter).
 struct ProfileConst {
-    uint64_t W;                      // 6*M*WP
+    uint64_t W;                      // 6*M*WP (times q0 on an extended profile)
+    uint32_t q0;                     // absorbed prime (1: none)
+    uint32_t _q0pad;
     uint32_t n_lines;
     uint32_t nB, nC;                 // counts of per-candidate primes
     uint32_t c32W_dummy;
@@ -93,6 +97,7 @@ struct HostProfile {
     uint32_t max_bases = 0;
     std::vector<uint64_t> witnesses;
     uint32_t primality = 1, prove_mode = 1;
+    uint32_t q0 = 1;                 // filter prime absorbed into the modulus (1: none)
 
     // lattice
     uint64_t M = 0, W = 0;
@@ -119,7 +124,7 @@ struct HostProfile {
 };
 
 // Builds the lattice and tables; returns "" or an error message.
-std::string build_profile(HostProfile& hp, uint32_t split_prime);
+std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0 = 1);
 
 uint32_t mod_inverse_u32(uint32_t a, uint32_t q);
 bool is_prime_u32(uint32_t n);

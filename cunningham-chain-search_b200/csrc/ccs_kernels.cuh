@@ -10,10 +10,11 @@ constexpr int kSweepThreads = 256;
 
 // One lattice range as the device sees it.
 struct RangeDev {
-    uint32_t J0[4];          // floor(tile_start / 6), u128 limbs
+    uint32_t J0[4];          // floor(floor(tile_start / 6) / q0), u128 limbs
     uint32_t e0;             // tile_start mod 6
+    uint32_t e1;             // floor(tile_start / 6) mod q0 (0 on a plain profile)
     uint32_t n_tiles;        // tiles in the range (< 2^32)
-    uint32_t n_words;        // ceil(ceil((e0 + n_tiles) / 6) / 64)
+    uint32_t n_words;        // 64-position words spanned by the range's lines
     uint32_t unit_words;     // words per work unit
     uint32_t profile;        // constant-memory profile slot
     uint32_t prime_base;     // offset of this profile's prime list (range setup)
@@ -78,11 +79,11 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride);
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
-                         uint32_t b_stride, uint32_t grid, bool std_a, cudaStream_t st);
+                         uint32_t b_stride, uint32_t grid, cudaStream_t st);
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_walk(const uint32_t* numbers, uint64_t n, uint32_t limbs, uint32_t* lengths,
                         int profile, cudaStream_t st);
-int sweep_blocks_per_sm(uint32_t b_stride, bool std_a);
+int sweep_blocks_per_sm(uint32_t b_stride);
 cudaError_t modmul_count(uint64_t* out, bool reset);
 
 }  // namespace ccs

@@ -74,21 +74,38 @@ struct DevBuf {
     }
 };
 
-}  // namespace
-
-struct ccs_engine {
-    int device = 0;
-    int slot = -1;
+// One filter variant of a profile: the lattice lines and the per-prime tables
+// the sweep reads, plus the constant-memory slot they are registered in.
+struct FilterSet {
     HostProfile hp;
-    ccs_tuning tune{};
-    int sms = 148;
-    cudaStream_t own_stream = nullptr;
-
-    // profile tables
+    int slot = -1;
     DevBuf<Line> lines;
     DevBuf<PrimeC> primesB, primesC;
     DevBuf<PrimeB> packB;
     DevBuf<uint32_t> bitmapB, listC, range_primes;
+    void free_() {
+        lines.free_(); primesB.free_(); primesC.free_(); packB.free_();
+        bitmapB.free_(); listC.free_(); range_primes.free_();
+    }
+};
+
+}  // namespace
+
+// fs[0] is the profile as given (the lattice of the reference); fs[1], when
+// present, is the same profile with its smallest bit-sliced filter prime q0
+// absorbed into the modulus (W' = q0 W, lines r + d W for the d in [0, q0)
+// that q0 does not kill).  Long ranges are swept on fs[1]; both produce the
+// same survivors in the same (base, k, tile) coordinates.
+struct ccs_engine {
+    int device = 0;
+    FilterSet fs[2];
+    int n_fs = 1;
+    ccs_tuning tune{};
+    int sms = 148;
+    cudaStream_t own_stream = nullptr;
+    int slot = -1;                   // == fs[0].slot: prove-side constants
+    HostProfile& hp = fs[0].hp;      // the profile as given
+
     DevBuf<uint64_t> bases;
 
     // plain-path working state
@@ -119,7 +136,7 @@ struct ccs_batch {
     DevBuf<uint32_t> d_jmod, d_primes;   // concatenated range-prime lists of all profiles
     DevBuf<uint32_t> d_surv, d_chains;
     DevBuf<uint32_t> d_counts;           // [0] surv [1] spare [2] chains [3] spare, then 3 per range
-    std::vector<uint32_t> prime_base;    // per profile offset into d_primes
+    std::vector<uint32_t> prime_base;    // offset into d_primes per (profile i, filter set v): [2 i + v]
     uint32_t max_range_primes = 0;
     uint32_t b_stride = 0;
     // pinned staging: ranges, prefix, header, counts
@@ -158,46 +175,52 @@ uint32_t words_for(uint32_t e0, uint64_t n_tiles) {
     return (uint32_t)((span + 63) / 64);
 }
 
-ccs_status upload_profile(ccs_engine* E, cudaStream_t st) {
-    HostProfile& hp = E->hp;
-    CU(E->lines.alloc(hp.lines.size()));
-    CU(cudaMemcpy(E->lines.p, hp.lines.data(), sizeof(Line) * hp.lines.size(), cudaMemcpyHostToDevice));
-    CU(E->primesB.alloc(hp.primesB.size()));
+ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
+    const HostProfile& hp = f.hp;
+    CU(f.lines.alloc(hp.lines.size()));
+    CU(cudaMemcpy(f.lines.p, hp.lines.data(), sizeof(Line) * hp.lines.size(), cudaMemcpyHostToDevice));
+    CU(f.primesB.alloc(hp.primesB.size()));
     if (!hp.primesB.empty())
-        CU(cudaMemcpy(E->primesB.p, hp.primesB.data(), sizeof(PrimeC) * hp.primesB.size(), cudaMemcpyHostToDevice));
-    CU(E->primesC.alloc(hp.primesC.size()));
+        CU(cudaMemcpy(f.primesB.p, hp.primesB.data(), sizeof(PrimeC) * hp.primesB.size(), cudaMemcpyHostToDevice));
+    CU(f.primesC.alloc(hp.primesC.size()));
     if (!hp.primesC.empty())
-        CU(cudaMemcpy(E->primesC.p, hp.primesC.data(), sizeof(PrimeC) * hp.primesC.size(), cudaMemcpyHostToDevice));
-    CU(E->packB.alloc(hp.packB.size()));
+        CU(cudaMemcpy(f.primesC.p, hp.primesC.data(), sizeof(PrimeC) * hp.primesC.size(), cudaMemcpyHostToDevice));
+    CU(f.packB.alloc(hp.packB.size()));
     if (!hp.packB.empty())
-        CU(cudaMemcpy(E->packB.p, hp.packB.data(), sizeof(PrimeB) * hp.packB.size(), cudaMemcpyHostToDevice));
-    CU(E->bitmapB.alloc(hp.bitmapB.size()));
+        CU(cudaMemcpy(f.packB.p, hp.packB.data(), sizeof(PrimeB) * hp.packB.size(), cudaMemcpyHostToDevice));
+    CU(f.bitmapB.alloc(hp.bitmapB.size()));
     if (!hp.bitmapB.empty())
-        CU(cudaMemcpy(E->bitmapB.p, hp.bitmapB.data(), 4 * hp.bitmapB.size(), cudaMemcpyHostToDevice));
-    CU(E->listC.alloc(hp.listC.size()));
+        CU(cudaMemcpy(f.bitmapB.p, hp.bitmapB.data(), 4 * hp.bitmapB.size(), cudaMemcpyHostToDevice));
+    CU(f.listC.alloc(hp.listC.size()));
     if (!hp.listC.empty())
-        CU(cudaMemcpy(E->listC.p, hp.listC.data(), 4 * hp.listC.size(), cudaMemcpyHostToDevice));
-    CU(E->range_primes.alloc(hp.range_primes.size()));
-    CU(cudaMemcpy(E->range_primes.p, hp.range_primes.data(), 4 * hp.range_primes.size(), cudaMemcpyHostToDevice));
-    CU(E->bases.alloc(hp.bases.size()));
-    CU(cudaMemcpy(E->bases.p, hp.bases.data(), 8 * hp.bases.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(f.listC.p, hp.listC.data(), 4 * hp.listC.size(), cudaMemcpyHostToDevice));
+    CU(f.range_primes.alloc(hp.range_primes.size()));
+    CU(cudaMemcpy(f.range_primes.p, hp.range_primes.data(), 4 * hp.range_primes.size(), cudaMemcpyHostToDevice));
 
     ProfileConst pc;
     memset(&pc, 0, sizeof(pc));
     pc.W = hp.W;
+    pc.q0 = hp.q0;
     pc.n_lines = (uint32_t)hp.lines.size();
     pc.nB = (uint32_t)hp.primesB.size();
     pc.nC = (uint32_t)hp.primesC.size();
     memcpy(pc.A, hp.A, sizeof(pc.A));
-    pc.lines = E->lines.p;
-    pc.primesB = E->primesB.p;
-    pc.packB = E->packB.p;
-    pc.bitmapB = E->bitmapB.p;
+    pc.lines = f.lines.p;
+    pc.primesB = f.primesB.p;
+    pc.packB = f.packB.p;
+    pc.bitmapB = f.bitmapB.p;
     pc.std_a = hp.std_a;
-    pc.primesC = E->primesC.p;
-    pc.listC = E->listC.p;
-    CU(upload_profile_const(E->slot, pc, st));
+    pc.primesC = f.primesC.p;
+    pc.listC = f.listC.p;
+    CU(upload_profile_const(f.slot, pc, st));
+    CU(cudaStreamSynchronize(st));
+    return CCS_OK;
+}
 
+ccs_status upload_prove(ccs_engine* E, cudaStream_t st) {
+    const HostProfile& hp = E->hp;
+    CU(E->bases.alloc(hp.bases.size()));
+    CU(cudaMemcpy(E->bases.p, hp.bases.data(), 8 * hp.bases.size(), cudaMemcpyHostToDevice));
     ProveConst pv;
     memset(&pv, 0, sizeof(pv));
     pv.bases = E->bases.p;
@@ -219,17 +242,17 @@ uint32_t b_stride_of(uint32_t nB) {
 }
 
 // work units for one range
-uint64_t units_of(const ccs_engine* E, uint32_t n_words, uint32_t unit_words) {
-    uint64_t groups = (E->hp.lines.size() + 31) / 32;
+uint64_t units_of(const FilterSet& f, uint32_t n_words, uint32_t unit_words) {
+    uint64_t groups = (f.hp.lines.size() + 31) / 32;
     uint64_t chunks = (n_words + unit_words - 1) / unit_words;
     return groups * chunks;
 }
 
 // words per work unit: the tuned length, shortened when the range is too
 // small to give every resident warp several units
-uint32_t choose_unit_words(const ccs_engine* E, uint32_t n_words) {
+uint32_t choose_unit_words(const ccs_engine* E, const FilterSet& f, uint32_t n_words) {
     uint32_t uw = E->tune.unit_words ? E->tune.unit_words : 1024;
-    uint64_t groups = (E->hp.lines.size() + 31) / 32;
+    uint64_t groups = (f.hp.lines.size() + 31) / 32;
     uint64_t warps = (uint64_t)E->sms * std::max<uint32_t>(E->tune.blocks_per_sm, 1) * (kSweepThreads / 32);
     uint64_t chunks_wanted = (4 * warps + groups - 1) / groups;
     if (chunks_wanted > 1) {
@@ -238,6 +261,32 @@ uint32_t choose_unit_words(const ccs_engine* E, uint32_t n_words) {
     }
     if (uw > n_words) uw = n_words ? n_words : 1;
     return uw;
+}
+
+// Places a range of n_tiles tiles from ts on one of the engine's filter sets:
+// the extended one when the range spans at least ext_min_words 64-position
+// words of it.  Fills J0, e0, e1, n_tiles, n_words, unit_words, profile and
+// n_range_primes; returns the filter set used.
+const FilterSet& place_range(const ccs_engine* E, unsigned __int128 ts, uint64_t n_tiles, RangeDev& R) {
+    const unsigned __int128 J = ts / 6;
+    R.e0 = (uint32_t)(ts % 6);
+    R.n_tiles = (uint32_t)n_tiles;
+    const uint64_t span = n_tiles ? (R.e0 + n_tiles + 5) / 6 : 0;     // blocks touched
+    int v = 0;
+    if (E->n_fs > 1 && E->tune.ext_min_words != 0xFFFFFFFFu) {
+        const uint32_t q0 = E->fs[1].hp.q0;
+        if (((span + q0 - 1) / q0 + 63) / 64 >= E->tune.ext_min_words) v = 1;
+    }
+    const FilterSet& f = E->fs[v];
+    const uint32_t q0 = f.hp.q0;
+    fill_J0(R.J0, J / q0);
+    R.e1 = (uint32_t)(J % q0);
+    const uint64_t positions = (span + R.e1 + q0 - 1) / q0;
+    R.n_words = n_tiles ? (uint32_t)((positions + 63) / 64) : 0;
+    R.unit_words = choose_unit_words(E, f, R.n_words);
+    R.profile = (uint32_t)f.slot;
+    R.n_range_primes = (uint32_t)f.hp.range_primes.size();
+    return f;
 }
 
 }  // namespace
@@ -349,20 +398,49 @@ ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out) {
     E->tune.block_threads = kSweepThreads;
     E->tune.unit_words = 1024;
     E->tune.split_prime = 1024;
-    E->slot = alloc_slot(device);
-    if (E->slot < 0) { delete E; return fail(CCS_ERR_BUSY, "all constant-memory profile slots in use (max 8 engines per device)"); }
+    E->tune.ext_min_words = 256;
+    // extended filter set: absorb the smallest bit-sliced prime when it is
+    // below 64 (one 64-bit window) and the lattice stays within 62 bits
+    if (hp.A[0].q > 1 && hp.A[0].q < 64) {
+        HostProfile& hx = E->fs[1].hp;
+        hx.target = hp.target; hx.depth = hp.depth; hx.bits = hp.bits;
+        hx.crt = hp.crt; hx.wheel = hp.wheel; hx.stages = hp.stages;
+        hx.max_bases = hp.max_bases; hx.witnesses = hp.witnesses;
+        hx.primality = hp.primality; hx.prove_mode = hp.prove_mode;
+        if (build_profile(hx, 1024, hp.A[0].q).empty() && hx.primesB.size() <= (size_t)kMaxLevelB)
+            E->n_fs = 2;
+    }
+    for (int v = 0; v < E->n_fs; v++) {
+        E->fs[v].slot = alloc_slot(device);
+        if (E->fs[v].slot < 0) {
+            ccs_destroy(E);
+            return fail(CCS_ERR_BUSY, "all constant-memory profile slots in use (max 16 filter profiles per device)");
+        }
+    }
+    E->slot = E->fs[0].slot;
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, device));
     E->sms = prop.multiProcessorCount;
     CU(cudaStreamCreateWithFlags(&E->own_stream, cudaStreamNonBlocking));
-    ccs_status st = upload_profile(E, E->own_stream);
-    if (st != CCS_OK) { ccs_destroy(E); return st; }
-    int bps = sweep_blocks_per_sm(b_stride_of((uint32_t)hp.primesB.size()), hp.std_a != 0);
+    for (int v = 0; v < E->n_fs; v++) {
+        ccs_status st = upload_filter(E->fs[v], E->own_stream);
+        if (st != CCS_OK) { ccs_destroy(E); return st; }
+    }
+    {
+        ccs_status st = upload_prove(E, E->own_stream);
+        if (st != CCS_OK) { ccs_destroy(E); return st; }
+    }
+    uint32_t max_np = 0, max_nb = 0;
+    for (int v = 0; v < E->n_fs; v++) {
+        max_np = std::max<uint32_t>(max_np, (uint32_t)E->fs[v].hp.range_primes.size());
+        max_nb = std::max<uint32_t>(max_nb, (uint32_t)E->fs[v].hp.primesB.size());
+    }
+    int bps = sweep_blocks_per_sm(b_stride_of(max_nb));
     E->tune.blocks_per_sm = bps > 0 ? (uint32_t)bps : 1;
 
     // plain-path state
     if (E->d_range.alloc(1) || E->d_prange.alloc(1) || E->d_prefix.alloc(2) || E->d_hdr.alloc(1) ||
-        E->d_jmod.alloc(hp.range_primes.size()) || E->d_counters.alloc(8)) {
+        E->d_jmod.alloc(max_np) || E->d_counters.alloc(8)) {
         ccs_destroy(E);
         return fail(CCS_ERR_NOMEM, "device allocation failed");
     }
@@ -379,14 +457,14 @@ ccs_status ccs_destroy(ccs_engine* E) {
     if (!E) return CCS_OK;
     cudaSetDevice(E->device);
     if (E->own_stream) cudaStreamSynchronize(E->own_stream);
-    E->lines.free_(); E->primesB.free_(); E->primesC.free_(); E->bitmapB.free_(); E->packB.free_();
-    E->listC.free_(); E->range_primes.free_(); E->bases.free_();
+    for (auto& f : E->fs) f.free_();
+    E->bases.free_();
     E->d_range.free_(); E->d_prange.free_(); E->d_prefix.free_(); E->d_hdr.free_();
     E->d_jmod.free_(); E->d_counters.free_();
     E->d_surv_scratch.free_(); E->d_chain_scratch.free_();
     if (E->h_stage) cudaFreeHost(E->h_stage);
     if (E->own_stream) cudaStreamDestroy(E->own_stream);
-    free_slot(E->device, E->slot);
+    for (auto& f : E->fs) free_slot(E->device, f.slot);
     delete E;
     return CCS_OK;
 }
@@ -420,6 +498,7 @@ ccs_status ccs_set_tuning(ccs_engine* E, const ccs_tuning* t) {
         return fail(CCS_ERR_INVALID, "split_prime is fixed at engine creation");
     if (t->unit_words) E->tune.unit_words = t->unit_words;
     if (t->blocks_per_sm) E->tune.blocks_per_sm = t->blocks_per_sm;
+    if (t->ext_min_words) E->tune.ext_min_words = t->ext_min_words;
     return CCS_OK;
 }
 
@@ -428,27 +507,20 @@ ccs_status ccs_set_tuning(ccs_engine* E, const ccs_tuning* t) {
 // ---------------------------------------------------------------------------
 static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_tiles, uint32_t bias,
                                ccs_survivor* out, uint64_t cap, cudaStream_t st) {
-    HostProfile& hp = E->hp;
     RangeDev* hr = (RangeDev*)E->h_stage;
     uint64_t* hpre = (uint64_t*)((char*)E->h_stage + 1024);
     SweepHeader* hh = (SweepHeader*)((char*)E->h_stage + 2048);
     memset(hr, 0, sizeof(RangeDev));
-    unsigned __int128 J0 = ts / 6;
-    fill_J0(hr->J0, J0);
-    hr->e0 = (uint32_t)(ts % 6);
-    hr->n_tiles = (uint32_t)n_tiles;
-    hr->n_words = words_for(hr->e0, n_tiles);
-    hr->unit_words = choose_unit_words(E, hr->n_words);
-    hr->profile = (uint32_t)E->slot;
+    const FilterSet& f = place_range(E, ts, n_tiles, *hr);
+    const HostProfile& hp = f.hp;
     hr->prime_base = 0;
-    hr->n_range_primes = (uint32_t)hp.range_primes.size();
     hr->surv_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
     hr->surv_count = E->d_counters.p;
     hr->surv = (uint32_t*)out;
     hr->range_count = nullptr;
     hr->range_id = 0;
     hr->tile_bias = bias;
-    uint64_t units = units_of(E, hr->n_words, hr->unit_words);
+    uint64_t units = units_of(f, hr->n_words, hr->unit_words);
     hpre[0] = 0;
     hpre[1] = units;
     hh->n_ranges = 1;
@@ -457,7 +529,7 @@ static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_t
     CU(cudaMemcpyAsync(E->d_prefix.p, hpre, 16, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(E->d_hdr.p, hh, sizeof(SweepHeader), cudaMemcpyHostToDevice, st));
     E->launches += 2;
-    CU(launch_range_setup(E->d_range.p, E->d_hdr.p, 1, E->range_primes.p,
+    CU(launch_range_setup(E->d_range.p, E->d_hdr.p, 1, f.range_primes.p,
                           (uint32_t)hp.range_primes.size(), E->d_jmod.p,
                           (uint32_t)hp.range_primes.size(), st));
     uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
@@ -465,7 +537,7 @@ static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_t
     if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
     CU(launch_sweep(E->d_range.p, E->d_prefix.p, E->d_hdr.p, E->d_jmod.p,
                     (uint32_t)hp.range_primes.size(), b_stride_of((uint32_t)hp.primesB.size()),
-                    grid, hp.std_a != 0, st));
+                    grid, st));
     return CCS_OK;
 }
 
@@ -640,7 +712,8 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
     if (!E || !n_out) return fail(CCS_ERR_INVALID, "null argument");
     if (cap && !out_dev) return fail(CCS_ERR_INVALID, "out_dev is null");
     if (n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
-    const HostProfile& hp = E->hp;
+    const FilterSet& f = E->fs[0];
+    const HostProfile& hp = f.hp;
     const uint32_t np = (uint32_t)hp.range_primes.size();
     if (np > kNoAllocMaxPrimes)
         return fail(CCS_ERR_INVALID, "ccs_filter_range_noalloc supports at most " +
@@ -672,14 +745,14 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
         hr.e0 = (uint32_t)(cts % 6);
         hr.n_tiles = (uint32_t)nt;
         hr.n_words = words_for(hr.e0, nt);
-        hr.unit_words = choose_unit_words(E, hr.n_words);
-        hr.profile = (uint32_t)E->slot;
+        hr.unit_words = choose_unit_words(E, f, hr.n_words);
+        hr.profile = (uint32_t)f.slot;
         hr.n_range_primes = np;
         hr.surv_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
         hr.surv_count = d_cnt;
         hr.surv = (uint32_t*)out_dev;
         hr.tile_bias = (uint32_t)off;
-        const uint64_t units = units_of(E, hr.n_words, hr.unit_words);
+        const uint64_t units = units_of(f, hr.n_words, hr.unit_words);
         uint64_t hpre[2] = {0, units};
         SweepHeader hh;
         memset(&hh, 0, sizeof(hh));
@@ -688,12 +761,12 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
         CU(cudaMemcpyAsync(d_range, &hr, sizeof(hr), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(d_prefix, hpre, sizeof(hpre), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(d_hdr, &hh, sizeof(hh), cudaMemcpyHostToDevice, st));
-        CU(launch_range_setup(d_range, d_hdr, 1, E->range_primes.p, np, d_jmod, np, st));
+        CU(launch_range_setup(d_range, d_hdr, 1, f.range_primes.p, np, d_jmod, np, st));
         uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
         const uint64_t need = (units + (kSweepThreads / 32) - 1) / (kSweepThreads / 32);
         if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
         CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, b_stride_of((uint32_t)hp.primesB.size()),
-                        grid, hp.std_a != 0, st));
+                        grid, st));
         E->launches += 2;
     }
     uint32_t cnt = 0;
@@ -742,10 +815,14 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     std::vector<uint32_t> allp;
     uint32_t maxnb = 0;
     for (auto* E : b->prof) {
-        b->prime_base.push_back((uint32_t)allp.size());
-        allp.insert(allp.end(), E->hp.range_primes.begin(), E->hp.range_primes.end());
-        b->max_range_primes = std::max<uint32_t>(b->max_range_primes, (uint32_t)E->hp.range_primes.size());
-        maxnb = std::max<uint32_t>(maxnb, (uint32_t)E->hp.primesB.size());
+        for (int v = 0; v < 2; v++) {
+            const HostProfile& hp = E->fs[v < E->n_fs ? v : 0].hp;
+            b->prime_base.push_back((uint32_t)allp.size());
+            if (v >= E->n_fs) continue;
+            allp.insert(allp.end(), hp.range_primes.begin(), hp.range_primes.end());
+            b->max_range_primes = std::max<uint32_t>(b->max_range_primes, (uint32_t)hp.range_primes.size());
+            maxnb = std::max<uint32_t>(maxnb, (uint32_t)hp.primesB.size());
+        }
     }
     b->b_stride = b_stride_of(maxnb);
     b->jstride = b->max_range_primes;
@@ -773,9 +850,7 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     CU(cudaEventCreate(&b->ev0));
     CU(cudaEventCreate(&b->ev1));
-    bool all_std = true;
-    for (auto* E : b->prof) all_std &= E->hp.std_a != 0;
-    int bps = sweep_blocks_per_sm(b->b_stride, all_std);
+    int bps = sweep_blocks_per_sm(b->b_stride);
     b->grid = (uint32_t)b->prof[0]->sms * (uint32_t)std::max(bps, 1);
 
     // record the whole batch once: H2D descriptors, setup, sweep, level C,
@@ -790,7 +865,7 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     launch_range_setup(b->d_ranges.p, b->d_hdr.p, max_ranges, b->d_primes.p, b->max_range_primes,
                        b->d_jmod.p, b->jstride, st);
     launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, b->b_stride,
-                 b->grid, all_std, st);
+                 b->grid, st);
     ProveArgs pa;
     pa.ranges = b->d_pranges.p;
     pa.surv = b->d_surv.p;
@@ -828,14 +903,8 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
         unsigned __int128 ts = mk128(rg.tile_start_lo, rg.tile_start_hi);
         RangeDev& R = b->h_ranges[i];
         memset(&R, 0, sizeof(R));
-        fill_J0(R.J0, ts / 6);
-        R.e0 = (uint32_t)(ts % 6);
-        R.n_tiles = (uint32_t)rg.n_tiles;
-        R.n_words = rg.n_tiles ? words_for(R.e0, rg.n_tiles) : 0;
-        R.unit_words = choose_unit_words(E, R.n_words);
-        R.profile = (uint32_t)E->slot;
-        R.prime_base = b->prime_base[rg.profile];
-        R.n_range_primes = (uint32_t)E->hp.range_primes.size();
+        const FilterSet& f = place_range(E, ts, rg.n_tiles, R);
+        R.prime_base = b->prime_base[2 * rg.profile + (&f == &E->fs[1] ? 1 : 0)];
         R.surv_cap = (uint32_t)b->surv_cap;
         R.surv_count = cnt;
         R.surv = b->d_surv.p;
@@ -851,7 +920,7 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
         P.chain_count = cnt + 4 + 3 * i + 1;
         P.prime_count = cnt + 4 + 3 * i + 2;
         b->h_prefix[i] = total;
-        total += R.n_words ? units_of(E, R.n_words, R.unit_words) : 0;
+        total += R.n_words ? units_of(f, R.n_words, R.unit_words) : 0;
     }
     b->h_prefix[n_ranges] = total;
     for (uint32_t i = n_ranges + 1; i <= b->max_ranges; i++) b->h_prefix[i] = total;

@@ -69,8 +69,12 @@ __global__ void range_setup_kernel(const RangeDev* __restrict__ ranges,
 // ---------------------------------------------------------------------------
 // survivor emission
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void emit_survivor(const RangeDev& R, const Line& ln, uint32_t j) {
-    uint32_t c = ln.bc >> 16;
+// p is the line's position (block index j on a plain profile; on an extended
+// profile j = q0 p + d - e1)
+__device__ __forceinline__ void emit_survivor(const RangeDev& R, const Line& ln, uint32_t p, uint32_t q0) {
+    const uint32_t c = (ln.bc >> 16) & 7u;
+    const uint32_t d = ln.bc >> 19;
+    const uint32_t j = q0 * p + d - R.e1;
     uint32_t slot = atomicAdd(R.surv_count, 1u);
     if (R.range_count) atomicAdd(R.range_count, 1u);
     if (slot < R.surv_cap) {
@@ -95,10 +99,13 @@ struct SweepArgs {
     uint32_t b_stride;             // level-B primes per lane column in shared memory
 };
 
-// standard level-A set (every prime 37..127): slots 0..6, 9..14, 15..21
-__device__ constexpr uint32_t kStdQ[kNumA] = {37, 41, 43, 47, 53, 59, 61, 1, 1,
-                                              67, 71, 73, 79, 83, 89,
-                                              97, 101, 103, 107, 109, 113, 127};
+// standard level-A sets: every prime 37..127 (STD = 1), and the same set
+// with 37 absorbed into an extended lattice (STD = 2)
+__device__ constexpr uint32_t kStdQ[3][kNumA] = {
+    {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
+    {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127},
+    {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127}};
+__device__ constexpr int kStdA1[3] = {kNumA1, 7, 6};
 
 constexpr int kQCap = 256;               // per-warp level-B queue (entries)
 constexpr int kCCap = 64;                // per-warp level-C list (entries)
@@ -164,7 +171,7 @@ __device__ __forceinline__ void c_process(LevelB& B, const SweepArgs& a, const R
             }
             killed = __any_sync(0xFFFFFFFFu, kill);
         }
-        if (!killed && lane == 0) emit_survivor(R, ln, j);
+        if (!killed && lane == 0) emit_survivor(R, ln, j, P.q0);
     }
     B.cnum = 0;
     __syncwarp();
@@ -200,7 +207,7 @@ __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const Ran
     const bool pass = B.cur != kNone && B.pi >= B.nB;
     if (P.nC == 0) {
         if (pass) {
-            emit_survivor(R, P.lines[g * 32 + (B.cur & 31u)], jbase + (B.cur >> 5));
+            emit_survivor(R, P.lines[g * 32 + (B.cur & 31u)], jbase + (B.cur >> 5), P.q0);
             B.cur = kNone;
         }
     } else {
@@ -214,49 +221,28 @@ __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const Ran
     }
 }
 
-template <bool STD>
-__global__ void __launch_bounds__(kSweepThreads)
-sweep_kernel(SweepArgs a) {
-    extern __shared__ uint32_t s_mem[];
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t lane_lt = (1u << lane) - 1u;
-    const uint32_t warp_in_block = threadIdx.x >> 5;
-    // per warp: level-B queue (kQCap u32), level-C list (kCCap u32), phases (b_stride * 32 u16)
-    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + kCCap + a.b_stride * 16);
-    uint32_t* Cw = Qw + kQCap;
-    uint16_t* S = reinterpret_cast<uint16_t*>(Cw + kCCap);
-    const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-
-    const uint32_t n_ranges = a.hdr->n_ranges;
-    const uint64_t total_units = a.hdr->total_units;
-    uint32_t cur_range = 0;
-    for (uint64_t u = gwarp; u < total_units; u += nwarps) {
-        if (u >= a.unit_prefix[cur_range + 1] || u < a.unit_prefix[cur_range]) {
-            uint32_t lo = 0, hi = n_ranges;                 // last prefix <= u
-            while (hi - lo > 1) {
-                uint32_t mid = (lo + hi) >> 1;
-                if (a.unit_prefix[mid] <= u) lo = mid; else hi = mid;
-            }
-            cur_range = lo;
-        }
-        const RangeDev& R = a.ranges[cur_range];
-        const ProfileConst& P = c_prof[R.profile];
+// One work unit: 32 lines of range cur_range, words [w0, w1).  STD selects
+// the level-A variant: 1 = primes 37..127, 2 = 41..127 (37 absorbed), 0 =
+// whatever the profile lists (shift amounts read from constant memory).
+template <int STD>
+__device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R, const ProfileConst& P,
+                                           uint32_t cur_range, uint32_t g, uint32_t w0, uint32_t w1,
+                                           uint32_t* Qw, uint32_t* Cw, uint16_t* S, uint32_t lane,
+                                           uint32_t lane_lt) {
         const uint32_t* jm = a.jmod + (uint64_t)cur_range * a.jmod_stride;
-        const uint64_t local = u - a.unit_prefix[cur_range];
-        const uint32_t n_groups = (P.n_lines + 31) >> 5;
-        const uint32_t g = (uint32_t)(local % n_groups);
-        const uint32_t wc = (uint32_t)(local / n_groups);
-        const uint32_t w0 = wc * R.unit_words;
-        const uint32_t w1 = min(w0 + R.unit_words, R.n_words);
-
         const uint32_t li = g * 32 + lane;
         const bool has_line = li < P.n_lines;
         const Line ln = has_line ? P.lines[li] : Line{0, 0, 0, 0};
-        const uint32_t c = ln.bc >> 16;
-        const uint32_t jlo = (c < R.e0) ? 1u : 0u;
+        const uint32_t c = (ln.bc >> 16) & 7u;
+        const uint32_t d = ln.bc >> 19;
+        const uint32_t q0 = P.q0;
+        // block range [jlo0, jhi0) of this line relative to floor(tile_start / 6)
+        const uint32_t jlo0 = (c < R.e0) ? 1u : 0u;
         const uint64_t endc = (uint64_t)R.e0 + R.n_tiles;
-        const uint32_t jhi = has_line && endc > c ? (uint32_t)((endc - c + 5) / 6) : 0u;
+        const uint64_t jhi0 = has_line && endc > c ? (endc - c + 5) / 6 : 0u;
+        // positions p with j = q0 p + d - e1 in that range
+        const uint32_t jlo = (jlo0 + R.e1 > d) ? (uint32_t)((jlo0 + R.e1 - d + q0 - 1) / q0) : 0u;
+        const uint32_t jhi = (jhi0 + R.e1 > d) ? (uint32_t)((jhi0 + R.e1 - d + q0 - 1) / q0) : 0u;
         const uint32_t jbase = w0 * 64;
 
         // ---- level A windows at block jbase ----
@@ -266,7 +252,7 @@ sweep_kernel(SweepArgs a) {
 #pragma unroll
         for (int i = 0; i < kNumA; i++) {
             const LevelA& la = P.A[i];
-            const uint32_t q = STD ? kStdQ[i] : la.q;
+            const uint32_t q = STD ? kStdQ[STD][i] : la.q;
             uint32_t ph = 0;
             if (q > 1) ph = phase_fast(ln.r_lo, ln.r_hi, q, la.magic, la.c32, la.winv, jm[i], jbase);
             uint32_t e[8];
@@ -311,8 +297,8 @@ sweep_kernel(SweepArgs a) {
             uint64_t kill = 0;
 #pragma unroll
             for (int i = 0; i < kNumA1; i++) {
-                if (STD && i >= 7) continue;                 // dummy slots of the standard set
-                const uint32_t q = STD ? kStdQ[i] : P.A[i].q;
+                if (STD && i >= kStdA1[STD]) continue;       // dummy slots of the standard sets
+                const uint32_t q = STD ? kStdQ[STD][i] : P.A[i].q;
                 const uint32_t s = STD ? (64u % q) : P.A[i].s;
                 const uint32_t t = STD ? (q - 64u % q) : P.A[i].t;
                 const uint64_t W = A1w[i];
@@ -321,7 +307,7 @@ sweep_kernel(SweepArgs a) {
             }
 #pragma unroll
             for (int i = 0; i < kNumA2; i++) {
-                const uint32_t t = STD ? (kStdQ[kNumA1 + i] - 64u) : P.A[kNumA1 + i].t;
+                const uint32_t t = STD ? (kStdQ[STD][kNumA1 + i] - 64u) : P.A[kNumA1 + i].t;
                 const uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
                 kill |= ((uint64_t)o1 << 32) | o0;
                 A2w[i][0] = o2 | (o0 << t);
@@ -330,7 +316,7 @@ sweep_kernel(SweepArgs a) {
             }
 #pragma unroll
             for (int i = 0; i < kNumA3; i++) {
-                const uint32_t t = STD ? (kStdQ[kNumA1 + kNumA2 + i] - 96u) : P.A[kNumA1 + kNumA2 + i].t;
+                const uint32_t t = STD ? (kStdQ[STD][kNumA1 + kNumA2 + i] - 96u) : P.A[kNumA1 + kNumA2 + i].t;
                 const uint32_t o0 = A3w[i][0], o1 = A3w[i][1], o2 = A3w[i][2], o3 = A3w[i][3];
                 kill |= ((uint64_t)o1 << 32) | o0;
                 A3w[i][0] = o2;
@@ -374,6 +360,44 @@ sweep_kernel(SweepArgs a) {
             b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
         if (B.cnum) c_process(B, a, R, P, cur_range, g, jbase, lane);
         __syncwarp();
+}
+
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_kernel(SweepArgs a) {
+    extern __shared__ uint32_t s_mem[];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lane_lt = (1u << lane) - 1u;
+    const uint32_t warp_in_block = threadIdx.x >> 5;
+    // per warp: level-B queue (kQCap u32), level-C list (kCCap u32), phases (b_stride * 32 u16)
+    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + kCCap + a.b_stride * 16);
+    uint32_t* Cw = Qw + kQCap;
+    uint16_t* S = reinterpret_cast<uint16_t*>(Cw + kCCap);
+    const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+
+    const uint32_t n_ranges = a.hdr->n_ranges;
+    const uint64_t total_units = a.hdr->total_units;
+    uint32_t cur_range = 0;
+    for (uint64_t u = gwarp; u < total_units; u += nwarps) {
+        if (u >= a.unit_prefix[cur_range + 1] || u < a.unit_prefix[cur_range]) {
+            uint32_t lo = 0, hi = n_ranges;                 // last prefix <= u
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (a.unit_prefix[mid] <= u) lo = mid; else hi = mid;
+            }
+            cur_range = lo;
+        }
+        const RangeDev& R = a.ranges[cur_range];
+        const ProfileConst& P = c_prof[R.profile];
+        const uint64_t local = u - a.unit_prefix[cur_range];
+        const uint32_t n_groups = (P.n_lines + 31) >> 5;
+        const uint32_t g = (uint32_t)(local % n_groups);
+        const uint32_t wc = (uint32_t)(local / n_groups);
+        const uint32_t w0 = wc * R.unit_words;
+        const uint32_t w1 = min(w0 + R.unit_words, R.n_words);
+        if (P.std_a == 1) sweep_unit<1>(a, R, P, cur_range, g, w0, w1, Qw, Cw, S, lane, lane_lt);
+        else if (P.std_a == 2) sweep_unit<2>(a, R, P, cur_range, g, w0, w1, Qw, Cw, S, lane, lane_lt);
+        else sweep_unit<0>(a, R, P, cur_range, g, w0, w1, Qw, Cw, S, lane, lane_lt);
     }
 }
 
@@ -407,28 +431,22 @@ static bool g_sweep_attr_set = false;
 static cudaError_t ensure_sweep_attr() {
     if (g_sweep_attr_set) return cudaSuccess;
     const int lim = (int)sweep_smem_bytes(kSweepThreads, kMaxLevelB);
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     if (e == cudaSuccess) g_sweep_attr_set = true;
     return e;
 }
 
-int sweep_blocks_per_sm(uint32_t b_stride, bool std_a) {
+int sweep_blocks_per_sm(uint32_t b_stride) {
     int nb = 0;
     if (ensure_sweep_attr() != cudaSuccess) return 0;
-    if (std_a)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<true>, kSweepThreads,
-                                                      sweep_smem_bytes(kSweepThreads, b_stride));
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel<false>, kSweepThreads,
-                                                      sweep_smem_bytes(kSweepThreads, b_stride));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel, kSweepThreads,
+                                                  sweep_smem_bytes(kSweepThreads, b_stride));
     return nb;
 }
 
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
-                         uint32_t b_stride, uint32_t grid, bool std_a, cudaStream_t st) {
+                         uint32_t b_stride, uint32_t grid, cudaStream_t st) {
     size_t smem = sweep_smem_bytes(kSweepThreads, b_stride);
     cudaError_t e = ensure_sweep_attr();
     if (e != cudaSuccess) return e;
@@ -439,8 +457,7 @@ cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
     a.jmod = jmod;
     a.jmod_stride = stride;
     a.b_stride = b_stride;
-    if (std_a) sweep_kernel<true><<<grid, kSweepThreads, smem, st>>>(a);
-    else sweep_kernel<false><<<grid, kSweepThreads, smem, st>>>(a);
+    sweep_kernel<<<grid, kSweepThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -63,7 +63,7 @@ static std::vector<uint32_t> forbidden_set(uint32_t q, uint32_t L, uint32_t pos_
     return std::vector<uint32_t>(s.begin(), s.end());
 }
 
-std::string build_profile(HostProfile& hp, uint32_t split_prime) {
+std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
     // ---- validation -------------------------------------------------------
     if (hp.crt.empty() || hp.wheel.empty()) return "crt and wheel prime lists must be non-empty";
     if (hp.target < 1 || hp.target > (uint32_t)kMaxChain) return "target out of range [1, 64]";
@@ -188,6 +188,35 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime) {
         hp.fprimes.push_back(fp);
     }
 
+    // ---- optional extension: absorb filter prime q0 into the modulus ------
+    hp.q0 = 1;
+    if (q0 > 1) {
+        const HostProfile::FPrime* fq = nullptr;
+        for (auto& fp : hp.fprimes)
+            if (fp.q == q0) fq = &fp;
+        if (!fq) return "extension prime is not a filter prime";
+        if ((unsigned __int128)hp.W * q0 >= ((unsigned __int128)1 << 62)) return "extended modulus too large";
+        std::vector<Line> ext;
+        ext.reserve(hp.lines.size() * (q0 - fq->forb.size()));
+        for (const Line& ln : hp.lines) {
+            const uint64_t r = ((uint64_t)ln.r_hi << 32) | ln.r_lo;
+            for (uint32_t d = 0; d < q0; d++) {
+                const uint64_t r2 = r + (uint64_t)d * hp.W;
+                if (std::binary_search(fq->forb.begin(), fq->forb.end(), (uint32_t)(r2 % q0))) continue;
+                Line e;
+                e.r_lo = (uint32_t)r2;
+                e.r_hi = (uint32_t)(r2 >> 32);
+                e.k = ln.k;
+                e.bc = ln.bc | (d << 19);
+                ext.push_back(e);
+            }
+        }
+        if (ext.size() >= (1ull << 31)) return "too many extended lines";
+        hp.lines.swap(ext);
+        hp.W *= q0;
+        hp.q0 = q0;
+    }
+
     // ---- level classification ----------------------------------------------
     memset(hp.A, 0, sizeof(hp.A));
     for (int i = 0; i < kNumA; i++) hp.A[i].q = 1;      // dummy: no kills
@@ -196,6 +225,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime) {
     const uint64_t Wm = hp.W;
     for (auto& fp : hp.fprimes) {
         uint32_t q = fp.q;
+        if (q == hp.q0) continue;                       // absorbed into the lattice
         uint32_t winv = mod_inverse_u32((uint32_t)(Wm % q), q);
         std::vector<uint32_t> g;
         for (uint32_t f : fp.forb) g.push_back((uint32_t)((uint64_t)f * winv % q));
@@ -246,12 +276,15 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime) {
     // the standard level-A set (every prime 37..127) has a kernel with
     // compile-time shift amounts
     {
-        static const uint32_t std_q[kNumA] = {37, 41, 43, 47, 53, 59, 61, 1, 1,
-                                              67, 71, 73, 79, 83, 89,
-                                              97, 101, 103, 107, 109, 113, 127};
-        hp.std_a = 1;
-        for (int i = 0; i < kNumA; i++)
-            if (hp.A[i].q != std_q[i]) hp.std_a = 0;
+        static const uint32_t std_q[2][kNumA] = {
+            {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127},
+            {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127}};
+        hp.std_a = 0;
+        for (int v = 0; v < 2; v++) {
+            bool same = true;
+            for (int i = 0; i < kNumA; i++) same &= hp.A[i].q == std_q[v][i];
+            if (same) hp.std_a = 1 + v;
+        }
     }
     hp.range_primes.clear();
     for (int i = 0; i < kNumA; i++) hp.range_primes.push_back(hp.A[i].q);

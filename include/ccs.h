@@ -291,6 +291,12 @@ typedef struct {
     uint32_t blocks_per_sm;   /* resident blocks requested per SM */
     uint32_t unit_words;      /* 64-candidate words per lane per work unit */
     uint32_t split_prime;     /* first prime tested by the deferred warp-cooperative stage */
+    uint32_t ext_min_words;   /* ranges spanning at least this many 64-position words of
+                               * the extended lattice (smallest bit-sliced filter prime
+                               * absorbed into the modulus) are swept on it; 1 = every
+                               * range, 0xFFFFFFFF = none.  Both lattices give identical
+                               * survivors. */
+    uint32_t _pad;
 } ccs_tuning;
 
 ccs_status ccs_get_tuning(const ccs_engine* eng, ccs_tuning* out);

@@ -116,6 +116,47 @@ def test_cpu_method_lattice_matches_oracle(ccs, ob):
     eng.close()
 
 
+@pytest.mark.parametrize("profile", ["reference", "cc16", "cpu_method"])
+def test_extended_lattice_matches_oracle(ccs, ob, profile):
+    """With ext_min_words = 1 every range is swept on the extended lattice
+    (smallest bit-sliced prime absorbed into the modulus); survivors must
+    still equal the oracle's in the reference's (base, k, tile) coordinates,
+    for every tile_start phase mod 6 and mod q0."""
+    if profile == "reference":
+        cfg, lat = {}, ob.Lattice()
+    elif profile == "cc16":
+        cfg = ccs.config_cc16_scale()
+        lat = ob.Lattice(lattice_len=16, depth=16, stages=cfg["stages"])
+    else:
+        cfg = ccs.config_cpu_method()
+        lat = ob.Lattice(wheel=[23], lattice_len=8, depth=8, stages=cfg["stages"])
+    eng = ccs.Engine(**cfg)
+    eng.set_tuning(ext_min_words=1)
+    r = random.Random(sum(map(ord, profile)))
+    reps = 1 if profile == "cc16" else 3          # the cc16 oracle needs ~7 ms per tile
+    for n in (1, 5, 6, 7, 223, 1300):
+        for _ in range(reps):
+            ts = r.randint(1 << 40, 1 << 62)
+            want = as_set(lat.filter_range(ts, n))
+            got = as_set(eng.filter_range(ts, n, cap=1 << 20))
+            assert got == want, (profile, ts, n)
+    eng.close()
+
+
+def test_extended_equals_plain_at_scale(ccs):
+    """The plain and the extended lattice give the same survivor set over
+    10^6 tiles (~7.3e10 candidates of the depth-16 profile)."""
+    eng = ccs.Engine(**ccs.config_cc16_scale())
+    ts = (1 << 87) // (1616615 * 20677) + 1234567
+    n = 1_000_000
+    eng.set_tuning(ext_min_words=0xFFFFFFFF)
+    plain = as_set(eng.filter_range(ts, n, cap=1 << 20))
+    eng.set_tuning(ext_min_words=1)
+    ext = as_set(eng.filter_range(ts, n, cap=1 << 20))
+    assert len(plain) > 100 and plain == ext
+    eng.close()
+
+
 def test_split_range_additivity_at_scale(ccs):
     """Filtering [T, T+N) equals filtering [T, T+a) and [T+a, T+N) with tile
     offsets shifted: an exact property checked at ~1.5e10 candidates."""
