@@ -28,6 +28,7 @@ constexpr int kNumA3 = 7;              // bit-sliced primes 96 < q < 128 (128-bi
 constexpr int kNumA = kNumA1 + kNumA2 + kNumA3;
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
+constexpr int kLevelBRound = 4;        // level-B primes tested per lane per round
 
 // One bit-sliced ("level A") prime: the 64-candidate kill window is advanced
 // by two shifts per 64 blocks (see filter.cu).
@@ -76,7 +77,7 @@ struct ProfileConst {
     uint32_t _q0pad;
     uint32_t n_lines;
     uint32_t nB, nC;                 // counts of per-candidate primes
-    uint32_t c32W_dummy;
+    uint32_t nBpad;                  // nB rounded up with never-killing dummies (packB length)
     LevelA A[kNumA];
     const Line* lines;
     const PrimeC* primesB;           // level B primes (ascending)

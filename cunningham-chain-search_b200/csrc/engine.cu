@@ -203,6 +203,7 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     pc.q0 = hp.q0;
     pc.n_lines = (uint32_t)hp.lines.size();
     pc.nB = (uint32_t)hp.primesB.size();
+    pc.nBpad = (uint32_t)hp.packB.size();
     pc.nC = (uint32_t)hp.primesC.size();
     memcpy(pc.A, hp.A, sizeof(pc.A));
     pc.lines = f.lines.p;

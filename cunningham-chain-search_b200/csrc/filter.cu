@@ -36,13 +36,6 @@ __device__ __forceinline__ uint32_t mod_magic64(uint64_t x, uint32_t q, uint64_t
     return (uint32_t)t;
 }
 
-__device__ __forceinline__ uint32_t sel8(const uint32_t (&e)[8], uint32_t idx) {
-    uint32_t v = 0;
-#pragma unroll
-    for (int x = 0; x < 8; x++) v = (idx == (uint32_t)x) ? e[x] : v;
-    return v;
-}
-
 // ---------------------------------------------------------------------------
 // per-range J0 mod q tables (replaces the host u128 prepare_batch)
 // ---------------------------------------------------------------------------
@@ -107,9 +100,14 @@ __device__ constexpr uint32_t kStdQ[3][kNumA] = {
     {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127}};
 __device__ constexpr int kStdA1[3] = {kNumA1, 7, 6};
 
-constexpr int kQCap = 256;               // per-warp level-B queue (entries)
+constexpr int kQCap = 512;               // per-warp level-B queue (entries, power of two)
+constexpr uint32_t kQLow = 96;           // level-B rounds run until at most this many are queued
 constexpr int kCCap = 64;                // per-warp level-C list (entries)
+constexpr int kBK = kLevelBRound;        // level-B primes tested per lane per round
+constexpr int kPAWords = kNumA * 8;      // per-warp copy of the level-A patterns (u32)
+constexpr int kSAWords = kNumA * 16;     // per-warp level-A phases, [kNumA][32] u16
 constexpr uint32_t kNone = 0xFFFFFFFFu;  // empty lane slot
+constexpr uint32_t kFull = 0xFFFFFFFFu;
 
 // x mod q for x < 2^32 via the profile's magic (fast init-time reductions)
 __device__ __forceinline__ uint32_t phase_fast(uint32_t rl, uint32_t rh, uint32_t q, uint32_t magic,
@@ -123,7 +121,7 @@ __device__ __forceinline__ uint32_t phase_fast(uint32_t rl, uint32_t rh, uint32_
     return v >= q ? v - q : v;
 }
 
-// Per-warp level-B machinery: a queue of (lane line, block offset) entries in
+// Per-warp level-B machinery: a queue of (block offset, line lane) entries in
 // shared memory and one candidate per lane, refilled whenever a lane's
 // candidate is decided, so lanes stay busy whichever line produced the work.
 struct LevelB {
@@ -133,7 +131,7 @@ struct LevelB {
     const uint16_t* S;             // [nB][32] phases of the unit's 32 lines at jbase
     const PrimeB* pb;
     const uint32_t* bm;
-    uint32_t nB;
+    uint32_t nB;                   // level-B primes, padded to a multiple of kBK
     uint32_t head, tail;           // warp-uniform
     uint32_t cur, pi;              // this lane's candidate and next prime index
 };
@@ -169,7 +167,7 @@ __device__ __forceinline__ void c_process(LevelB& B, const SweepArgs& a, const R
                 }
                 kill = lo < pc.cnt && __ldg(lst + lo) == uph;
             }
-            killed = __any_sync(0xFFFFFFFFu, kill);
+            killed = __any_sync(kFull, kill);
         }
         if (!killed && lane == 0) emit_survivor(R, ln, j, P.q0);
     }
@@ -177,31 +175,34 @@ __device__ __forceinline__ void c_process(LevelB& B, const SweepArgs& a, const R
     __syncwarp();
 }
 
-// one round: refill empty lanes from the queue, then test two primes
+// One round: refill empty lanes from the queue, then test kBK primes of each
+// lane's candidate.  The kBK tests are independent (their loads and
+// reductions overlap); a candidate killed by any of them is dropped, so the
+// outcome equals the one-prime-at-a-time test.
 __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const RangeDev& R,
                                         const ProfileConst& P, uint32_t cur_range, uint32_t g,
                                         uint32_t jbase, uint32_t lane_lt) {
     const bool needy = B.cur == kNone;
-    const uint32_t nm = __ballot_sync(0xFFFFFFFFu, needy);
+    const uint32_t nm = __ballot_sync(kFull, needy);
     const uint32_t avail = B.tail - B.head;
     if (needy) {
         const uint32_t rk = __popc(nm & lane_lt);
         if (rk < avail) { B.cur = B.Q[(B.head + rk) & (kQCap - 1)]; B.pi = 0; }
     }
     B.head += min((uint32_t)__popc(nm), avail);
-    if (B.cur != kNone) {
+    if (B.cur != kNone && B.pi < B.nB) {
         const uint32_t L = B.cur & 31u, jrel = B.cur >> 5;
+        uint32_t hit = 0;
 #pragma unroll
-        for (int t = 0; t < 2; t++) {
-            if (B.cur != kNone && B.pi < B.nB) {
-                const uint2 pr2 = __ldg(reinterpret_cast<const uint2*>(B.pb) + B.pi);
-                const PrimeB pr{pr2.x, pr2.y};
-                const uint32_t q = pr.q_off & 0xFFFFu;
-                const uint32_t u = mod_magic((uint32_t)B.S[B.pi * 32 + L] + jrel, q, pr.magic);
-                const uint32_t wv = __ldg(B.bm + (pr.q_off >> 16) + (u >> 5));
-                if ((wv >> (u & 31)) & 1u) B.cur = kNone; else B.pi++;
-            }
+        for (int t = 0; t < kBK; t++) {
+            const uint32_t idx = B.pi + t;
+            const uint2 pr = __ldg(reinterpret_cast<const uint2*>(B.pb) + idx);
+            const uint32_t q = pr.y & 0xFFFFu;
+            const uint32_t u = mod_magic((uint32_t)B.S[idx * 32 + L] + jrel, q, pr.x);
+            const uint32_t wv = __ldg(B.bm + (pr.y >> 16) + (u >> 5));
+            hit |= wv >> (u & 31);
         }
+        if (hit & 1u) B.cur = kNone; else B.pi += kBK;
     }
     // candidates that passed every level-B prime
     const bool pass = B.cur != kNone && B.pi >= B.nB;
@@ -211,7 +212,7 @@ __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const Ran
             B.cur = kNone;
         }
     } else {
-        const uint32_t pm = __ballot_sync(0xFFFFFFFFu, pass);
+        const uint32_t pm = __ballot_sync(kFull, pass);
         if (pass) {
             B.Cl[B.cnum + __popc(pm & lane_lt)] = B.cur;
             B.cur = kNone;
@@ -224,11 +225,18 @@ __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const Ran
 // One work unit: 32 lines of range cur_range, words [w0, w1).  STD selects
 // the level-A variant: 1 = primes 37..127, 2 = 41..127 (37 absorbed), 0 =
 // whatever the profile lists (shift amounts read from constant memory).
+//
+// The unit alternates two phases.  Level A sweeps words with the kill
+// windows in registers and queues the surviving positions until the queue is
+// full; level B then runs rounds until the queue is nearly empty.  The
+// windows are rebuilt from the per-lane phases at the start of every level-A
+// phase, so they are dead while level B runs and its independent tests have
+// the registers.
 template <int STD>
 __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R, const ProfileConst& P,
                                            uint32_t cur_range, uint32_t g, uint32_t w0, uint32_t w1,
-                                           uint32_t* Qw, uint32_t* Cw, uint16_t* S, uint32_t lane,
-                                           uint32_t lane_lt) {
+                                           uint32_t* Qw, uint32_t* Cw, uint32_t* PA, uint16_t* SA,
+                                           uint16_t* S, uint32_t lane, uint32_t lane_lt) {
         const uint32_t* jm = a.jmod + (uint64_t)cur_range * a.jmod_stride;
         const uint32_t li = g * 32 + lane;
         const bool has_line = li < P.n_lines;
@@ -245,35 +253,24 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         const uint32_t jhi = (jhi0 + R.e1 > d) ? (uint32_t)((jhi0 + R.e1 - d + q0 - 1) / q0) : 0u;
         const uint32_t jbase = w0 * 64;
 
-        // ---- level A windows at block jbase ----
-        uint64_t A1w[kNumA1];
-        uint32_t A2w[kNumA2][3];
-        uint32_t A3w[kNumA3][4];
+        // ---- per-warp pattern copy, per-lane phases at block jbase ----
+        for (uint32_t x = lane; x < (uint32_t)kPAWords; x += 32) PA[x] = P.A[x >> 3].ext[x & 7];
 #pragma unroll
         for (int i = 0; i < kNumA; i++) {
             const LevelA& la = P.A[i];
             const uint32_t q = STD ? kStdQ[STD][i] : la.q;
             uint32_t ph = 0;
             if (q > 1) ph = phase_fast(ln.r_lo, ln.r_hi, q, la.magic, la.c32, la.winv, jm[i], jbase);
-            uint32_t e[8];
-#pragma unroll
-            for (int m = 0; m < 8; m++) e[m] = la.ext[m];
-            const uint32_t aw = ph >> 5, b = ph & 31;
-            uint32_t wds[4];
-#pragma unroll
-            for (int m = 0; m < 4; m++)
-                wds[m] = __funnelshift_r(sel8(e, aw + m), sel8(e, aw + m + 1), b);
-            if (i < kNumA1) {
-                A1w[i] = ((uint64_t)wds[1] << 32) | wds[0];
-            } else if (i < kNumA1 + kNumA2) {
-#pragma unroll
-                for (int m = 0; m < 3; m++) A2w[i - kNumA1][m] = wds[m];
-            } else {
-#pragma unroll
-                for (int m = 0; m < 4; m++) A3w[i - kNumA1 - kNumA2][m] = wds[m];
-            }
+            SA[i * 32 + lane] = (uint16_t)ph;
         }
-        // ---- level B phases at block jbase, one column per line ----
+        for (uint32_t p = 0; p < P.nBpad; p++) {
+            uint32_t ph = 0;
+            if (p < P.nB) {
+                const PrimeC pc = P.primesB[p];
+                ph = phase_fast(ln.r_lo, ln.r_hi, pc.q, pc.magic, pc.c32, pc.winv, jm[kNumA + p], jbase);
+            }
+            S[p * 32 + lane] = (uint16_t)ph;
+        }
         LevelB B;
         B.Q = Qw;
         B.Cl = Cw;
@@ -281,82 +278,124 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         B.S = S;
         B.pb = P.packB;
         B.bm = P.bitmapB;
-        B.nB = P.nB;
+        B.nB = P.nBpad;
         B.head = 0;
         B.tail = 0;
         B.cur = kNone;
         B.pi = 0;
-        for (uint32_t p = 0; p < B.nB; p++) {
-            const PrimeC pc = P.primesB[p];
-            S[p * 32 + lane] = (uint16_t)phase_fast(ln.r_lo, ln.r_hi, pc.q, pc.magic, pc.c32, pc.winv,
-                                                    jm[kNumA + p], jbase);
-        }
         __syncwarp();
 
-        for (uint32_t w = w0; w < w1; w++) {
-            uint64_t kill = 0;
+        uint64_t mrem = 0;          // positions of word wbm not yet queued
+        uint32_t wbm = 0;
+        uint32_t w = w0;            // next word to sweep
+        for (;;) {
+            // ---- level A: windows at word w ----
+            uint64_t A1w[kNumA1];
+            uint32_t A2w[kNumA2][3];
+            uint32_t A3w[kNumA3][4];
+            const uint32_t off = (w - w0) * 64;
 #pragma unroll
-            for (int i = 0; i < kNumA1; i++) {
-                if (STD && i >= kStdA1[STD]) continue;       // dummy slots of the standard sets
+            for (int i = 0; i < kNumA; i++) {
                 const uint32_t q = STD ? kStdQ[STD][i] : P.A[i].q;
-                const uint32_t s = STD ? (64u % q) : P.A[i].s;
-                const uint32_t t = STD ? (q - 64u % q) : P.A[i].t;
-                const uint64_t W = A1w[i];
-                kill |= W;
-                A1w[i] = (W >> s) | (W << t);
-            }
+                uint32_t ph = (uint32_t)SA[i * 32 + lane] + off;
+                if (STD) ph = q > 1 ? ph % q : 0;
+                else ph = mod_magic(ph, q, P.A[i].magic);
+                const uint32_t* pa = PA + i * 8 + (ph >> 5);
+                const uint32_t b = ph & 31;
+                if (i < kNumA1) {
+                    A1w[i] = ((uint64_t)__funnelshift_r(pa[1], pa[2], b) << 32) | __funnelshift_r(pa[0], pa[1], b);
+                } else if (i < kNumA1 + kNumA2) {
 #pragma unroll
-            for (int i = 0; i < kNumA2; i++) {
-                const uint32_t t = STD ? (kStdQ[STD][kNumA1 + i] - 64u) : P.A[kNumA1 + i].t;
-                const uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
-                kill |= ((uint64_t)o1 << 32) | o0;
-                A2w[i][0] = o2 | (o0 << t);
-                A2w[i][1] = __funnelshift_l(o0, o1, t);
-                A2w[i][2] = __funnelshift_l(o1, o2, t);
-            }
+                    for (int m = 0; m < 3; m++) A2w[i - kNumA1][m] = __funnelshift_r(pa[m], pa[m + 1], b);
+                } else {
 #pragma unroll
-            for (int i = 0; i < kNumA3; i++) {
-                const uint32_t t = STD ? (kStdQ[STD][kNumA1 + kNumA2 + i] - 96u) : P.A[kNumA1 + kNumA2 + i].t;
-                const uint32_t o0 = A3w[i][0], o1 = A3w[i][1], o2 = A3w[i][2], o3 = A3w[i][3];
-                kill |= ((uint64_t)o1 << 32) | o0;
-                A3w[i][0] = o2;
-                A3w[i][1] = o3 | (o0 << t);
-                A3w[i][2] = __funnelshift_l(o0, o1, t);
-                A3w[i][3] = __funnelshift_l(o1, o2, t);
+                    for (int m = 0; m < 4; m++) A3w[i - kNumA1 - kNumA2][m] = __funnelshift_r(pa[m], pa[m + 1], b);
+                }
             }
-            // positions of this word inside [jlo, jhi)
-            const uint32_t wb = w * 64;
-            uint64_t valid = 0;
-            if (jhi > wb && jlo < wb + 64) {
-                const uint32_t lo = jlo > wb ? jlo - wb : 0;
-                const uint32_t hi = jhi - wb < 64 ? jhi - wb : 64;
-                valid = (hi >= 64 ? ~0ull : ((1ull << hi) - 1)) & ~((1ull << lo) - 1);
-            }
-            uint64_t m = ~kill & valid;
-            // push this lane's survivors into the warp queue
             for (;;) {
-                const bool has = m != 0;
-                const uint32_t bmask = __ballot_sync(0xFFFFFFFFu, has);
-                if (!bmask) break;
-                const uint32_t n = __popc(bmask);
-                if (n > (uint32_t)kQCap - (B.tail - B.head)) {
-                    __syncwarp();
-                    b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
-                    continue;
+                if (!__any_sync(kFull, mrem != 0)) {
+                    if (w >= w1) break;
+                    uint64_t kill = 0;
+#pragma unroll
+                    for (int i = 0; i < kNumA1; i++) {
+                        if (STD && i >= kStdA1[STD]) continue;       // dummy slots of the standard sets
+                        const uint32_t q = STD ? kStdQ[STD][i] : P.A[i].q;
+                        const uint32_t s = STD ? (64u % q) : P.A[i].s;
+                        const uint32_t t = STD ? (q - 64u % q) : P.A[i].t;
+                        const uint64_t W = A1w[i];
+                        kill |= W;
+                        A1w[i] = (W >> s) | (W << t);
+                    }
+#pragma unroll
+                    for (int i = 0; i < kNumA2; i++) {
+                        const uint32_t t = STD ? (kStdQ[STD][kNumA1 + i] - 64u) : P.A[kNumA1 + i].t;
+                        const uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
+                        kill |= ((uint64_t)o1 << 32) | o0;
+                        A2w[i][0] = o2 | (o0 << t);
+                        A2w[i][1] = __funnelshift_l(o0, o1, t);
+                        A2w[i][2] = __funnelshift_l(o1, o2, t);
+                    }
+#pragma unroll
+                    for (int i = 0; i < kNumA3; i++) {
+                        const uint32_t t = STD ? (kStdQ[STD][kNumA1 + kNumA2 + i] - 96u)
+                                               : P.A[kNumA1 + kNumA2 + i].t;
+                        const uint32_t o0 = A3w[i][0], o1 = A3w[i][1], o2 = A3w[i][2], o3 = A3w[i][3];
+                        kill |= ((uint64_t)o1 << 32) | o0;
+                        A3w[i][0] = o2;
+                        A3w[i][1] = o3 | (o0 << t);
+                        A3w[i][2] = __funnelshift_l(o0, o1, t);
+                        A3w[i][3] = __funnelshift_l(o1, o2, t);
+                    }
+                    // positions of this word inside [jlo, jhi)
+                    const uint32_t wb = w * 64;
+                    uint64_t valid = 0;
+                    if (jhi > wb && jlo < wb + 64) {
+                        const uint32_t lo = jlo > wb ? jlo - wb : 0;
+                        const uint32_t hi = jhi - wb < 64 ? jhi - wb : 64;
+                        valid = (hi >= 64 ? ~0ull : ((1ull << hi) - 1)) & ~((1ull << lo) - 1);
+                    }
+                    mrem = ~kill & valid;
+                    wbm = wb - jbase;
+                    w++;
                 }
-                if (has) {
-                    const uint32_t rk = __popc(bmask & lane_lt);
-                    const uint32_t bit = __ffsll((long long)m) - 1;
-                    m &= m - 1;
-                    B.Q[(B.tail + rk) & (kQCap - 1)] = ((wb + bit - jbase) << 5) | lane;
+                // queue this lane's survivors: warp prefix sum of the counts
+                const uint32_t cnt = __popcll(mrem);
+                uint32_t incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= (uint32_t)o) incl += v;
                 }
-                B.tail += n;
+                const uint32_t total = __shfl_sync(kFull, incl, 31);
+                const uint32_t room = (uint32_t)kQCap - (B.tail - B.head);
+                if (total <= room) {
+                    uint32_t pos = B.tail + incl - cnt;
+                    while (mrem) {
+                        const uint32_t bit = __ffsll((long long)mrem) - 1;
+                        mrem &= mrem - 1;
+                        B.Q[pos++ & (kQCap - 1)] = ((wbm + bit) << 5) | lane;
+                    }
+                    B.tail += total;
+                } else {
+                    // fill the remaining room in warp order, keep the rest
+                    uint32_t pos = incl - cnt;
+                    while (mrem && pos < room) {
+                        const uint32_t bit = __ffsll((long long)mrem) - 1;
+                        mrem &= mrem - 1;
+                        B.Q[(B.tail + pos) & (kQCap - 1)] = ((wbm + bit) << 5) | lane;
+                        pos++;
+                    }
+                    B.tail += room;
+                    break;
+                }
             }
             __syncwarp();
-            while (B.tail - B.head >= 32) b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
+            if (w >= w1 && !__any_sync(kFull, mrem != 0)) break;
+            // ---- level B until the queue has room again ----
+            while (B.tail - B.head > kQLow) b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
         }
         // drain before the unit's phases are replaced
-        while (__any_sync(0xFFFFFFFFu, B.cur != kNone) || B.tail != B.head)
+        while (__any_sync(kFull, B.cur != kNone) || B.tail != B.head)
             b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
         if (B.cnum) c_process(B, a, R, P, cur_range, g, jbase, lane);
         __syncwarp();
@@ -368,10 +407,14 @@ sweep_kernel(SweepArgs a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lane_lt = (1u << lane) - 1u;
     const uint32_t warp_in_block = threadIdx.x >> 5;
-    // per warp: level-B queue (kQCap u32), level-C list (kCCap u32), phases (b_stride * 32 u16)
-    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + kCCap + a.b_stride * 16);
+    // per warp: level-B queue (kQCap u32), level-C list (kCCap u32), level-A
+    // patterns (kPAWords u32), level-A phases (kNumA * 32 u16), level-B
+    // phases (b_stride * 32 u16)
+    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + kCCap + kPAWords + kSAWords + a.b_stride * 16);
     uint32_t* Cw = Qw + kQCap;
-    uint16_t* S = reinterpret_cast<uint16_t*>(Cw + kCCap);
+    uint32_t* PA = Cw + kCCap;
+    uint16_t* SA = reinterpret_cast<uint16_t*>(PA + kPAWords);
+    uint16_t* S = reinterpret_cast<uint16_t*>(PA + kPAWords + kSAWords);
     const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
@@ -395,9 +438,9 @@ sweep_kernel(SweepArgs a) {
         const uint32_t wc = (uint32_t)(local / n_groups);
         const uint32_t w0 = wc * R.unit_words;
         const uint32_t w1 = min(w0 + R.unit_words, R.n_words);
-        if (P.std_a == 1) sweep_unit<1>(a, R, P, cur_range, g, w0, w1, Qw, Cw, S, lane, lane_lt);
-        else if (P.std_a == 2) sweep_unit<2>(a, R, P, cur_range, g, w0, w1, Qw, Cw, S, lane, lane_lt);
-        else sweep_unit<0>(a, R, P, cur_range, g, w0, w1, Qw, Cw, S, lane, lane_lt);
+        if (P.std_a == 1) sweep_unit<1>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt);
+        else if (P.std_a == 2) sweep_unit<2>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt);
+        else sweep_unit<0>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt);
     }
 }
 
@@ -421,7 +464,8 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
 }
 
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride) {
-    return (size_t)(block_threads / 32) * (kQCap + kCCap + (size_t)b_stride * 16) * sizeof(uint32_t);
+    return (size_t)(block_threads / 32) * (kQCap + kCCap + kPAWords + kSAWords + (size_t)b_stride * 16) *
+           sizeof(uint32_t);
 }
 
 static bool g_sweep_attr_set = false;

@@ -273,6 +273,19 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             hp.primesC.push_back(pc);
         }
     }
+    // pad the level-B records to a multiple of the per-round test count with
+    // entries that never kill (q = 2, all-zero bitmap word)
+    if (!hp.packB.empty() && hp.packB.size() % kLevelBRound) {
+        if (hp.bitmapB.size() >= 65536) return "level-B bitmaps too large";
+        const uint32_t zero_off = (uint32_t)hp.bitmapB.size();
+        hp.bitmapB.push_back(0);
+        while (hp.packB.size() % kLevelBRound) {
+            PrimeB pb;
+            pb.magic = 0xFFFFFFFFu / 2;
+            pb.q_off = 2u | (zero_off << 16);
+            hp.packB.push_back(pb);
+        }
+    }
     // the standard level-A set (every prime 37..127) has a kernel with
     // compile-time shift amounts
     {
