@@ -22,25 +22,36 @@ constexpr int kMaxStages = 4;
 constexpr int kMaxChain = 64;          // v13:164 MAX_CHAIN
 constexpr int kMaxDepth = 32;          // v13:159 MAX_SIEVE_CHAIN_LEN
 constexpr int kMaxLimbs = 6;           // 192-bit chain members
-constexpr int kNumA1 = 9;              // bit-sliced primes q < 64
-constexpr int kNumA2 = 6;              // bit-sliced primes 64 < q < 96 (96-bit windows)
-constexpr int kNumA3 = 7;              // bit-sliced primes 96 < q < 128 (128-bit windows)
-constexpr int kNumA = kNumA1 + kNumA2 + kNumA3;
+constexpr int kNumA1 = 9;              // bit-sliced primes q < 64 (64-bit register windows)
+constexpr int kNumA2 = 6;              // bit-sliced primes 64 < q < 96 (96-bit register windows)
+constexpr int kNumT = 22;              // bit-sliced primes 96 < q < kTLimit (table windows)
+constexpr int kNumAR = kNumA1 + kNumA2;
+constexpr int kNumA = kNumAR + kNumT;  // level-A slots
+constexpr uint32_t kTLimit = 211;
+constexpr int kPatTMax = 224;          // pattern-table words of the table-window primes
+constexpr double kTAdmit = 0.18;       // table-window admission (level-A survivors per 64 positions)
+
+// Pattern words of a table-window prime: a 64-bit window at any phase < q
+// lies inside them.
+constexpr uint32_t t_words(uint32_t q) { return (q - 1) / 32 + 3; }
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
 constexpr int kLevelBRound = 4;        // level-B primes tested per lane per round
 
-// One bit-sliced ("level A") prime: the 64-candidate kill window is advanced
-// by two shifts per 64 blocks (see filter.cu).
+// One bit-sliced ("level A") prime.  Register-window primes (A1, A2) keep
+// their 64/96-bit kill window in registers and advance it by shifts per 64
+// blocks; table-window primes (T) keep only their phase and read the window
+// from a replicated pattern table in shared memory (see filter.cu).
 struct LevelA {
-    uint32_t q;
-    uint32_t s;          // A1: 64 mod q          A2/A3: unused
-    uint32_t t;          // A1: q - s             A2: q - 64   A3: q - 96
+    uint32_t q;          // 1: dummy slot (no kills)
+    uint32_t s;          // A1: 64 mod q          A2, T: unused
+    uint32_t t;          // A1: q - s             A2: q - 64    T: unused
     uint32_t winv;       // W^{-1} mod q
     uint32_t magic;      // floor(2^32 / q)
     uint32_t c32;        // 2^32 mod q
-    uint32_t _pad[2];
-    uint32_t ext[8];     // 256 bits: bit x = [x mod q in G_q]; all zero = dummy
+    uint32_t toff;       // T: first word of the pattern in the table
+    uint32_t tnw;        // T: pattern words, t_words(q)
+    uint32_t ext[8];     // A1, A2: 256 bits, bit x = [x mod q in G_q]; all zero = dummy
 };
 
 // Level-B prime record read per candidate test: x = floor(2^32/q),
@@ -78,7 +89,9 @@ struct ProfileConst {
     uint32_t n_lines;
     uint32_t nB, nC;                 // counts of per-candidate primes
     uint32_t nBpad;                  // nB rounded up with never-killing dummies (packB length)
-    LevelA A[kNumA];
+    LevelA A[kNumA];                 // A1 slots, A2 slots, T slots
+    const uint32_t* patT;            // T pattern table (patT_words u32)
+    uint32_t patT_words;
     const Line* lines;
     const PrimeC* primesB;           // level B primes (ascending)
     const PrimeB* packB;             // compact level B records for the per-candidate test
@@ -116,6 +129,7 @@ struct HostProfile {
 
     // device-facing tables
     LevelA A[kNumA];
+    std::vector<uint32_t> patT;      // T pattern table: bit x of a prime's block = [x mod q in G_q]
     std::vector<PrimeC> primesB, primesC;
     std::vector<PrimeB> packB;
     uint32_t std_a = 0;

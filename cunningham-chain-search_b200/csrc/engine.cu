@@ -82,10 +82,10 @@ struct FilterSet {
     DevBuf<Line> lines;
     DevBuf<PrimeC> primesB, primesC;
     DevBuf<PrimeB> packB;
-    DevBuf<uint32_t> bitmapB, listC, range_primes;
+    DevBuf<uint32_t> bitmapB, listC, range_primes, patT;
     void free_() {
         lines.free_(); primesB.free_(); primesC.free_(); packB.free_();
-        bitmapB.free_(); listC.free_(); range_primes.free_();
+        bitmapB.free_(); listC.free_(); range_primes.free_(); patT.free_();
     }
 };
 
@@ -194,6 +194,8 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     CU(f.listC.alloc(hp.listC.size()));
     if (!hp.listC.empty())
         CU(cudaMemcpy(f.listC.p, hp.listC.data(), 4 * hp.listC.size(), cudaMemcpyHostToDevice));
+    CU(f.patT.alloc(hp.patT.size()));
+    CU(cudaMemcpy(f.patT.p, hp.patT.data(), 4 * hp.patT.size(), cudaMemcpyHostToDevice));
     CU(f.range_primes.alloc(hp.range_primes.size()));
     CU(cudaMemcpy(f.range_primes.p, hp.range_primes.data(), 4 * hp.range_primes.size(), cudaMemcpyHostToDevice));
 
@@ -206,6 +208,8 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     pc.nBpad = (uint32_t)hp.packB.size();
     pc.nC = (uint32_t)hp.primesC.size();
     memcpy(pc.A, hp.A, sizeof(pc.A));
+    pc.patT = f.patT.p;
+    pc.patT_words = (uint32_t)hp.patT.size();
     pc.lines = f.lines.p;
     pc.primesB = f.primesB.p;
     pc.packB = f.packB.p;

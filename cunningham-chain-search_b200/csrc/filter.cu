@@ -92,20 +92,38 @@ struct SweepArgs {
     uint32_t b_stride;             // level-B primes per lane column in shared memory
 };
 
-// standard level-A sets: every prime 37..127 (STD = 1), and the same set
-// with 37 absorbed into an extended lattice (STD = 2)
-__device__ constexpr uint32_t kStdQ[3][kNumA] = {
-    {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
-    {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127},
-    {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127}};
-__device__ constexpr int kStdA1[3] = {kNumA1, 7, 6};
+// standard level-A sets, with compile-time primes: STD = 1, 2: primes
+// 37..127 / 41..127 (37 absorbed into an extended lattice); STD = 3, 4: the
+// same with table windows up to 199
+#define CCS_STD_T7 97, 101, 103, 107, 109, 113, 127
+#define CCS_STD_T22 CCS_STD_T7, 131, 137, 139, 149, 151, 157, 163, 167, 173, 179, 181, 191, 193, 197, 199
+#define CCS_NO_T15 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1
+__device__ constexpr uint32_t kStdQ[5][kNumA] = {
+    {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1,
+     1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
+    {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89, CCS_STD_T7, CCS_NO_T15},
+    {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89, CCS_STD_T7, CCS_NO_T15},
+    {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89, CCS_STD_T22},
+    {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89, CCS_STD_T22}};
+#undef CCS_STD_T7
+#undef CCS_STD_T22
+#undef CCS_NO_T15
+__device__ constexpr int kStdA1[5] = {kNumA1, 7, 6, 7, 6};
+__device__ constexpr int kStdNT[5] = {kNumT, 7, 7, 22, 22};
+// pattern-table offset of table-window slot i in a standard set (t_words(q)
+// words per prime, in slot order)
+__device__ constexpr uint32_t std_toff(int i) {
+    uint32_t o = 0;
+    for (int k = 0; k < i; k++) o += t_words(kStdQ[3][kNumAR + k]);
+    return o;
+}
 
 constexpr int kQCap = 512;               // per-warp level-B queue (entries, power of two)
 constexpr uint32_t kQLow = 96;           // level-B rounds run until at most this many are queued
 constexpr int kCCap = 64;                // per-warp level-C list (entries)
 constexpr int kBK = kLevelBRound;        // level-B primes tested per lane per round
-constexpr int kPAWords = kNumA * 8;      // per-warp copy of the level-A patterns (u32)
-constexpr int kSAWords = kNumA * 16;     // per-warp level-A phases, [kNumA][32] u16
+constexpr int kPAWords = kNumAR * 8 + kPatTMax;   // per-warp copy of the level-A patterns (u32)
+constexpr int kSAWords = kNumA * 8;      // per-warp level-A phases, [kNumA][32] u8
 constexpr uint32_t kNone = 0xFFFFFFFFu;  // empty lane slot
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 
@@ -235,7 +253,7 @@ __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const Ran
 template <int STD>
 __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R, const ProfileConst& P,
                                            uint32_t cur_range, uint32_t g, uint32_t w0, uint32_t w1,
-                                           uint32_t* Qw, uint32_t* Cw, uint32_t* PA, uint16_t* SA,
+                                           uint32_t* Qw, uint32_t* Cw, uint32_t* PA, uint8_t* SA,
                                            uint16_t* S, uint32_t lane, uint32_t lane_lt) {
         const uint32_t* jm = a.jmod + (uint64_t)cur_range * a.jmod_stride;
         const uint32_t li = g * 32 + lane;
@@ -254,14 +272,17 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         const uint32_t jbase = w0 * 64;
 
         // ---- per-warp pattern copy, per-lane phases at block jbase ----
-        for (uint32_t x = lane; x < (uint32_t)kPAWords; x += 32) PA[x] = P.A[x >> 3].ext[x & 7];
+        for (uint32_t x = lane; x < (uint32_t)kNumAR * 8; x += 32) PA[x] = P.A[x >> 3].ext[x & 7];
+        uint32_t* PT = PA + kNumAR * 8;
+        for (uint32_t x = lane; x < P.patT_words; x += 32) PT[x] = __ldg(P.patT + x);
 #pragma unroll
         for (int i = 0; i < kNumA; i++) {
+            if (STD && i >= kNumAR + kStdNT[STD]) continue;
             const LevelA& la = P.A[i];
             const uint32_t q = STD ? kStdQ[STD][i] : la.q;
             uint32_t ph = 0;
             if (q > 1) ph = phase_fast(ln.r_lo, ln.r_hi, q, la.magic, la.c32, la.winv, jm[i], jbase);
-            SA[i * 32 + lane] = (uint16_t)ph;
+            SA[i * 32 + lane] = (uint8_t)ph;
         }
         for (uint32_t p = 0; p < P.nBpad; p++) {
             uint32_t ph = 0;
@@ -292,24 +313,23 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
             // ---- level A: windows at word w ----
             uint64_t A1w[kNumA1];
             uint32_t A2w[kNumA2][3];
-            uint32_t A3w[kNumA3][4];
+            uint32_t Tph[kNumT];
             const uint32_t off = (w - w0) * 64;
 #pragma unroll
             for (int i = 0; i < kNumA; i++) {
+                if (STD && i >= kNumAR + kStdNT[STD]) continue;
                 const uint32_t q = STD ? kStdQ[STD][i] : P.A[i].q;
                 uint32_t ph = (uint32_t)SA[i * 32 + lane] + off;
                 if (STD) ph = q > 1 ? ph % q : 0;
                 else ph = mod_magic(ph, q, P.A[i].magic);
+                if (i >= kNumAR) { Tph[i - kNumAR] = ph; continue; }
                 const uint32_t* pa = PA + i * 8 + (ph >> 5);
                 const uint32_t b = ph & 31;
                 if (i < kNumA1) {
                     A1w[i] = ((uint64_t)__funnelshift_r(pa[1], pa[2], b) << 32) | __funnelshift_r(pa[0], pa[1], b);
-                } else if (i < kNumA1 + kNumA2) {
-#pragma unroll
-                    for (int m = 0; m < 3; m++) A2w[i - kNumA1][m] = __funnelshift_r(pa[m], pa[m + 1], b);
                 } else {
 #pragma unroll
-                    for (int m = 0; m < 4; m++) A3w[i - kNumA1 - kNumA2][m] = __funnelshift_r(pa[m], pa[m + 1], b);
+                    for (int m = 0; m < 3; m++) A2w[i - kNumA1][m] = __funnelshift_r(pa[m], pa[m + 1], b);
                 }
             }
             for (;;) {
@@ -335,16 +355,20 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                         A2w[i][1] = __funnelshift_l(o0, o1, t);
                         A2w[i][2] = __funnelshift_l(o1, o2, t);
                     }
+                    // table windows: 64 pattern bits from the phase, phase += 64 mod q
 #pragma unroll
-                    for (int i = 0; i < kNumA3; i++) {
-                        const uint32_t t = STD ? (kStdQ[STD][kNumA1 + kNumA2 + i] - 96u)
-                                               : P.A[kNumA1 + kNumA2 + i].t;
-                        const uint32_t o0 = A3w[i][0], o1 = A3w[i][1], o2 = A3w[i][2], o3 = A3w[i][3];
-                        kill |= ((uint64_t)o1 << 32) | o0;
-                        A3w[i][0] = o2;
-                        A3w[i][1] = o3 | (o0 << t);
-                        A3w[i][2] = __funnelshift_l(o0, o1, t);
-                        A3w[i][3] = __funnelshift_l(o1, o2, t);
+                    for (int i = 0; i < kNumT; i++) {
+                        if (STD && i >= kStdNT[STD]) continue;
+                        const uint32_t q = STD ? kStdQ[STD][kNumAR + i] : P.A[kNumAR + i].q;
+                        const uint32_t toff = STD ? std_toff(i) : P.A[kNumAR + i].toff;
+                        const uint32_t ph = Tph[i];
+                        const uint32_t* pt = PT + toff + (ph >> 5);
+                        const uint32_t b = ph & 31;
+                        const uint32_t x0 = pt[0], x1 = pt[1], x2 = pt[2];
+                        kill |= ((uint64_t)__funnelshift_r(x1, x2, b) << 32) | __funnelshift_r(x0, x1, b);
+                        uint32_t nx = min(ph + 64u, ph + 64u - q);
+                        if (!STD) nx = q > 1 ? nx : 0u;
+                        Tph[i] = nx;
                     }
                     // positions of this word inside [jlo, jhi)
                     const uint32_t wb = w * 64;
@@ -408,12 +432,12 @@ sweep_kernel(SweepArgs a) {
     const uint32_t lane_lt = (1u << lane) - 1u;
     const uint32_t warp_in_block = threadIdx.x >> 5;
     // per warp: level-B queue (kQCap u32), level-C list (kCCap u32), level-A
-    // patterns (kPAWords u32), level-A phases (kNumA * 32 u16), level-B
+    // patterns (kPAWords u32), level-A phases (kNumA * 32 u8), level-B
     // phases (b_stride * 32 u16)
     uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + kCCap + kPAWords + kSAWords + a.b_stride * 16);
     uint32_t* Cw = Qw + kQCap;
     uint32_t* PA = Cw + kCCap;
-    uint16_t* SA = reinterpret_cast<uint16_t*>(PA + kPAWords);
+    uint8_t* SA = reinterpret_cast<uint8_t*>(PA + kPAWords);
     uint16_t* S = reinterpret_cast<uint16_t*>(PA + kPAWords + kSAWords);
     const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -438,9 +462,13 @@ sweep_kernel(SweepArgs a) {
         const uint32_t wc = (uint32_t)(local / n_groups);
         const uint32_t w0 = wc * R.unit_words;
         const uint32_t w1 = min(w0 + R.unit_words, R.n_words);
-        if (P.std_a == 1) sweep_unit<1>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt);
-        else if (P.std_a == 2) sweep_unit<2>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt);
-        else sweep_unit<0>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt);
+        switch (P.std_a) {
+        case 1: sweep_unit<1>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
+        case 2: sweep_unit<2>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
+        case 3: sweep_unit<3>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
+        case 4: sweep_unit<4>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
+        default: sweep_unit<0>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
+        }
     }
 }
 

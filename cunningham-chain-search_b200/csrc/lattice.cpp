@@ -220,9 +220,33 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
     // ---- level classification ----------------------------------------------
     memset(hp.A, 0, sizeof(hp.A));
     for (int i = 0; i < kNumA; i++) hp.A[i].q = 1;      // dummy: no kills
-    int nA1 = 0, nA2 = 0, nA3 = 0;
+    int nA1 = 0, nA2 = 0, nT = 0;
     hp.primesB.clear(); hp.primesC.clear(); hp.bitmapB.clear(); hp.listC.clear(); hp.packB.clear();
+    hp.patT.clear();
     const uint64_t Wm = hp.W;
+    // How many table-window primes: one costs about as much per 64-position
+    // word as a fifth of a level-B test per lane, so the next prime is taken
+    // while the expected level-A survivors per word (64 x product of the pass
+    // fractions taken so far) stay above kTAdmit; the count is then rounded
+    // to one of the two compiled standard sizes (7: primes < 128, or 22).
+    int nT_max = 0;
+    {
+        double as = 64.0;
+        int a1 = 0, a2 = 0, nt = 0, avail = 0;
+        bool open = true;
+        for (auto& fp : hp.fprimes) {
+            const uint32_t q = fp.q;
+            if (q == hp.q0) continue;
+            const double pass = 1.0 - (double)fp.forb.size() / q;
+            if (q < 64 && a1 < kNumA1) { a1++; as *= pass; }
+            else if (q > 64 && q < 96 && a2 < kNumA2) { a2++; as *= pass; }
+            else if (q > 96 && q < kTLimit && avail < kNumT) {
+                avail++;
+                if (open && as >= kTAdmit) { nt++; as *= pass; } else open = false;
+            }
+        }
+        nT_max = nt <= 14 ? std::min(7, avail) : std::min(kNumT, avail);
+    }
     for (auto& fp : hp.fprimes) {
         uint32_t q = fp.q;
         if (q == hp.q0) continue;                       // absorbed into the lattice
@@ -233,7 +257,9 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
         int slot = -1;
         if (q < 64 && nA1 < kNumA1) slot = nA1++;
         else if (q > 64 && q < 96 && nA2 < kNumA2) slot = kNumA1 + nA2++;
-        else if (q > 96 && q < 128 && nA3 < kNumA3) slot = kNumA1 + kNumA2 + nA3++;
+        else if (q > 96 && q < kTLimit && nT < nT_max &&
+                 hp.patT.size() + t_words(q) + 3 <= (size_t)kPatTMax)
+            slot = kNumAR + nT++;
         if (slot >= 0) {
             LevelA& a = hp.A[slot];
             a.q = q;
@@ -241,10 +267,21 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             a.magic = 0xFFFFFFFFu / q;
             a.c32 = (uint32_t)((1ull << 32) % q);
             if (slot < kNumA1) { a.s = 64 % q; a.t = q - a.s; }
-            else if (slot < kNumA1 + kNumA2) { a.s = 0; a.t = q - 64; }
-            else { a.s = 0; a.t = q - 96; }
-            for (uint32_t x = 0; x < 256; x++)
-                if (std::binary_search(g.begin(), g.end(), x % q)) a.ext[x >> 5] |= 1u << (x & 31);
+            else if (slot < kNumAR) { a.s = 0; a.t = q - 64; }
+            if (slot < kNumAR) {
+                for (uint32_t x = 0; x < 256; x++)
+                    if (std::binary_search(g.begin(), g.end(), x % q)) a.ext[x >> 5] |= 1u << (x & 31);
+            } else {
+                // replicated pattern: a 64-bit window at any phase < q lies in tnw words
+                a.toff = (uint32_t)hp.patT.size();
+                a.tnw = t_words(q);
+                for (uint32_t wd = 0; wd < a.tnw; wd++) {
+                    uint32_t v = 0;
+                    for (uint32_t bit = 0; bit < 32; bit++)
+                        if (std::binary_search(g.begin(), g.end(), (wd * 32 + bit) % q)) v |= 1u << bit;
+                    hp.patT.push_back(v);
+                }
+            }
             continue;
         }
         PrimeC pc;
@@ -273,6 +310,12 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             hp.primesC.push_back(pc);
         }
     }
+    // dummy table-window slots read an all-zero block (phase stays 0)
+    {
+        const uint32_t zoff = (uint32_t)hp.patT.size();
+        for (int i = 0; i < 3; i++) hp.patT.push_back(0);
+        for (int i = nT; i < kNumT; i++) { hp.A[kNumAR + i].toff = zoff; hp.A[kNumAR + i].tnw = 3; }
+    }
     // pad the level-B records to a multiple of the per-round test count with
     // entries that never kill (q = 2, all-zero bitmap word)
     if (!hp.packB.empty() && hp.packB.size() % kLevelBRound) {
@@ -286,14 +329,23 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             hp.packB.push_back(pb);
         }
     }
-    // the standard level-A set (every prime 37..127) has a kernel with
+    // the standard level-A sets (primes 37..127 or 37..199, with or without 37
+    // absorbed into the lattice) have kernels with
     // compile-time shift amounts
     {
-        static const uint32_t std_q[2][kNumA] = {
-            {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127},
-            {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127}};
+        static const uint32_t std_q[4][kNumA] = {
+            {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89,
+             97, 101, 103, 107, 109, 113, 127, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
+            {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89,
+             97, 101, 103, 107, 109, 113, 127, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
+            {37, 41, 43, 47, 53, 59, 61, 1, 1, 67, 71, 73, 79, 83, 89,
+             97, 101, 103, 107, 109, 113, 127, 131, 137, 139, 149, 151, 157, 163, 167, 173, 179, 181,
+             191, 193, 197, 199},
+            {41, 43, 47, 53, 59, 61, 1, 1, 1, 67, 71, 73, 79, 83, 89,
+             97, 101, 103, 107, 109, 113, 127, 131, 137, 139, 149, 151, 157, 163, 167, 173, 179, 181,
+             191, 193, 197, 199}};
         hp.std_a = 0;
-        for (int v = 0; v < 2; v++) {
+        for (int v = 0; v < 4; v++) {
             bool same = true;
             for (int i = 0; i < kNumA; i++) same &= hp.A[i].q == std_q[v][i];
             if (same) hp.std_a = 1 + v;
