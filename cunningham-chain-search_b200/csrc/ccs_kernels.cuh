@@ -81,8 +81,33 @@ cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
                          uint32_t b_stride, uint32_t grid, cudaStream_t st);
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
-cudaError_t launch_walk(const uint32_t* numbers, uint64_t n, uint32_t limbs, uint32_t* lengths,
-                        int profile, cudaStream_t st);
+// breadth-first chain walk (prove.cu)
+struct WalkItem {
+    uint32_t x[kMaxLimbs];   // current chain member
+    uint32_t idx;            // position in the caller's batch
+    uint32_t len;            // primes found so far
+};
+struct WalkState {
+    uint32_t n_act;                      // items tested this round
+    uint32_t n_next;                     // items for the next round
+    uint32_t n_region[kMaxLimbs + 1];    // items per Montgomery limb count
+    uint32_t off_region[kMaxLimbs + 1];
+    uint32_t fill[kMaxLimbs + 1];
+    uint32_t n_lucas[kMaxLimbs + 1];     // base-2 probable primes per limb count
+};
+struct WalkArgs {
+    WalkState* st;
+    const WalkItem* act;
+    WalkItem* sorted;                    // act, grouped by limb count
+    WalkItem* lucas;                     // same regions as sorted
+    WalkItem* next;
+    uint8_t* code;                       // trial-stage verdict per act item
+    uint32_t* lengths;
+    int profile;
+};
+cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
+                             WalkItem* out, cudaStream_t st);
+cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, uint32_t primality, cudaStream_t st);
 int sweep_blocks_per_sm(uint32_t b_stride);
 cudaError_t modmul_count(uint64_t* out, bool reset);
 

@@ -117,6 +117,10 @@ struct ccs_engine {
     DevBuf<uint32_t> d_counters;     // [0] surv, [1] spare, [2] chains, [3] primes
     // host-path scratch
     DevBuf<uint32_t> d_surv_scratch, d_chain_scratch;
+    // chain-walk rounds: items, sorted / Lucas regions, next round, codes, state
+    DevBuf<WalkItem> w_act, w_next, w_sorted, w_lucas;
+    DevBuf<uint8_t> w_code;
+    DevBuf<WalkState> w_state;
     // pinned staging
     void* h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -467,6 +471,8 @@ ccs_status ccs_destroy(ccs_engine* E) {
     E->d_range.free_(); E->d_prange.free_(); E->d_prefix.free_(); E->d_hdr.free_();
     E->d_jmod.free_(); E->d_counters.free_();
     E->d_surv_scratch.free_(); E->d_chain_scratch.free_();
+    E->w_act.free_(); E->w_next.free_(); E->w_sorted.free_(); E->w_lucas.free_();
+    E->w_code.free_(); E->w_state.free_();
     if (E->h_stage) cudaFreeHost(E->h_stage);
     if (E->own_stream) cudaStreamDestroy(E->own_stream);
     for (auto& f : E->fs) free_slot(E->device, f.slot);
@@ -658,7 +664,45 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
     if (n && (!numbers_dev || !lengths_dev)) return fail(CCS_ERR_INVALID, "null buffer");
     CU(cudaSetDevice(E->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : E->own_stream;
-    if (n) { CU(launch_walk(numbers_dev, n, limbs, lengths_dev, E->slot, st)); E->launches += 1; }
+    if (!n) return CCS_OK;
+    // numbers are walked in chunks of up to 2^22, each in rounds until every
+    // walk has ended (at most MAX_CHAIN rounds)
+    const uint64_t chunk = std::min<uint64_t>(n, 1ull << 22);
+    if (E->w_act.n < chunk) {
+        CU(E->w_act.alloc(chunk)); CU(E->w_next.alloc(chunk));
+        CU(E->w_sorted.alloc(chunk)); CU(E->w_lucas.alloc(chunk));
+        CU(E->w_code.alloc(chunk));
+    }
+    if (!E->w_state.p) CU(E->w_state.alloc(1));
+    WalkState* hs = (WalkState*)((char*)E->h_stage + 12288);
+    for (uint64_t first = 0; first < n; first += chunk) {
+        const uint32_t cn = (uint32_t)std::min<uint64_t>(chunk, n - first);
+        CU(launch_walk_load(numbers_dev, first, cn, limbs, E->w_act.p, st));
+        E->launches += 1;
+        WalkItem* act = E->w_act.p;
+        WalkItem* nxt = E->w_next.p;
+        uint32_t n_act = cn;
+        for (int round = 0; n_act && round <= kMaxChain; round++) {
+            memset(hs, 0, sizeof(WalkState));
+            hs->n_act = n_act;
+            CU(cudaMemcpyAsync(E->w_state.p, hs, sizeof(WalkState), cudaMemcpyHostToDevice, st));
+            WalkArgs a;
+            a.st = E->w_state.p;
+            a.act = act;
+            a.sorted = E->w_sorted.p;
+            a.lucas = E->w_lucas.p;
+            a.next = nxt;
+            a.code = E->w_code.p;
+            a.lengths = lengths_dev;
+            a.profile = E->slot;
+            CU(launch_walk_round(a, n_act, E->hp.primality, st));
+            E->launches += E->hp.primality == CCS_PRIME_BPSW ? 5 : 4;
+            CU(cudaMemcpyAsync(hs, &E->w_state.p->n_next, 4, cudaMemcpyDeviceToHost, st));
+            CU(cudaStreamSynchronize(st));
+            n_act = hs->n_act;
+            std::swap(act, nxt);
+        }
+    }
     CU(cudaStreamSynchronize(st));
     return CCS_OK;
 }

@@ -41,11 +41,35 @@ __device__ __forceinline__ int big_bits(const Big& a) {
     return 0;
 }
 
+// x mod q for x < 2^32, magic = floor((2^32 - 1) / q)
+__device__ __forceinline__ uint32_t mod_m32(uint32_t x, uint32_t q, uint32_t magic) {
+    const uint32_t t = x - __umulhi(x, magic) * q;
+    return t >= q ? t - q : t;
+}
+
+// a mod q for q < 2^16: 16-bit digits, one reciprocal
 __device__ __forceinline__ uint32_t big_mod_small(const Big& a, uint32_t q) {
-    uint64_t acc = 0;
+    const uint32_t magic = 0xFFFFFFFFu / q;
+    uint32_t r = 0;
 #pragma unroll
-    for (int i = kMaxLimbs - 1; i >= 0; i--) acc = ((acc << 32) | a.w[i]) % q;
-    return (uint32_t)acc;
+    for (int i = kMaxLimbs - 1; i >= 0; i--) {
+        r = mod_m32((r << 16) | (a.w[i] >> 16), q, magic);
+        r = mod_m32((r << 16) | (a.w[i] & 0xFFFFu), q, magic);
+    }
+    return r;
+}
+
+// a mod m for m < 2^32 with magic64 = floor((2^64 - 1) / m)
+__device__ __forceinline__ uint32_t big_mod_u32(const Big& a, uint32_t m, uint64_t magic64) {
+    uint64_t r = 0;
+#pragma unroll
+    for (int i = kMaxLimbs - 1; i >= 0; i--) {
+        const uint64_t x = (r << 32) | a.w[i];
+        uint64_t t = x - __umul64hi(x, magic64) * m;
+        while (t >= m) t -= m;
+        r = t;
+    }
+    return (uint32_t)r;
 }
 
 // a = 2a + 1 (returns carry-out)
@@ -275,26 +299,39 @@ __device__ bool strong_prp(Mont<NL>& M, const Big& nb, uint32_t a) {
             break;
         }
         s = lz;
-        // d >>= s
-        int ws = s >> 5, bs = s & 31;
+        // d >>= s: whole limbs first, then bits (static limb indices)
+        const int ws = s >> 5, bs = s & 31;
+        for (int k = 0; k < ws; k++) {
 #pragma unroll
-        for (int i = 0; i < kMaxLimbs; i++) {
-            uint32_t lo = (i + ws < kMaxLimbs) ? d.w[i + ws] : 0;
-            uint32_t hi = (i + ws + 1 < kMaxLimbs) ? d.w[i + ws + 1] : 0;
-            d.w[i] = bs ? ((lo >> bs) | (hi << (32 - bs))) : lo;
+            for (int i = 0; i < kMaxLimbs; i++) d.w[i] = (i + 1 < kMaxLimbs) ? d.w[i + 1] : 0u;
+        }
+        if (bs) {
+#pragma unroll
+            for (int i = 0; i < kMaxLimbs; i++) {
+                const uint32_t hi = (i + 1 < kMaxLimbs) ? d.w[i + 1] : 0u;
+                d.w[i] = (d.w[i] >> bs) | (hi << (32 - bs));
+            }
         }
     }
     uint32_t am[NL], x[NL];
     to_mont_small<NL>(am, a, M);
 #pragma unroll
     for (int i = 0; i < NL; i++) x[i] = am[i];
+    // left-to-right over the bits of d below its top bit; the limb loop is
+    // unrolled so d stays in registers
     const int top = big_bits(d) - 1;
-    for (int b = top - 1; b >= 0; b--) {
-        montmul<NL>(x, x, x, M.n, M.ninv);
-        M.count++;
-        if ((d.w[b >> 5] >> (b & 31)) & 1u) {
-            if (a == 2) dblmod<NL>(x, x, M.n);
-            else { montmul<NL>(x, x, am, M.n, M.ninv); M.count++; }
+#pragma unroll
+    for (int wi = kMaxLimbs - 1; wi >= 0; wi--) {
+        if (32 * wi > top - 1) continue;
+        const uint32_t word = d.w[wi];
+        const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
+        for (int b = hb; b >= 0; b--) {
+            montmul<NL>(x, x, x, M.n, M.ninv);
+            M.count++;
+            if ((word >> b) & 1u) {
+                if (a == 2) dblmod<NL>(x, x, M.n);
+                else { montmul<NL>(x, x, am, M.n, M.ninv); M.count++; }
+            }
         }
     }
     if (eq<NL>(x, M.one) || eq<NL>(x, M.mone)) return true;
@@ -387,14 +424,20 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
     uint32_t U[NL], V[NL], Qk[NL], t1[NL], t2[NL];
 #pragma unroll
     for (int i = 0; i < NL; i++) { U[i] = M.one[i]; V[i] = M.one[i]; Qk[i] = Qm[i]; }
-    for (int b = big_bits(d) - 2; b >= 0; b--) {
+    const int top = big_bits(d) - 1;
+#pragma unroll
+    for (int wi = kMaxLimbs - 1; wi >= 0; wi--) {
+      if (32 * wi > top - 1) continue;
+      const uint32_t word = d.w[wi];
+      const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
+      for (int b = hb; b >= 0; b--) {
         montmul<NL>(U, U, V, M.n, M.ninv);
         montmul<NL>(t1, V, V, M.n, M.ninv);
         addmod<NL>(t2, Qk, Qk, M.n);
         submod<NL>(V, t1, t2, M.n);
         montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
         M.count += 3;
-        if ((d.w[b >> 5] >> (b & 31)) & 1u) {
+        if ((word >> b) & 1u) {
             uint32_t nu[NL], nv[NL];
             addmod<NL>(nu, U, V, M.n);
             halfmod<NL>(nu, M.n);
@@ -406,6 +449,7 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
             montmul<NL>(Qk, Qk, Qm, M.n, M.ninv);
             M.count += 2;
         }
+      }
     }
     if (is_zero<NL>(U) || is_zero<NL>(V)) return true;
     for (int r = 1; r < s; r++) {
@@ -437,38 +481,75 @@ __device__ bool prp_suite(const Big& nb, int nbits, uint32_t primality, const Pr
 
 __constant__ uint32_t c_small_primes[27] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47,
                                             53, 59, 61, 67, 71, 73, 79, 83, 89, 97, 101, 1093, 3511};
+// the trial primes in five groups whose products fit 32 bits: one multi-limb
+// reduction per group, then 32-bit reductions per prime (groups 0..2 are the
+// 19 primes 3..71 of the MR predicate)
+__constant__ uint32_t c_group_prod[5] = {3234846615u, 95041567u, 907383479u, 4132280413u, 387589823u};
+__constant__ uint8_t c_group_end[5] = {9, 14, 19, 24, 27};
+#define CCS_M(p) (0xFFFFFFFFu / (p))
+__constant__ uint32_t c_small_magic[27] = {
+    CCS_M(3), CCS_M(5), CCS_M(7), CCS_M(11), CCS_M(13), CCS_M(17), CCS_M(19), CCS_M(23), CCS_M(29),
+    CCS_M(31), CCS_M(37), CCS_M(41), CCS_M(43), CCS_M(47), CCS_M(53), CCS_M(59), CCS_M(61), CCS_M(67),
+    CCS_M(71), CCS_M(73), CCS_M(79), CCS_M(83), CCS_M(89), CCS_M(97), CCS_M(101), CCS_M(1093),
+    CCS_M(3511)};
+#undef CCS_M
+
+// Trial stage of the primality predicate (every branch of v13 gpu_is_prime,
+// v13:1428-1452, and of the BPSW screen): returns 0 = composite, 1 = prime
+// without a probable-prime test, or the Montgomery limb count (2..6) of the
+// test that decides.
+__device__ int prime_screen(const Big& nb, const ProveConst& pc, int& nbits_out) {
+    const int nbits = big_bits(nb);
+    nbits_out = nbits;
+    if (nbits <= 1) return 0;
+    const uint32_t lo = nb.w[0];
+    const bool mr = pc.primality == CCS_PRIME_MR;
+    const int ntrial = mr ? 19 : 27;
+    if (mr) {
+        if (nbits <= 64 && nb.w[1] == 0) {
+            if (lo < 2) return 0;
+            if (lo == 2 || lo == 3) return 1;
+            if ((lo & 1u) == 0) return 0;
+            if (lo < 9) return 1;
+        }
+        if ((lo & 1u) == 0) return 0;
+    } else {
+        if (nbits <= 32 && lo == 2) return 1;
+        if ((lo & 1u) == 0) return 0;
+    }
+    if (nbits <= 32) {
+        // small n: the prime list in order (n may equal one of them)
+        for (int i = 0; i < ntrial; i++) {
+            const uint32_t p = c_small_primes[i];
+            if (mr) {
+                if (lo % p == 0) return lo == p ? 1 : 0;
+            } else {
+                if (lo == p) return 1;
+                if (lo % p == 0) return 0;
+            }
+        }
+        if (!mr && lo < 103u * 103u) return 1;
+    } else {
+        const int ngroups = mr ? 3 : 5;
+        int i = 0;
+        for (int g = 0; g < ngroups; g++) {
+            const uint32_t G = c_group_prod[g];
+            const uint32_t rg = big_mod_u32(nb, G, ~0ull / G);
+            for (; i < c_group_end[g]; i++)
+                if (mod_m32(rg, c_small_primes[i], c_small_magic[i]) == 0) return 0;
+        }
+    }
+    const int nl = (nbits + 31) >> 5;
+    return nl <= 2 ? 2 : nl;
+}
 
 // primality predicate of the profile for any n < 2^192; mm counts the
 // Montgomery products spent
 __device__ bool is_prime_dev(const Big& nb, const ProveConst& pc, uint32_t& mm) {
-    const int nbits = big_bits(nb);
-    if (nbits <= 1) return false;
-    const uint32_t lo = nb.w[0];
-    if (pc.primality == CCS_PRIME_MR) {
-        // v13:1428-1452
-        if (nbits <= 64 && nb.w[1] == 0) {
-            if (lo < 2) return false;
-            if (lo == 2 || lo == 3) return true;
-            if ((lo & 1u) == 0) return false;
-            if (lo < 9) return true;
-        }
-        if ((lo & 1u) == 0) return false;
-        for (int i = 0; i < 19; i++) {
-            uint32_t p = c_small_primes[i];
-            if (big_mod_small(nb, p) == 0) return nbits <= 32 && lo == p;
-        }
-    } else {
-        if (nbits <= 32 && lo == 2) return true;
-        if ((lo & 1u) == 0) return false;
-        for (int i = 0; i < 27; i++) {
-            uint32_t p = c_small_primes[i];
-            if (nbits <= 32 && lo == p) return true;
-            if (big_mod_small(nb, p) == 0) return false;
-        }
-        if (nbits <= 32 && lo < 103u * 103u) return true;
-    }
-    const int nl = (nbits + 31) >> 5;
-    switch (nl <= 2 ? 2 : nl) {
+    int nbits;
+    const int v = prime_screen(nb, pc, nbits);
+    if (v < 2) return v == 1;
+    switch (v) {
         case 2: return prp_suite<2>(nb, nbits, pc.primality, pc, mm);
         case 3: return prp_suite<3>(nb, nbits, pc.primality, pc, mm);
         case 4: return prp_suite<4>(nb, nbits, pc.primality, pc, mm);
@@ -579,21 +660,195 @@ prove_kernel(ProveArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// walk kernel: chain length from each given number
+// breadth-first chain walk
+//
+// Every number of a walk batch is an item {member, index, primes so far}.
+// A round tests the current member of every live item: a screen kernel runs
+// the trial stage and sorts the items that need a probable-prime test into
+// one region per Montgomery limb count, a test kernel per region runs the
+// base-2 strong test (or the witness list), a second one the strong Lucas
+// test of the base-2 probable primes; members found prime advance to 2p + 1
+// for the next round, the others end their walk.  Warps therefore run one
+// limb count and one test at a time, whatever the chain lengths.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
-walk_kernel(const uint32_t* __restrict__ numbers, uint64_t n, uint32_t limbs,
-            uint32_t* __restrict__ lengths, int profile) {
-    const ProveConst& pc = c_prove[profile];
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        Big x;
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, want);
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    const int leader = __ffs(m) - 1;
+    if (m && (int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader < 0 ? 0 : leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void walk_count_mm(uint32_t mm) {
+    const uint32_t tot = __reduce_add_sync(0xFFFFFFFFu, mm);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&g_modmul_count, (unsigned long long)tot);
+}
+
+// member found prime: count it, continue with 2p + 1 or end the walk
+// (MAX_CHAIN, or a next member beyond 192 bits; v13:1519-1528, 1873-1881)
+__device__ __forceinline__ void walk_advance(const WalkItem& it, int nbits, bool live, WalkArgs& a) {
+    const uint32_t len = it.len + 1;
+    const bool more = live && len < (uint32_t)kMaxChain && nbits < 32 * kMaxLimbs;
+    const uint32_t pos = warp_append(&a.st->n_next, more);
+    if (!live) return;
+    if (more) {
+        WalkItem nx = it;
+        uint32_t carry = 1;
 #pragma unroll
-        for (int w = 0; w < kMaxLimbs; w++) x.w[w] = (w < (int)limbs) ? numbers[i * limbs + w] : 0u;
-        uint32_t mm = 0;
-        lengths[i] = is_prime_dev(x, pc, mm) ? (uint32_t)walk_forward(x, pc, mm) : 0u;
-        atomicAdd(&g_modmul_count, (unsigned long long)mm);
+        for (int i = 0; i < kMaxLimbs; i++) {
+            const uint32_t nc = nx.x[i] >> 31;
+            nx.x[i] = (nx.x[i] << 1) | carry;
+            carry = nc;
+        }
+        nx.len = len;
+        a.next[pos] = nx;
+    } else {
+        a.lengths[it.idx] = len;
     }
+}
+
+__global__ void __launch_bounds__(256)
+walk_load_kernel(const uint32_t* __restrict__ numbers, uint64_t first, uint32_t n, uint32_t limbs,
+                 WalkItem* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        WalkItem it;
+#pragma unroll
+        for (int w = 0; w < kMaxLimbs; w++)
+            it.x[w] = (w < (int)limbs) ? numbers[(first + i) * limbs + w] : 0u;
+        it.idx = (uint32_t)(first + i);
+        it.len = 0;
+        out[i] = it;
+    }
+}
+
+// trial stage; records the verdict code of every item and counts each region
+__global__ void __launch_bounds__(256)
+walk_screen_kernel(WalkArgs a) {
+    const ProveConst& pc = c_prove[a.profile];
+    const uint32_t n = a.st->n_act;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        const bool live = i < n;
+        WalkItem it;
+        int nbits = 0, v = 0;
+        if (live) {
+            it = a.act[i];
+            Big b;
+#pragma unroll
+            for (int w = 0; w < kMaxLimbs; w++) b.w[w] = it.x[w];
+            v = prime_screen(b, pc, nbits);
+            a.code[i] = (uint8_t)v;
+            if (v == 0) a.lengths[it.idx] = it.len;
+        }
+        walk_advance(it, nbits, live && v == 1, a);
+#pragma unroll
+        for (int nl = 2; nl <= kMaxLimbs; nl++) {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, live && v == nl);
+            if (m && (threadIdx.x & 31) == (uint32_t)(__ffs(m) - 1)) atomicAdd(&a.st->n_region[nl], __popc(m));
+        }
+    }
+}
+
+__global__ void walk_regions_kernel(WalkState* st) {
+    if (threadIdx.x == 0) {
+        uint32_t o = 0;
+        for (int nl = 0; nl <= kMaxLimbs; nl++) {
+            st->off_region[nl] = o;
+            st->fill[nl] = o;
+            o += st->n_region[nl];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256)
+walk_scatter_kernel(WalkArgs a) {
+    const uint32_t n = a.st->n_act;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        const int v = i < n ? a.code[i] : 0;
+#pragma unroll
+        for (int nl = 2; nl <= kMaxLimbs; nl++) {
+            const uint32_t pos = warp_append(&a.st->fill[nl], v == nl);
+            if (v == nl) a.sorted[pos] = a.act[i];
+        }
+    }
+}
+
+template <int NL>
+__device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& pc, int stage) {
+    const uint32_t off = a.st->off_region[NL];
+    const uint32_t n = stage == 0 ? a.st->n_region[NL] : a.st->n_lucas[NL];
+    const WalkItem* src = stage == 0 ? a.sorted : a.lucas;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        const bool live = i < n;
+        WalkItem it;
+        Big b;
+        int nbits = 0;
+        bool prime = false, to_lucas = false;
+        uint32_t mm = 0;
+        if (live) {
+            it = src[off + i];
+#pragma unroll
+            for (int w = 0; w < kMaxLimbs; w++) b.w[w] = it.x[w];
+            nbits = big_bits(b);
+            Mont<NL> M;
+            mont_setup<NL>(M, b, nbits);
+            M.count = 0;
+            if (stage == 0) {
+                if (pc.primality == CCS_PRIME_BPSW) {
+                    to_lucas = strong_prp<NL>(M, b, 2);
+                } else {
+                    prime = true;
+                    for (uint32_t k = 0; k < pc.n_wit && prime; k++) prime = strong_prp<NL>(M, b, pc.wit[k]);
+                }
+            } else {
+                prime = strong_lucas<NL>(M, b);
+            }
+            mm = M.count;
+            if (!prime && !to_lucas) a.lengths[it.idx] = it.len;
+        }
+        walk_count_mm(mm);
+        if (stage == 0) {
+            const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas);
+            if (to_lucas) a.lucas[off + pos] = it;
+        }
+        walk_advance(it, nbits, prime, a);
+    }
+}
+
+// blockIdx.y selects the limb count (2 + y); stage 0 = base-2 strong test (or
+// the witness list), stage 1 = strong Lucas test
+__global__ void __launch_bounds__(128, 4)
+walk_test_kernel(WalkArgs a, int stage) {
+    const ProveConst& pc = c_prove[a.profile];
+    switch (blockIdx.y + 2) {
+        case 2: walk_test_region<2>(a, pc, stage); break;
+        case 3: walk_test_region<3>(a, pc, stage); break;
+        case 4: walk_test_region<4>(a, pc, stage); break;
+        case 5: walk_test_region<5>(a, pc, stage); break;
+        default: walk_test_region<6>(a, pc, stage); break;
+    }
+}
+
+cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
+                             WalkItem* out, cudaStream_t st) {
+    const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, 148 * 8);
+    walk_load_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(numbers, first, n, limbs, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, uint32_t primality, cudaStream_t st) {
+    const uint32_t blocks = std::min<uint32_t>((n_act + 255) / 256, 148 * 8);
+    walk_screen_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(a);
+    walk_regions_kernel<<<1, 32, 0, st>>>(a.st);
+    walk_scatter_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(a);
+    const uint32_t tb = std::min<uint32_t>((n_act + 127) / 128, 148 * 16);
+    walk_test_kernel<<<dim3(tb ? tb : 1, kMaxLimbs - 1), 128, 0, st>>>(a, 0);
+    if (primality == CCS_PRIME_BPSW) walk_test_kernel<<<dim3(tb ? tb : 1, kMaxLimbs - 1), 128, 0, st>>>(a, 1);
+    return cudaGetLastError();
 }
 
 cudaError_t modmul_count(uint64_t* out, bool reset) {
@@ -614,13 +869,5 @@ cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_walk(const uint32_t* numbers, uint64_t n, uint32_t limbs, uint32_t* lengths,
-                        int profile, cudaStream_t st) {
-    uint64_t blocks = (n + 127) / 128;
-    if (blocks == 0) blocks = 1;
-    if (blocks > 148 * 64) blocks = 148 * 64;
-    walk_kernel<<<(unsigned)blocks, 128, 0, st>>>(numbers, n, limbs, lengths, profile);
-    return cudaGetLastError();
-}
 
 }  // namespace ccs

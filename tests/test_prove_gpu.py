@@ -151,3 +151,27 @@ def test_roots_mode_matches_reference_k2(ccs, ob):
     assert got == ref
     assert primes == pr.value
     eng.close()
+
+
+def test_walk_rounds_across_chunks(ccs, ob, eng_bpsw):
+    """5e6 numbers (two walk chunks of 2^22): 40,000 distinct 80..110-bit odd
+    numbers repeated 125 times give 125 identical length vectors, equal to
+    the oracle's on a seeded sample."""
+    import torch
+    r = random.Random(2024)
+    distinct = []
+    for _ in range(40000):
+        b = r.randint(80, 110)
+        distinct.append(r.getrandbits(b) | (1 << (b - 1)) | 1)
+    arr = np.zeros((len(distinct), 4), dtype=np.uint32)
+    for i, v in enumerate(distinct):
+        for w in range(4):
+            arr[i, w] = (v >> (32 * w)) & 0xFFFFFFFF
+    base = torch.from_numpy(arr.view(np.int32)).cuda()
+    nums = base.repeat(125, 1).contiguous()
+    lengths = torch.full((nums.shape[0],), -1, dtype=torch.int32, device="cuda")
+    eng_bpsw.walk_numbers_dev(nums, 4, lengths)
+    L = lengths.cpu().numpy().reshape(125, -1)
+    assert (L == L[0]).all()
+    for i in r.sample(range(len(distinct)), 300):
+        assert L[0, i] == ob.chain_from(distinct[i], ob.PRIME_BPSW), distinct[i]
