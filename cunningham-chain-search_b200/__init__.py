@@ -168,6 +168,7 @@ _SIGS = {
     "ccs_measure_int32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "ccs_measure_imad_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "ccs_walk_modmuls": (C.c_int, [_vp, C.POINTER(_u64), C.c_int]),
+    "ccs_walk_word_products": (C.c_int, [_vp, C.POINTER(_u64), C.POINTER(_u64), C.c_int]),
     "ccs_set_tuning": (C.c_int, [_vp, C.POINTER(_Tuning)]),
 }
 
@@ -440,6 +441,13 @@ class Engine:
         v = _u64(0)
         _check(load_library().ccs_walk_modmuls(self.h, C.byref(v), 1 if reset else 0))
         return v.value
+
+    def walk_word_products(self, reset=True):
+        """(Montgomery products, 32x32-bit word products) spent by walk
+        launches since the last reset."""
+        v, w = _u64(0), _u64(0)
+        _check(load_library().ccs_walk_word_products(self.h, C.byref(v), C.byref(w), 1 if reset else 0))
+        return v.value, w.value
 
     def walk_numbers_dev(self, numbers_dev, limbs, lengths_dev):
         _check(load_library().ccs_walk_numbers(self.h, numbers_dev.data_ptr(), numbers_dev.shape[0],

@@ -109,6 +109,6 @@ cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n
                              WalkItem* out, cudaStream_t st);
 cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, uint32_t primality, cudaStream_t st);
 int sweep_blocks_per_sm(uint32_t b_stride);
-cudaError_t modmul_count(uint64_t* out, bool reset);
+cudaError_t modmul_count(uint64_t* out, uint64_t* words, bool reset);
 
 }  // namespace ccs

@@ -710,7 +710,14 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
 ccs_status ccs_walk_modmuls(ccs_engine* E, uint64_t* count, int reset) {
     if (!E || !count) return fail(CCS_ERR_INVALID, "null argument");
     CU(cudaSetDevice(E->device));
-    CU(modmul_count(count, reset != 0));
+    CU(modmul_count(count, nullptr, reset != 0));
+    return CCS_OK;
+}
+
+ccs_status ccs_walk_word_products(ccs_engine* E, uint64_t* modmuls, uint64_t* words, int reset) {
+    if (!E || !modmuls || !words) return fail(CCS_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(E->device));
+    CU(modmul_count(modmuls, words, reset != 0));
     return CCS_OK;
 }
 

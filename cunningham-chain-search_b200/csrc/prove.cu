@@ -21,6 +21,8 @@ __constant__ ProveConst c_prove[kMaxProfiles];
 
 // Montgomery products executed by walk launches (one atomic per number)
 __device__ unsigned long long g_modmul_count = 0;
+// 32 x 32-bit word products of those (2 NL^2 + NL per CIOS product)
+__device__ unsigned long long g_wordmul_count = 0;
 
 cudaError_t upload_prove_const(int slot, const ProveConst& pc, cudaStream_t st) {
     return cudaMemcpyToSymbolAsync(c_prove, &pc, sizeof(ProveConst), slot * sizeof(ProveConst),
@@ -393,9 +395,7 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
         if (++tries > 64) return false;
     }
     const int Qs = (1 - D) / 4;
-    uint32_t Dm[NL], Qm[NL];
-    if (D >= 0) to_mont_small<NL>(Dm, (uint32_t)D, M);
-    else { uint32_t t[NL]; to_mont_small<NL>(t, (uint32_t)(-D), M); submod<NL>(Dm, M.n, t, M.n); }
+    uint32_t Qm[NL];
     if (Qs >= 0) to_mont_small<NL>(Qm, (uint32_t)Qs, M);
     else { uint32_t t[NL]; to_mont_small<NL>(t, (uint32_t)(-Qs), M); uint32_t z[NL];
 #pragma unroll
@@ -421,9 +421,17 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
         }
         s++;
     }
-    uint32_t U[NL], V[NL], Qk[NL], t1[NL], t2[NL];
+    // V ladder (P = 1): keep (V_k, V_{k+1}, Q^k) from k = 1 over the bits of d,
+    //   bit 0: V_2k   = V_k^2 - 2 Q^k,          V_2k+1 = V_k V_k+1 - Q^k,  Q^2k
+    //   bit 1: V_2k+1 = V_k V_k+1 - Q^k,        V_2k+2 = V_k+1^2 - 2 Q^(k+1),  Q^(2k+1)
+    // done branch-free (the same four products for either bit value, so a
+    // warp never runs both); then D U_d = 2 V_(d+1) - V_d with D a unit mod n
+    // ((D/n) = -1), so U_d = 0 exactly when 2 V_(d+1) = V_d.
+    uint32_t V0[NL], V1[NL], Qk[NL], t1[NL], t2[NL];
 #pragma unroll
-    for (int i = 0; i < NL; i++) { U[i] = M.one[i]; V[i] = M.one[i]; Qk[i] = Qm[i]; }
+    for (int i = 0; i < NL; i++) { V0[i] = M.one[i]; Qk[i] = Qm[i]; }
+    dblmod<NL>(t1, Qm, M.n);
+    submod<NL>(V1, M.one, t1, M.n);                 // V_2 = P^2 - 2Q
     const int top = big_bits(d) - 1;
 #pragma unroll
     for (int wi = kMaxLimbs - 1; wi >= 0; wi--) {
@@ -431,32 +439,30 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
       const uint32_t word = d.w[wi];
       const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
       for (int b = hb; b >= 0; b--) {
-        montmul<NL>(U, U, V, M.n, M.ninv);
-        montmul<NL>(t1, V, V, M.n, M.ninv);
-        addmod<NL>(t2, Qk, Qk, M.n);
-        submod<NL>(V, t1, t2, M.n);
-        montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
-        M.count += 3;
-        if ((word >> b) & 1u) {
-            uint32_t nu[NL], nv[NL];
-            addmod<NL>(nu, U, V, M.n);
-            halfmod<NL>(nu, M.n);
-            montmul<NL>(t1, Dm, U, M.n, M.ninv);
-            addmod<NL>(nv, t1, V, M.n);
-            halfmod<NL>(nv, M.n);
+        const bool bit = (word >> b) & 1u;
+        uint32_t X[NL], Y[NL], S[NL];
+        montmul<NL>(t1, V0, V1, M.n, M.ninv);
+        submod<NL>(t1, t1, Qk, M.n);                // V_2k+1
+        montmul<NL>(t2, Qk, Qm, M.n, M.ninv);       // Q^(k+1)
 #pragma unroll
-            for (int i = 0; i < NL; i++) { U[i] = nu[i]; V[i] = nv[i]; }
-            montmul<NL>(Qk, Qk, Qm, M.n, M.ninv);
-            M.count += 2;
-        }
+        for (int i = 0; i < NL; i++) { X[i] = bit ? V1[i] : V0[i]; Y[i] = bit ? t2[i] : Qk[i]; }
+        montmul<NL>(S, X, X, M.n, M.ninv);
+        dblmod<NL>(X, Y, M.n);
+        submod<NL>(S, S, X, M.n);                   // V_2k (bit 0) or V_2k+2 (bit 1)
+        montmul<NL>(Qk, Qk, Y, M.n, M.ninv);        // Q^2k or Q^(2k+1)
+#pragma unroll
+        for (int i = 0; i < NL; i++) { V0[i] = bit ? t1[i] : S[i]; V1[i] = bit ? S[i] : t1[i]; }
+        M.count += 4;
       }
     }
-    if (is_zero<NL>(U) || is_zero<NL>(V)) return true;
+    // V0 = V_d, V1 = V_(d+1), Qk = Q^d
+    dblmod<NL>(t1, V1, M.n);
+    if (eq<NL>(t1, V0) || is_zero<NL>(V0)) return true;
     for (int r = 1; r < s; r++) {
-        montmul<NL>(t1, V, V, M.n, M.ninv);
-        addmod<NL>(t2, Qk, Qk, M.n);
-        submod<NL>(V, t1, t2, M.n);
-        if (is_zero<NL>(V)) return true;
+        montmul<NL>(t1, V0, V0, M.n, M.ninv);
+        dblmod<NL>(t2, Qk, M.n);
+        submod<NL>(V0, t1, t2, M.n);
+        if (is_zero<NL>(V0)) return true;
         montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
         M.count += 2;
     }
@@ -681,9 +687,13 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
-__device__ __forceinline__ void walk_count_mm(uint32_t mm) {
+__device__ __forceinline__ void walk_count_mm(uint32_t mm, uint32_t words) {
     const uint32_t tot = __reduce_add_sync(0xFFFFFFFFu, mm);
-    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&g_modmul_count, (unsigned long long)tot);
+    const uint32_t wtot = __reduce_add_sync(0xFFFFFFFFu, words);
+    if ((threadIdx.x & 31) == 0 && tot) {
+        atomicAdd(&g_modmul_count, (unsigned long long)tot);
+        atomicAdd(&g_wordmul_count, (unsigned long long)wtot);
+    }
 }
 
 // member found prime: count it, continue with 2p + 1 or end the walk
@@ -788,7 +798,7 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
         Big b;
         int nbits = 0;
         bool prime = false, to_lucas = false;
-        uint32_t mm = 0;
+        uint32_t mm = 0, words = 0;
         if (live) {
             it = src[off + i];
 #pragma unroll
@@ -797,7 +807,7 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
             Mont<NL> M;
             mont_setup<NL>(M, b, nbits);
             M.count = 0;
-            if (stage == 0) {
+                    if (stage == 0) {
                 if (pc.primality == CCS_PRIME_BPSW) {
                     to_lucas = strong_prp<NL>(M, b, 2);
                 } else {
@@ -808,9 +818,10 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
                 prime = strong_lucas<NL>(M, b);
             }
             mm = M.count;
+            words = M.count * (2 * NL * NL + NL);
             if (!prime && !to_lucas) a.lengths[it.idx] = it.len;
         }
-        walk_count_mm(mm);
+        walk_count_mm(mm, words);
         if (stage == 0) {
             const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas);
             if (to_lucas) a.lucas[off + pos] = it;
@@ -851,14 +862,17 @@ cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, uint32_t primal
     return cudaGetLastError();
 }
 
-cudaError_t modmul_count(uint64_t* out, bool reset) {
-    unsigned long long v = 0;
+cudaError_t modmul_count(uint64_t* out, uint64_t* words, bool reset) {
+    unsigned long long v = 0, w = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&v, g_modmul_count, sizeof(v));
+    if (e == cudaSuccess) e = cudaMemcpyFromSymbol(&w, g_wordmul_count, sizeof(w));
     if (e != cudaSuccess) return e;
-    *out = v;
+    if (out) *out = v;
+    if (words) *words = w;
     if (reset) {
         v = 0;
         e = cudaMemcpyToSymbol(g_modmul_count, &v, sizeof(v));
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_wordmul_count, &v, sizeof(v));
     }
     return e;
 }

@@ -317,6 +317,11 @@ ccs_status ccs_measure_imad_peak(int device, double* tops);
  * since the last reset (reset != 0 clears after reading). */
 ccs_status ccs_walk_modmuls(ccs_engine* eng, uint64_t* count, int reset);
 
+/* The same count together with the 32 x 32-bit word products those
+ * Montgomery products executed (2 NL^2 + NL per product for NL limbs); each
+ * word product is one IMAD lo/hi pair. */
+ccs_status ccs_walk_word_products(ccs_engine* eng, uint64_t* modmuls, uint64_t* words, int reset);
+
 #ifdef __cplusplus
 }
 #endif
