@@ -129,7 +129,14 @@ class _RequestResult(C.Structure):
 class _Tuning(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("unit_words", C.c_uint32), ("split_prime", C.c_uint32),
-                ("ext_min_words", C.c_uint32), ("_pad", C.c_uint32)]
+                ("ext_min_words", C.c_uint32), ("table_primes", C.c_uint32)]
+
+
+class _TunePoint(C.Structure):
+    _fields_ = [("tuning", _Tuning), ("n_tiles", C.c_uint64), ("ms", C.c_float), ("_pad", C.c_uint32)]
+
+
+TUNE_LATTICE, TUNE_STAGES, TUNE_UNITS, TUNE_SHAPE, TUNE_ALL = 1, 2, 4, 8, 15
 
 
 # exported symbols of include/ccs.h, with their ctypes signatures
@@ -170,6 +177,8 @@ _SIGS = {
     "ccs_walk_modmuls": (C.c_int, [_vp, C.POINTER(_u64), C.c_int]),
     "ccs_walk_word_products": (C.c_int, [_vp, C.POINTER(_u64), C.POINTER(_u64), C.c_int]),
     "ccs_set_tuning": (C.c_int, [_vp, C.POINTER(_Tuning)]),
+    "ccs_autotune": (C.c_int, [_vp, _u64, _u64, _u64, C.c_uint32, C.POINTER(_TunePoint), C.c_uint32,
+                               C.POINTER(C.c_uint32), C.POINTER(_Tuning)]),
 }
 
 _LIB = None
@@ -365,6 +374,20 @@ class Engine:
         for k, v in kw.items():
             setattr(t, k, v)
         _check(load_library().ccs_set_tuning(self.h, C.byref(t)), "ccs_set_tuning")
+
+    def autotune(self, tile_start, n_tiles, what=TUNE_ALL, cap=256):
+        """Project autotuner: times the filter on [tile_start, tile_start +
+        n_tiles) under candidate tunings (stage splits, lattice threshold,
+        positions per thread, block shape), keeps the fastest on the engine
+        and returns (chosen tuning dict, [(tuning dict, n_tiles, ms), ...])."""
+        pts = (_TunePoint * cap)()
+        n = C.c_uint32(0)
+        t = _Tuning()
+        lo, hi = _split128(tile_start)
+        _check(load_library().ccs_autotune(self.h, lo, hi, n_tiles, what, pts, cap, C.byref(n), C.byref(t)),
+               "ccs_autotune")
+        as_dict = lambda x: {f: getattr(x, f) for f, _ in _Tuning._fields_}
+        return as_dict(t), [(as_dict(p.tuning), p.n_tiles, p.ms) for p in pts[:min(n.value, cap)]]
 
     # --- device path -------------------------------------------------------
     def filter_range(self, tile_start, n_tiles, cap=1 << 20, out=None, stream=None):

@@ -79,7 +79,7 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride);
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
-                         uint32_t b_stride, uint32_t grid, cudaStream_t st);
+                         uint32_t b_stride, uint32_t grid, uint32_t block_threads, cudaStream_t st);
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
 // breadth-first chain walk (prove.cu)
 struct WalkItem {
@@ -108,7 +108,7 @@ struct WalkArgs {
 cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
                              WalkItem* out, cudaStream_t st);
 cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, uint32_t primality, cudaStream_t st);
-int sweep_blocks_per_sm(uint32_t b_stride);
+int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads);
 cudaError_t modmul_count(uint64_t* out, uint64_t* words, bool reset);
 
 }  // namespace ccs

@@ -105,6 +105,7 @@ struct ccs_engine {
     cudaStream_t own_stream = nullptr;
     int slot = -1;                   // == fs[0].slot: prove-side constants
     HostProfile& hp = fs[0].hp;      // the profile as given
+    int users = 0;                   // batches / servers referencing the tables
 
     DevBuf<uint64_t> bases;
 
@@ -250,6 +251,68 @@ uint32_t b_stride_of(uint32_t nB) {
     return (s + 7) & ~7u;
 }
 
+uint32_t max_level_b(const ccs_engine* E) {
+    uint32_t nb = 0;
+    for (int v = 0; v < E->n_fs; v++) nb = std::max<uint32_t>(nb, (uint32_t)E->fs[v].hp.primesB.size());
+    return nb;
+}
+
+// resident sweep blocks per SM for a block size (at least 1)
+uint32_t max_blocks_per_sm(const ccs_engine* E, uint32_t block_threads) {
+    const int bps = sweep_blocks_per_sm(b_stride_of(max_level_b(E)), block_threads);
+    return bps > 0 ? (uint32_t)bps : 1u;
+}
+
+// (Re)builds the engine's filter sets for a level-B/C split prime and a
+// table-window count: the profile as given (fs[0]) and, when its smallest
+// bit-sliced prime q0 is below 64, the extended lattice that absorbs q0
+// (fs[1]).  Tables are uploaded into the engine's constant-memory slots
+// (allocated on first use).  The engine stream is drained first.
+ccs_status build_filters(ccs_engine* E, uint32_t split, uint32_t t_count) {
+    HostProfile nh[2];
+    auto params_of = [&](HostProfile& d) {
+        const HostProfile& s = E->fs[0].hp;
+        d.target = s.target; d.depth = s.depth; d.bits = s.bits;
+        d.crt = s.crt; d.wheel = s.wheel; d.stages = s.stages;
+        d.max_bases = s.max_bases; d.witnesses = s.witnesses;
+        d.primality = s.primality; d.prove_mode = s.prove_mode;
+        d.t_count = t_count;
+    };
+    params_of(nh[0]);
+    std::string err = build_profile(nh[0], split);
+    if (!err.empty()) return fail(CCS_ERR_INVALID, err);
+    if (nh[0].primesB.size() > (size_t)kMaxLevelB) return fail(CCS_ERR_INVALID, "too many level-B primes");
+    int n_new = 1;
+    if (nh[0].A[0].q > 1 && nh[0].A[0].q < 64) {
+        params_of(nh[1]);
+        if (build_profile(nh[1], split, nh[0].A[0].q).empty() && nh[1].primesB.size() <= (size_t)kMaxLevelB)
+            n_new = 2;
+    }
+    if (E->own_stream) CU(cudaStreamSynchronize(E->own_stream));
+    for (int v = 0; v < 2; v++) {
+        if (v < n_new && E->fs[v].slot < 0) {
+            E->fs[v].slot = alloc_slot(E->device);
+            if (E->fs[v].slot < 0)
+                return fail(CCS_ERR_BUSY, "all constant-memory profile slots in use (max 16 filter profiles per device)");
+        }
+        if (v >= n_new && E->fs[v].slot >= 0) { free_slot(E->device, E->fs[v].slot); E->fs[v].slot = -1; }
+        E->fs[v].free_();
+    }
+    uint32_t max_np = 0;
+    for (int v = 0; v < n_new; v++) {
+        E->fs[v].hp = nh[v];
+        ccs_status st = upload_filter(E->fs[v], E->own_stream);
+        if (st != CCS_OK) return st;
+        max_np = std::max<uint32_t>(max_np, (uint32_t)nh[v].range_primes.size());
+    }
+    E->n_fs = n_new;
+    E->slot = E->fs[0].slot;
+    if (E->d_jmod.n < max_np) CU(E->d_jmod.alloc(max_np));
+    E->tune.split_prime = split;
+    E->tune.table_primes = t_count;
+    return CCS_OK;
+}
+
 // work units for one range
 uint64_t units_of(const FilterSet& f, uint32_t n_words, uint32_t unit_words) {
     uint64_t groups = (f.hp.lines.size() + 31) / 32;
@@ -262,7 +325,7 @@ uint64_t units_of(const FilterSet& f, uint32_t n_words, uint32_t unit_words) {
 uint32_t choose_unit_words(const ccs_engine* E, const FilterSet& f, uint32_t n_words) {
     uint32_t uw = E->tune.unit_words ? E->tune.unit_words : 1024;
     uint64_t groups = (f.hp.lines.size() + 31) / 32;
-    uint64_t warps = (uint64_t)E->sms * std::max<uint32_t>(E->tune.blocks_per_sm, 1) * (kSweepThreads / 32);
+    uint64_t warps = (uint64_t)E->sms * std::max<uint32_t>(E->tune.blocks_per_sm, 1) * (E->tune.block_threads / 32);
     uint64_t chunks_wanted = (4 * warps + groups - 1) / groups;
     if (chunks_wanted > 1) {
         uint64_t fit = (n_words + chunks_wanted - 1) / chunks_wanted;
@@ -408,48 +471,22 @@ ccs_status ccs_create(const ccs_params* params, int device, ccs_engine** out) {
     E->tune.unit_words = 1024;
     E->tune.split_prime = 1024;
     E->tune.ext_min_words = 256;
-    // extended filter set: absorb the smallest bit-sliced prime when it is
-    // below 64 (one 64-bit window) and the lattice stays within 62 bits
-    if (hp.A[0].q > 1 && hp.A[0].q < 64) {
-        HostProfile& hx = E->fs[1].hp;
-        hx.target = hp.target; hx.depth = hp.depth; hx.bits = hp.bits;
-        hx.crt = hp.crt; hx.wheel = hp.wheel; hx.stages = hp.stages;
-        hx.max_bases = hp.max_bases; hx.witnesses = hp.witnesses;
-        hx.primality = hp.primality; hx.prove_mode = hp.prove_mode;
-        if (build_profile(hx, 1024, hp.A[0].q).empty() && hx.primesB.size() <= (size_t)kMaxLevelB)
-            E->n_fs = 2;
-    }
-    for (int v = 0; v < E->n_fs; v++) {
-        E->fs[v].slot = alloc_slot(device);
-        if (E->fs[v].slot < 0) {
-            ccs_destroy(E);
-            return fail(CCS_ERR_BUSY, "all constant-memory profile slots in use (max 16 filter profiles per device)");
-        }
-    }
-    E->slot = E->fs[0].slot;
+    E->tune.table_primes = 0;
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, device));
     E->sms = prop.multiProcessorCount;
     CU(cudaStreamCreateWithFlags(&E->own_stream, cudaStreamNonBlocking));
-    for (int v = 0; v < E->n_fs; v++) {
-        ccs_status st = upload_filter(E->fs[v], E->own_stream);
-        if (st != CCS_OK) { ccs_destroy(E); return st; }
-    }
     {
-        ccs_status st = upload_prove(E, E->own_stream);
+        ccs_status st = build_filters(E, 1024, 0);
+        if (st != CCS_OK) { ccs_destroy(E); return st; }
+        st = upload_prove(E, E->own_stream);
         if (st != CCS_OK) { ccs_destroy(E); return st; }
     }
-    uint32_t max_np = 0, max_nb = 0;
-    for (int v = 0; v < E->n_fs; v++) {
-        max_np = std::max<uint32_t>(max_np, (uint32_t)E->fs[v].hp.range_primes.size());
-        max_nb = std::max<uint32_t>(max_nb, (uint32_t)E->fs[v].hp.primesB.size());
-    }
-    int bps = sweep_blocks_per_sm(b_stride_of(max_nb));
-    E->tune.blocks_per_sm = bps > 0 ? (uint32_t)bps : 1;
+    E->tune.blocks_per_sm = max_blocks_per_sm(E, E->tune.block_threads);
 
     // plain-path state
     if (E->d_range.alloc(1) || E->d_prange.alloc(1) || E->d_prefix.alloc(2) || E->d_hdr.alloc(1) ||
-        E->d_jmod.alloc(max_np) || E->d_counters.alloc(8)) {
+        E->d_counters.alloc(8)) {
         ccs_destroy(E);
         return fail(CCS_ERR_NOMEM, "device allocation failed");
     }
@@ -502,14 +539,27 @@ ccs_status ccs_get_tuning(const ccs_engine* E, ccs_tuning* t) {
 
 ccs_status ccs_set_tuning(ccs_engine* E, const ccs_tuning* t) {
     if (!E || !t) return fail(CCS_ERR_INVALID, "null argument");
-    if (t->block_threads && t->block_threads != (uint32_t)kSweepThreads)
-        return fail(CCS_ERR_INVALID, "block_threads is fixed at 256 in this build");
+    if (t->block_threads && t->block_threads != 128 && t->block_threads != 256)
+        return fail(CCS_ERR_INVALID, "block_threads must be 128 or 256");
     if (t->unit_words > (1u << 20)) return fail(CCS_ERR_INVALID, "unit_words too large");
-    if (t->split_prime && t->split_prime != E->tune.split_prime)
-        return fail(CCS_ERR_INVALID, "split_prime is fixed at engine creation");
+    if (t->split_prime && (t->split_prime < 128 || t->split_prime > (1u << 16)))
+        return fail(CCS_ERR_INVALID, "split_prime must be in [128, 65536]");
+    if (t->table_primes && t->table_primes != 7 && t->table_primes != (uint32_t)kNumT)
+        return fail(CCS_ERR_INVALID, "table_primes must be 0, 7 or 22");
+    const uint32_t split = t->split_prime ? t->split_prime : E->tune.split_prime;
+    const uint32_t tabl = t->table_primes ? t->table_primes : E->tune.table_primes;
+    if (split != E->tune.split_prime || tabl != E->tune.table_primes) {
+        if (E->users) return fail(CCS_ERR_BUSY, "engine tables are in use by a batch or server");
+        CU(cudaSetDevice(E->device));
+        ccs_status st = build_filters(E, split, tabl);
+        if (st != CCS_OK) return st;
+    }
+    if (t->block_threads) E->tune.block_threads = t->block_threads;
     if (t->unit_words) E->tune.unit_words = t->unit_words;
     if (t->blocks_per_sm) E->tune.blocks_per_sm = t->blocks_per_sm;
     if (t->ext_min_words) E->tune.ext_min_words = t->ext_min_words;
+    const uint32_t mx = max_blocks_per_sm(E, E->tune.block_threads);
+    if (E->tune.blocks_per_sm > mx) E->tune.blocks_per_sm = mx;
     return CCS_OK;
 }
 
@@ -544,11 +594,12 @@ static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_t
                           (uint32_t)hp.range_primes.size(), E->d_jmod.p,
                           (uint32_t)hp.range_primes.size(), st));
     uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
-    uint64_t need = (units + (kSweepThreads / 32) - 1) / (kSweepThreads / 32);
+    const uint32_t wpb = E->tune.block_threads / 32;
+    uint64_t need = (units + wpb - 1) / wpb;
     if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
     CU(launch_sweep(E->d_range.p, E->d_prefix.p, E->d_hdr.p, E->d_jmod.p,
                     (uint32_t)hp.range_primes.size(), b_stride_of((uint32_t)hp.primesB.size()),
-                    grid, st));
+                    grid, E->tune.block_threads, st));
     return CCS_OK;
 }
 
@@ -819,10 +870,11 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
         CU(cudaMemcpyAsync(d_hdr, &hh, sizeof(hh), cudaMemcpyHostToDevice, st));
         CU(launch_range_setup(d_range, d_hdr, 1, f.range_primes.p, np, d_jmod, np, st));
         uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
-        const uint64_t need = (units + (kSweepThreads / 32) - 1) / (kSweepThreads / 32);
+        const uint32_t wpb = E->tune.block_threads / 32;
+        const uint64_t need = (units + wpb - 1) / wpb;
         if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
         CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, b_stride_of((uint32_t)hp.primesB.size()),
-                        grid, st));
+                        grid, E->tune.block_threads, st));
         E->launches += 2;
     }
     uint32_t cnt = 0;
@@ -834,12 +886,177 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
 }
 
 // ---------------------------------------------------------------------------
+// autotuner
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Tuner {
+    ccs_engine* E;
+    unsigned __int128 ts;
+    ccs_tune_point* points;
+    uint32_t cap, n = 0;
+    DevBuf<uint32_t> out;
+    uint64_t out_cap = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+    // device time of one filter launch over n_tiles tiles (best of two after
+    // a warm-up run); -1 on error
+    float time(uint64_t n_tiles) {
+        cudaStream_t st = E->own_stream;
+        float best = -1.0f;
+        for (int rep = 0; rep < 3; rep++) {
+            if (cudaMemsetAsync(E->d_counters.p, 0, 4, st) != cudaSuccess) return -1.0f;
+            if (cudaEventRecord(e0, st) != cudaSuccess) return -1.0f;
+            if (filter_chunk(E, ts, n_tiles, 0, (ccs_survivor*)out.p, out_cap, st) != CCS_OK) return -1.0f;
+            if (cudaEventRecord(e1, st) != cudaSuccess) return -1.0f;
+            if (cudaEventSynchronize(e1) != cudaSuccess) return -1.0f;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0 && (best < 0 || ms < best)) best = ms;
+        }
+        return best;
+    }
+    float record(uint64_t n_tiles) {
+        const float ms = time(n_tiles);
+        if (n < cap && points) {
+            points[n].tuning = E->tune;
+            points[n].n_tiles = n_tiles;
+            points[n].ms = ms;
+            points[n]._pad = 0;
+        }
+        n++;
+        return ms;
+    }
+};
+
+}  // namespace
+
+ccs_status ccs_autotune(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint64_t n_tiles, uint32_t what,
+                        ccs_tune_point* points, uint32_t cap, uint32_t* n_points, ccs_tuning* chosen) {
+    if (!E) return fail(CCS_ERR_INVALID, "null engine");
+    if (n_tiles == 0 || n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be in [1, 2^32)");
+    if (cap && !points) return fail(CCS_ERR_INVALID, "points is null");
+    if (what == 0) what = CCS_TUNE_ALL;
+    if ((what & CCS_TUNE_STAGES) && E->users) return fail(CCS_ERR_BUSY, "engine tables are in use by a batch or server");
+    const unsigned __int128 ts = mk128(ts_lo, ts_hi);
+    if (ts + n_tiles < ts) return fail(CCS_ERR_INVALID, "tile range wraps 2^128");
+    CU(cudaSetDevice(E->device));
+    Tuner T;
+    T.E = E;
+    T.ts = ts;
+    T.points = points;
+    T.cap = cap;
+    {
+        // survivor buffer: 4x the expected count, at least 2^16, at most 2^24
+        uint64_t cpt = 0;
+        for (uint32_t w : E->hp.wheel_total) cpt += w;
+        cpt /= 6;
+        const double expect = (double)n_tiles * (double)cpt * E->hp.pass_rate;
+        T.out_cap = (uint64_t)std::min(std::max(4.0 * expect, 65536.0), 16777216.0);
+        CU(T.out.alloc(4 * T.out_cap));
+    }
+    CU(cudaEventCreate(&T.e0));
+    CU(cudaEventCreate(&T.e1));
+    ccs_status status = CCS_OK;
+    auto finish = [&]() {
+        cudaEventDestroy(T.e0);
+        cudaEventDestroy(T.e1);
+        T.out.free_();
+    };
+    auto set = [&](const ccs_tuning& t) {
+        ccs_status s = ccs_set_tuning(E, &t);
+        if (s != CCS_OK) status = s;
+        return s == CCS_OK;
+    };
+    ccs_tuning best = E->tune;
+    float best_ms = T.record(n_tiles);
+    if (best_ms < 0) { finish(); return fail(CCS_ERR_CUDA, "probe launch failed"); }
+
+    // stage-split thresholds: level-B/C split and table-window count
+    if ((what & CCS_TUNE_STAGES) && status == CCS_OK) {
+        const uint32_t splits[3] = {512, 1024, 2048};
+        const uint32_t tables[2] = {7, (uint32_t)kNumT};
+        for (uint32_t sp : splits)
+            for (uint32_t tb : tables) {
+                ccs_tuning t = best;
+                t.split_prime = sp;
+                t.table_primes = tb;
+                if (!set(t)) { status = CCS_OK; continue; }   // e.g. too many level-B primes
+                const float ms = T.record(n_tiles);
+                if (ms > 0 && ms < best_ms) { best_ms = ms; best = E->tune; }
+            }
+        set(best);
+    }
+    // lattice threshold: the smallest probe prefix (n, n/4, n/16, n/64) on
+    // which the extended lattice is faster sets ext_min_words
+    if ((what & CCS_TUNE_LATTICE) && E->n_fs > 1 && status == CCS_OK) {
+        uint32_t threshold = 0xFFFFFFFFu;
+        for (uint64_t len = n_tiles; len >= 64; len /= 4) {
+            ccs_tuning t = best;
+            t.ext_min_words = 0xFFFFFFFFu;
+            set(t);
+            const float plain = T.record(len);
+            t.ext_min_words = 1;
+            set(t);
+            const float ext = T.record(len);
+            if (ext > 0 && plain > 0 && ext < plain) {
+                const uint32_t q0 = E->fs[1].hp.q0;
+                const uint64_t span = (len + 5) / 6 + 1;
+                threshold = (uint32_t)(((span + q0 - 1) / q0 + 63) / 64);
+            } else {
+                break;
+            }
+            if (len / 4 < 64) break;
+        }
+        best.ext_min_words = threshold;
+        set(best);
+        best_ms = T.time(n_tiles);
+    }
+    // positions per thread and work unit
+    if ((what & CCS_TUNE_UNITS) && status == CCS_OK) {
+        const uint32_t units[6] = {128, 256, 512, 1024, 2048, 4096};
+        const ccs_tuning base = best;
+        for (uint32_t uw : units) {
+            ccs_tuning t = base;
+            t.unit_words = uw;
+            set(t);
+            const float ms = T.record(n_tiles);
+            if (ms > 0 && ms < best_ms) { best_ms = ms; best = E->tune; }
+        }
+        set(best);
+    }
+    // block shape
+    if ((what & CCS_TUNE_SHAPE) && status == CCS_OK) {
+        const ccs_tuning base = best;
+        for (uint32_t bt : {128u, 256u}) {
+            const uint32_t mx = max_blocks_per_sm(E, bt);
+            for (uint32_t b = 1; b <= mx; b++) {
+                ccs_tuning t = base;
+                t.block_threads = bt;
+                t.blocks_per_sm = b;
+                set(t);
+                if (E->tune.block_threads != bt || E->tune.blocks_per_sm != b) continue;
+                const float ms = T.record(n_tiles);
+                if (ms > 0 && ms < best_ms) { best_ms = ms; best = E->tune; }
+            }
+        }
+        set(best);
+    }
+    finish();
+    if (status != CCS_OK) return status;
+    if (n_points) *n_points = T.n;
+    if (chosen) *chosen = E->tune;
+    return CCS_OK;
+}
+
+// ---------------------------------------------------------------------------
 // batched executor
 // ---------------------------------------------------------------------------
 ccs_status ccs_batch_destroy(ccs_batch* b) {
     if (!b) return CCS_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto* E : b->prof) E->users--;
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->d_ranges.free_(); b->d_pranges.free_(); b->d_prefix.free_(); b->d_hdr.free_();
@@ -860,9 +1077,11 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     *out = nullptr;
     ccs_batch* b = new ccs_batch();
     b->device = profiles[0]->device;
-    for (uint32_t i = 0; i < n_profiles; i++) {
+    for (uint32_t i = 0; i < n_profiles; i++)
         if (!profiles[i] || profiles[i]->device != b->device) { delete b; return fail(CCS_ERR_INVALID, "profiles must share one device"); }
+    for (uint32_t i = 0; i < n_profiles; i++) {
         b->prof.push_back(profiles[i]);
+        profiles[i]->users++;
     }
     CU(cudaSetDevice(b->device));
     b->max_ranges = max_ranges;
@@ -906,7 +1125,8 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     CU(cudaEventCreate(&b->ev0));
     CU(cudaEventCreate(&b->ev1));
-    int bps = sweep_blocks_per_sm(b->b_stride);
+    const uint32_t bt = b->prof[0]->tune.block_threads;
+    int bps = sweep_blocks_per_sm(b->b_stride, bt);
     b->grid = (uint32_t)b->prof[0]->sms * (uint32_t)std::max(bps, 1);
 
     // record the whole batch once: H2D descriptors, setup, sweep, level C,
@@ -921,7 +1141,7 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     launch_range_setup(b->d_ranges.p, b->d_hdr.p, max_ranges, b->d_primes.p, b->max_range_primes,
                        b->d_jmod.p, b->jstride, st);
     launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, b->b_stride,
-                 b->grid, st);
+                 b->grid, bt, st);
     ProveArgs pa;
     pa.ranges = b->d_pranges.p;
     pa.surv = b->d_surv.p;

@@ -508,18 +508,19 @@ static cudaError_t ensure_sweep_attr() {
     return e;
 }
 
-int sweep_blocks_per_sm(uint32_t b_stride) {
+int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads) {
     int nb = 0;
     if (ensure_sweep_attr() != cudaSuccess) return 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel, kSweepThreads,
-                                                  sweep_smem_bytes(kSweepThreads, b_stride));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel, (int)block_threads,
+                                                  sweep_smem_bytes(block_threads, b_stride));
     return nb;
 }
 
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
-                         uint32_t b_stride, uint32_t grid, cudaStream_t st) {
-    size_t smem = sweep_smem_bytes(kSweepThreads, b_stride);
+                         uint32_t b_stride, uint32_t grid, uint32_t block_threads, cudaStream_t st) {
+    if (block_threads != 128 && block_threads != 256) return cudaErrorInvalidValue;
+    size_t smem = sweep_smem_bytes(block_threads, b_stride);
     cudaError_t e = ensure_sweep_attr();
     if (e != cudaSuccess) return e;
     SweepArgs a;
@@ -529,7 +530,7 @@ cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
     a.jmod = jmod;
     a.jmod_stride = stride;
     a.b_stride = b_stride;
-    sweep_kernel<<<grid, kSweepThreads, smem, st>>>(a);
+    sweep_kernel<<<grid, block_threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -246,6 +246,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             }
         }
         nT_max = nt <= 14 ? std::min(7, avail) : std::min(kNumT, avail);
+        if (hp.t_count) nT_max = std::min<int>((int)hp.t_count, avail);
     }
     for (auto& fp : hp.fprimes) {
         uint32_t q = fp.q;

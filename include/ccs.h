@@ -287,20 +287,56 @@ ccs_status ccs_server_stats(ccs_server* s, uint64_t* out6);
 /* ---- tuning -------------------------------------------------------------- */
 
 typedef struct {
-    uint32_t block_threads;   /* threads per block of the filter sweep */
+    uint32_t block_threads;   /* threads per block of the filter sweep: 128 or 256 */
     uint32_t blocks_per_sm;   /* resident blocks requested per SM */
-    uint32_t unit_words;      /* 64-candidate words per lane per work unit */
-    uint32_t split_prime;     /* first prime tested by the deferred warp-cooperative stage */
+    uint32_t unit_words;      /* 64-position words each lane sweeps per work unit (one lane
+                               * owns one lattice residue: residues-per-thread = 1, positions
+                               * per thread and unit = 64 x unit_words) */
+    uint32_t split_prime;     /* first prime tested by the deferred warp-cooperative stage
+                               * (changing it rebuilds the engine's filter tables) */
     uint32_t ext_min_words;   /* ranges spanning at least this many 64-position words of
                                * the extended lattice (smallest bit-sliced filter prime
                                * absorbed into the modulus) are swept on it; 1 = every
                                * range, 0xFFFFFFFF = none.  Both lattices give identical
                                * survivors. */
-    uint32_t _pad;
+    uint32_t table_primes;    /* bit-sliced primes above 96 read from a pattern table (7 or
+                               * 22; 0 = chosen by the engine's cost rule; changing it
+                               * rebuilds the filter tables) */
 } ccs_tuning;
 
 ccs_status ccs_get_tuning(const ccs_engine* eng, ccs_tuning* out);
+/* Zero fields keep their value.  A new split_prime or table_primes rebuilds
+ * the engine's tables and is refused (CCS_ERR_BUSY) while a batch or server
+ * uses the engine. */
 ccs_status ccs_set_tuning(ccs_engine* eng, const ccs_tuning* t);
+
+/* ---- autotuner ------------------------------------------------------------- */
+
+/* One configuration the autotuner measured: the tuning and the device time
+ * of one filter launch over the probe range. */
+typedef struct {
+    ccs_tuning tuning;
+    uint64_t n_tiles;         /* probe size of this measurement */
+    float ms;
+    uint32_t _pad;
+} ccs_tune_point;
+
+#define CCS_TUNE_LATTICE 1u   /* plain vs extended lattice: the ext_min_words threshold */
+#define CCS_TUNE_STAGES 2u    /* stage-split thresholds: split_prime, table_primes */
+#define CCS_TUNE_UNITS 4u     /* positions per thread and work unit: unit_words */
+#define CCS_TUNE_SHAPE 8u     /* block shape: block_threads, blocks_per_sm */
+#define CCS_TUNE_ALL 15u
+
+/* Times the filter on [ts, ts + n_tiles) (and, for the lattice threshold, on
+ * shorter prefixes of it) under candidate tunings, one group of knobs after
+ * another, keeps the fastest and leaves it set on the engine.  Every measured
+ * point is written to points (up to cap; n_points gets the total).  Results
+ * of the engine do not depend on the tuning.  Not thread-safe with other
+ * calls on the same engine; refused (CCS_ERR_BUSY) for CCS_TUNE_STAGES while
+ * a batch or server uses the engine. */
+ccs_status ccs_autotune(ccs_engine* eng, uint64_t ts_lo, uint64_t ts_hi, uint64_t n_tiles,
+                        uint32_t what, ccs_tune_point* points, uint32_t cap, uint32_t* n_points,
+                        ccs_tuning* chosen);
 
 /* ---- diagnostics ----------------------------------------------------------- */
 
