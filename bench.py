@@ -252,6 +252,22 @@ def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
             "cpu_baseline": cpu}
 
 
+def autotune_engines(ccs, engines, seed):
+    """Project autotuner on every depth profile: probe of ~2^30 candidates at
+    a seeded 88-bit start (before any batch holds the engines)."""
+    import random
+    r = random.Random(seed)
+    out = []
+    t0 = time.time()
+    for e in engines:
+        info = e.info
+        nt = max(1024, (1 << 30) // info["candidates_per_tile"])
+        lo, hi = ccs.bit_tile_range(88, e.bases(), info["lattice_m"], info["wheel_period"])
+        chosen, pts = e.autotune(r.randint(lo, hi - nt - 1), nt)
+        out.append({"depth": info["depth"], "chosen": chosen, "points": len(pts)})
+    return {"seconds": time.time() - t0, "engines": out}
+
+
 def section_batched(ccs, engines, n_ranges=4096):
     """Uneven ranges: one batched graph replay versus per-range plain calls."""
     ranges = ccs.mixed_ranges(engines, n_ranges, SEED + 11)
@@ -364,11 +380,19 @@ def run_ours(args):
     cfg = ccs.config_cc16_scale()
     eng = ccs.Engine(device=local, **cfg)
     TILES = args.tiles_per_step
+    info = eng.info
+    tune_report = None
+    if not args.no_autotune:
+        # project autotuner on a 2^22-tile probe away from the timed tiles
+        bases0 = eng.bases()
+        lo0, hi0 = ccs.bit_tile_range(BITS, bases0, info["lattice_m"], info["wheel_period"])
+        t_tune = time.time()
+        chosen, pts = eng.autotune(lo0 + 1000, 1 << 22)
+        tune_report = {"probe_tiles": 1 << 22, "points": len(pts), "seconds": time.time() - t_tune}
     if args.unit_words:
         eng.set_tuning(unit_words=args.unit_words)
     if args.ext_min_words:
         eng.set_tuning(ext_min_words=args.ext_min_words)
-    info = eng.info
     cpt = info["candidates_per_tile"]
     bases = eng.bases()
     t_lo, t_hi = ccs.bit_tile_range(BITS, bases, info["lattice_m"], info["wheel_period"])
@@ -470,6 +494,11 @@ def run_ours(args):
         except Exception as ex:                       # report, keep the headline
             extra["prove"] = {"error": repr(ex)}
         depth_engines = [ccs.Engine(device=local, **ccs.config_depth_profile(d)) for d in range(14, 20)]
+        if not args.no_autotune:
+            try:
+                extra["autotune_depth_profiles"] = autotune_engines(ccs, depth_engines, SEED + 5)
+            except Exception as ex:
+                extra["autotune_depth_profiles"] = {"error": repr(ex)}
         try:
             extra["batched"] = section_batched(ccs, depth_engines, args.batch_ranges)
         except Exception as ex:
@@ -489,7 +518,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "tiles_per_step": TILES,
                        "candidates_per_step": cand_step, "bits": BITS, "seed": SEED,
                        "start_tile": start, "l2": "flushed (512 MB write) between timed steps",
-                       "parallelism": f"lanes{ws}", "tuning": eng.tuning()},
+                       "parallelism": f"lanes{ws}", "tuning": eng.tuning(), "autotune": tune_report},
             "survivors": n_surv, "chains": n_chain, "primes": n_prime,
             "survivor_rate": n_surv / (args.steps * cand_step),
             "roofline": {"bound": "int32", "achieved": achieved, "peak": int_peak, "unit": "TOPS",
@@ -524,6 +553,7 @@ def main():
     ap.add_argument("--tiles-per-step", type=int, default=TILES_PER_STEP,
                     help="tiles per step (smaller values: profiling cases)")
     ap.add_argument("--unit-words", type=int, default=0, help="sweep work-unit length (0: tuned)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default tuning")
     ap.add_argument("--ext-min-words", type=lambda v: int(v, 0), default=0,
                     help="extended-lattice threshold in 64-position words (0: engine default, "
                          "0xFFFFFFFF: plain lattice only)")

@@ -81,6 +81,11 @@ struct Line {
     uint32_t bc;         // base_idx | (c << 16) | (d << 19)   (c = tile mod 6)
 };
 
+// Per-slot constants of the line phase table.
+struct alignas(16) SlotConst {
+    uint32_t q, magic, c32, winv;   // magic = floor((2^32 - 1) / q), c32 = 2^32 mod q, winv = W^-1 mod q
+};
+
 // Constant-memory image of one profile (lattice + filter).
 struct ProfileConst {
     uint64_t W;                      // 6*M*WP (times q0 on an extended profile)
@@ -99,7 +104,20 @@ struct ProfileConst {
     uint32_t std_a;                  // 1: level-A slots hold the standard set 37..127
     const PrimeC* primesC;           // level C primes (ascending)
     const uint32_t* listC;           // sorted G_q lists of level C primes
+    // line phases r W^-1 mod q, [line][ptab_stride] u16 (null: computed per
+    // work unit): level-A slot i at i, level-B prime p at kSlotB + p; and the
+    // constants of those ptab_stride slots
+    const uint16_t* ptab;
+    const SlotConst* pq;
+    uint32_t ptab_stride;
+    uint32_t _ptpad;
 };
+
+// First level-B slot of a line phase table row (level-A slots padded to 8).
+constexpr int kSlotB = (kNumA + 7) / 8 * 8;
+
+// Line phase tables are kept when they need at most this many bytes.
+constexpr size_t kPhaseTableMax = 1ull << 30;
 
 // Host-side profile (everything derived from ccs_params).
 struct HostProfile {

@@ -73,6 +73,8 @@ struct ProveConst {
 
 cudaError_t upload_profile_const(int slot, const ProfileConst& pc, cudaStream_t st);
 cudaError_t upload_prove_const(int slot, const ProveConst& pc, cudaStream_t st);
+cudaError_t launch_phase_table(const Line* lines, uint32_t n_lines, const SlotConst* pq, uint32_t n_slots,
+                               uint16_t* tab, cudaStream_t st);
 cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, uint32_t max_ranges,
                                const uint32_t* primes, uint32_t max_primes, uint32_t* jmod,
                                uint32_t stride, cudaStream_t st);

@@ -83,9 +83,12 @@ struct FilterSet {
     DevBuf<PrimeC> primesB, primesC;
     DevBuf<PrimeB> packB;
     DevBuf<uint32_t> bitmapB, listC, range_primes, patT;
+    DevBuf<uint16_t> ptab;           // line phase table (may stay empty)
+    DevBuf<SlotConst> pq;
     void free_() {
         lines.free_(); primesB.free_(); primesC.free_(); packB.free_();
         bitmapB.free_(); listC.free_(); range_primes.free_(); patT.free_();
+        ptab.free_(); pq.free_();
     }
 };
 
@@ -222,6 +225,28 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     pc.std_a = hp.std_a;
     pc.primesC = f.primesC.p;
     pc.listC = f.listC.p;
+    // line phase table for every level-A slot and level-B prime, when it fits
+    {
+        const uint32_t nb = hp.primesB.empty() ? 1u : (uint32_t)hp.primesB.size();
+        const uint32_t n_slots = kSlotB + ((nb + 7) & ~7u);           // level-B rows as in shared memory
+        const size_t bytes = 2ull * n_slots * hp.lines.size();
+        if (bytes <= kPhaseTableMax && !hp.lines.empty()) {
+            std::vector<SlotConst> pq(n_slots, SlotConst{2u, 0xFFFFFFFFu / 2, 0u, 0u});   // pads: phase 0
+            for (int i = 0; i < kNumA; i++) pq[i] = SlotConst{hp.A[i].q, hp.A[i].magic, hp.A[i].c32, hp.A[i].winv};
+            for (int i = kNumA; i < kSlotB; i++) pq[i] = SlotConst{1u, 0xFFFFFFFFu, 0u, 0u};
+            for (size_t p = 0; p < hp.primesB.size(); p++) {
+                const PrimeC& b = hp.primesB[p];
+                pq[kSlotB + p] = SlotConst{b.q, b.magic, b.c32, b.winv};
+            }
+            CU(f.pq.alloc(n_slots));
+            CU(cudaMemcpy(f.pq.p, pq.data(), sizeof(SlotConst) * n_slots, cudaMemcpyHostToDevice));
+            CU(f.ptab.alloc((size_t)n_slots * hp.lines.size()));
+            CU(launch_phase_table(f.lines.p, (uint32_t)hp.lines.size(), f.pq.p, n_slots, f.ptab.p, st));
+            pc.ptab = f.ptab.p;
+            pc.pq = f.pq.p;
+            pc.ptab_stride = n_slots;
+        }
+    }
     CU(upload_profile_const(f.slot, pc, st));
     CU(cudaStreamSynchronize(st));
     return CCS_OK;
@@ -320,14 +345,14 @@ uint64_t units_of(const FilterSet& f, uint32_t n_words, uint32_t unit_words) {
     return groups * chunks;
 }
 
-// words per work unit: the tuned length, shortened when the range is too
-// small to give every resident warp several units
-uint32_t choose_unit_words(const ccs_engine* E, const FilterSet& f, uint32_t n_words) {
+// words per work unit: the tuned length; when the range runs alone on the
+// GPU (fill_gpu) it is shortened so every resident warp gets several units
+uint32_t choose_unit_words(const ccs_engine* E, const FilterSet& f, uint32_t n_words, bool fill_gpu) {
     uint32_t uw = E->tune.unit_words ? E->tune.unit_words : 1024;
     uint64_t groups = (f.hp.lines.size() + 31) / 32;
     uint64_t warps = (uint64_t)E->sms * std::max<uint32_t>(E->tune.blocks_per_sm, 1) * (E->tune.block_threads / 32);
     uint64_t chunks_wanted = (4 * warps + groups - 1) / groups;
-    if (chunks_wanted > 1) {
+    if (fill_gpu && chunks_wanted > 1) {
         uint64_t fit = (n_words + chunks_wanted - 1) / chunks_wanted;
         if (fit < uw) uw = (uint32_t)std::max<uint64_t>(fit, 32);
     }
@@ -339,7 +364,8 @@ uint32_t choose_unit_words(const ccs_engine* E, const FilterSet& f, uint32_t n_w
 // the extended one when the range spans at least ext_min_words 64-position
 // words of it.  Fills J0, e0, e1, n_tiles, n_words, unit_words, profile and
 // n_range_primes; returns the filter set used.
-const FilterSet& place_range(const ccs_engine* E, unsigned __int128 ts, uint64_t n_tiles, RangeDev& R) {
+const FilterSet& place_range(const ccs_engine* E, unsigned __int128 ts, uint64_t n_tiles, RangeDev& R,
+                             bool fill_gpu = true) {
     const unsigned __int128 J = ts / 6;
     R.e0 = (uint32_t)(ts % 6);
     R.n_tiles = (uint32_t)n_tiles;
@@ -355,7 +381,7 @@ const FilterSet& place_range(const ccs_engine* E, unsigned __int128 ts, uint64_t
     R.e1 = (uint32_t)(J % q0);
     const uint64_t positions = (span + R.e1 + q0 - 1) / q0;
     R.n_words = n_tiles ? (uint32_t)((positions + 63) / 64) : 0;
-    R.unit_words = choose_unit_words(E, f, R.n_words);
+    R.unit_words = choose_unit_words(E, f, R.n_words, fill_gpu);
     R.profile = (uint32_t)f.slot;
     R.n_range_primes = (uint32_t)f.hp.range_primes.size();
     return f;
@@ -852,7 +878,7 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
         hr.e0 = (uint32_t)(cts % 6);
         hr.n_tiles = (uint32_t)nt;
         hr.n_words = words_for(hr.e0, nt);
-        hr.unit_words = choose_unit_words(E, f, hr.n_words);
+        hr.unit_words = choose_unit_words(E, f, hr.n_words, true);
         hr.profile = (uint32_t)f.slot;
         hr.n_range_primes = np;
         hr.surv_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
@@ -1179,7 +1205,7 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
         unsigned __int128 ts = mk128(rg.tile_start_lo, rg.tile_start_hi);
         RangeDev& R = b->h_ranges[i];
         memset(&R, 0, sizeof(R));
-        const FilterSet& f = place_range(E, ts, rg.n_tiles, R);
+        const FilterSet& f = place_range(E, ts, rg.n_tiles, R, false);   // ranges share the GPU
         R.prime_base = b->prime_base[2 * rg.profile + (&f == &E->fs[1] ? 1 : 0)];
         R.surv_cap = (uint32_t)b->surv_cap;
         R.surv_count = cnt;

@@ -59,6 +59,28 @@ __global__ void range_setup_kernel(const RangeDev* __restrict__ ranges,
     (void)n_primes;
 }
 
+// line phases r W^-1 mod q for every (line, slot) of a profile, row per line
+__global__ void phase_table_kernel(const Line* __restrict__ lines, uint32_t n_lines,
+                                   const SlotConst* __restrict__ pq, uint32_t n_slots,
+                                   uint16_t* __restrict__ tab) {
+    const uint64_t total = (uint64_t)n_lines * n_slots;
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t l = (uint32_t)(x / n_slots), s = (uint32_t)(x % n_slots);
+        const SlotConst c = pq[s];
+        const Line ln = lines[l];
+        uint32_t a = mod_magic(ln.r_hi, c.q, c.magic) * c.c32 + mod_magic(ln.r_lo, c.q, c.magic);
+        a = mod_magic(a, c.q, c.magic);
+        tab[x] = (uint16_t)mod_magic(a * c.winv, c.q, c.magic);
+    }
+}
+
+cudaError_t launch_phase_table(const Line* lines, uint32_t n_lines, const SlotConst* pq, uint32_t n_slots,
+                               uint16_t* tab, cudaStream_t st) {
+    phase_table_kernel<<<148 * 8, 256, 0, st>>>(lines, n_lines, pq, n_slots, tab);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // survivor emission
 // ---------------------------------------------------------------------------
@@ -177,13 +199,13 @@ __device__ __forceinline__ void c_process(LevelB& B, const SweepArgs& a, const R
                 const uint32_t rw = mod_magic64((uint64_t)rm * pc.winv, pc.q, pc.magic64);
                 const uint32_t jq = mod_magic64(j, pc.q, pc.magic64);
                 const uint32_t uph = mod_magic64((uint64_t)rw + jm[p] + jq, pc.q, pc.magic64);
-                const uint32_t* lst = P.listC + pc.off;
-                uint32_t lo = 0, hi = pc.cnt;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (__ldg(lst + mid) < uph) lo = mid + 1; else hi = mid;
+                // the padded list, four entries per load, all loads independent
+                const uint4* lst = reinterpret_cast<const uint4*>(P.listC + pc.off);
+                const uint32_t n4 = (pc.cnt + 3) >> 2;
+                for (uint32_t k = 0; k < n4; k++) {
+                    const uint4 v = __ldg(lst + k);
+                    kill |= (v.x == uph) | (v.y == uph) | (v.z == uph) | (v.w == uph);
                 }
-                kill = lo < pc.cnt && __ldg(lst + lo) == uph;
             }
             killed = __any_sync(kFull, kill);
         }
@@ -275,22 +297,72 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         for (uint32_t x = lane; x < (uint32_t)kNumAR * 8; x += 32) PA[x] = P.A[x >> 3].ext[x & 7];
         uint32_t* PT = PA + kNumAR * 8;
         for (uint32_t x = lane; x < P.patT_words; x += 32) PT[x] = __ldg(P.patT + x);
-#pragma unroll
-        for (int i = 0; i < kNumA; i++) {
-            if (STD && i >= kNumAR + kStdNT[STD]) continue;
-            const LevelA& la = P.A[i];
-            const uint32_t q = STD ? kStdQ[STD][i] : la.q;
-            uint32_t ph = 0;
-            if (q > 1) ph = phase_fast(ln.r_lo, ln.r_hi, q, la.magic, la.c32, la.winv, jm[i], jbase);
-            SA[i * 32 + lane] = (uint8_t)ph;
-        }
-        for (uint32_t p = 0; p < P.nBpad; p++) {
-            uint32_t ph = 0;
-            if (p < P.nB) {
-                const PrimeC pc = P.primesB[p];
-                ph = phase_fast(ln.r_lo, ln.r_hi, pc.q, pc.magic, pc.c32, pc.winv, jm[kNumA + p], jbase);
+        if (P.ptab) {
+            // phase = line phase (one table row per line, read with 16-byte
+            // loads) + (J0 + jbase) mod q; the second term is the same for
+            // the warp's 32 lines: one slot per lane, parked as (q << 16 | o)
+            // in the (still empty) queue
+            const uint32_t stride = P.ptab_stride;
+            for (uint32_t s = lane; s < stride; s += 32) {
+                const uint4 c = __ldg(reinterpret_cast<const uint4*>(P.pq) + s);   // q, magic, ...
+                uint32_t j0q = 0;
+                if (s < (uint32_t)kNumA) j0q = jm[s];
+                else if (s >= (uint32_t)kSlotB && s - kSlotB < P.nB) j0q = jm[kNumA + (s - kSlotB)];
+                const uint32_t o = j0q + mod_magic(jbase, c.x, c.y);
+                Qw[s] = (c.x << 16) | (o >= c.x ? o - c.x : o);
             }
-            S[p * 32 + lane] = (uint16_t)ph;
+            __syncwarp();
+            if (has_line) {
+                const uint4* row = reinterpret_cast<const uint4*>(P.ptab + (size_t)li * stride);
+#pragma unroll
+                for (int c = 0; c < kSlotB / 8; c++) {
+                    const uint4 v = __ldg(row + c);
+                    const uint32_t hw[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const int i = c * 8 + k;
+                        if (i >= kNumA || (STD && i >= kNumAR + kStdNT[STD])) continue;
+                        const uint32_t qo = Qw[i], q = qo >> 16;
+                        uint32_t ph = ((hw[k >> 1] >> (16 * (k & 1))) & 0xFFFFu) + (qo & 0xFFFFu);
+                        ph = ph >= q ? ph - q : ph;
+                        SA[i * 32 + lane] = (uint8_t)ph;
+                    }
+                }
+                const uint32_t nbc = (stride - kSlotB) / 8;
+#pragma unroll 4
+                for (uint32_t c = 0; c < nbc; c++) {
+                    const uint4 v = __ldg(row + kSlotB / 8 + c);
+                    const uint32_t hw[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const uint32_t p = c * 8 + k;
+                        const uint32_t qo = Qw[kSlotB + p], q = qo >> 16;
+                        uint32_t ph = ((hw[k >> 1] >> (16 * (k & 1))) & 0xFFFFu) + (qo & 0xFFFFu);
+                        ph = ph >= q ? ph - q : ph;
+                        S[p * 32 + lane] = (uint16_t)ph;
+                    }
+                }
+            }
+            __syncwarp();
+        } else {
+#pragma unroll
+            for (int i = 0; i < kNumA; i++) {
+                if (STD && i >= kNumAR + kStdNT[STD]) continue;
+                const LevelA& la = P.A[i];
+                const uint32_t q = STD ? kStdQ[STD][i] : la.q;
+                uint32_t ph = 0;
+                if (q > 1) ph = phase_fast(ln.r_lo, ln.r_hi, q, la.magic, la.c32, la.winv, jm[i], jbase);
+                SA[i * 32 + lane] = (uint8_t)ph;
+            }
+#pragma unroll 4
+            for (uint32_t p = 0; p < P.nBpad; p++) {
+                uint32_t ph = 0;
+                if (p < P.nB) {
+                    const PrimeC pc = P.primesB[p];
+                    ph = phase_fast(ln.r_lo, ln.r_hi, pc.q, pc.magic, pc.c32, pc.winv, jm[kNumA + p], jbase);
+                }
+                S[p * 32 + lane] = (uint16_t)ph;
+            }
         }
         LevelB B;
         B.Q = Qw;
@@ -321,7 +393,7 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                 const uint32_t q = STD ? kStdQ[STD][i] : P.A[i].q;
                 uint32_t ph = (uint32_t)SA[i * 32 + lane] + off;
                 if (STD) ph = q > 1 ? ph % q : 0;
-                else ph = mod_magic(ph, q, P.A[i].magic);
+                else ph = q > 1 ? mod_magic(ph, q, P.A[i].magic) : 0u;
                 if (i >= kNumAR) { Tph[i - kNumAR] = ph; continue; }
                 const uint32_t* pa = PA + i * 8 + (ph >> 5);
                 const uint32_t b = ph & 31;

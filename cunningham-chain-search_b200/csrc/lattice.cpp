@@ -219,7 +219,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
 
     // ---- level classification ----------------------------------------------
     memset(hp.A, 0, sizeof(hp.A));
-    for (int i = 0; i < kNumA; i++) hp.A[i].q = 1;      // dummy: no kills
+    for (int i = 0; i < kNumA; i++) { hp.A[i].q = 1; hp.A[i].magic = 0xFFFFFFFFu; }   // dummy: no kills
     int nA1 = 0, nA2 = 0, nT = 0;
     hp.primesB.clear(); hp.primesC.clear(); hp.bitmapB.clear(); hp.listC.clear(); hp.packB.clear();
     hp.patT.clear();
@@ -305,9 +305,12 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             pb.q_off = q | (pc.off << 16);
             hp.packB.push_back(pb);
         } else {
+            // sorted list padded to a multiple of 4 entries (0xFFFFFFFF never
+            // matches a phase), 16-byte aligned for vector loads
             pc.off = (uint32_t)hp.listC.size();
             pc.cnt = (uint32_t)g.size();
             hp.listC.insert(hp.listC.end(), g.begin(), g.end());
+            while (hp.listC.size() % 4) hp.listC.push_back(0xFFFFFFFFu);
             hp.primesC.push_back(pc);
         }
     }

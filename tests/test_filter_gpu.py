@@ -105,6 +105,20 @@ def test_each_filter_level_alone(ccs, ob, primes):
     eng.close()
 
 
+def test_profile_without_level_a_long_range(ccs, ob):
+    """No bit-sliced primes at all (every level-A slot is a dummy) and a
+    range long enough for many queue segments per work unit: the generic
+    kernel path must still equal the oracle."""
+    stages = [(ccs.primes_in(131, 1024), 0)]
+    eng = ccs.Engine(target=16, depth=16, stages=stages)
+    eng.set_tuning(ext_min_words=0xFFFFFFFF, unit_words=4)
+    lat = ob.Lattice(lattice_len=16, depth=16, stages=stages)
+    ts = (1 << 52) + 98765
+    want = as_set(lat.filter_range(ts, 420))
+    assert as_set(eng.filter_range(ts, 420, cap=1 << 22)) == want and len(want) > 1000
+    eng.close()
+
+
 def test_cpu_method_lattice_matches_oracle(ccs, ob):
     cfg = ccs.config_cpu_method()
     eng = ccs.Engine(**cfg)
