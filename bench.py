@@ -272,6 +272,10 @@ def section_batched(ccs, engines, n_ranges=4096):
     """Uneven ranges: one batched graph replay versus per-range plain calls."""
     ranges = ccs.mixed_ranges(engines, n_ranges, SEED + 11)
     batch = ccs.Batch(engines, n_ranges, surv_cap=1 << 22, chain_cap=1 << 20)
+    # batch autotuner on a separately drawn sample of the same distribution
+    t_tune = time.time()
+    chosen, pts = batch.autotune(ccs.mixed_ranges(engines, min(512, n_ranges), SEED + 13))
+    tune = {"chosen": chosen, "points": len(pts), "seconds": time.time() - t_tune}
     batch.run(ranges[:32], want_records=False)
     t0 = time.time()
     res, surv, ch = batch.run(ranges)
@@ -297,10 +301,11 @@ def section_batched(ccs, engines, n_ranges=4096):
             "batched_device_ms": dev_ms, "plain_candidates_per_s": cand / tp,
             "speedup": tp / tb, "survivors": nsurv, "plain_survivors": psurv,
             "primes": nprimes, "plain_primes": pprimes,
-            "batched_proofs_per_s": nprimes / tb, "plain_proofs_per_s": pprimes / tp}
+            "batched_proofs_per_s": nprimes / tb, "plain_proofs_per_s": pprimes / tp,
+            "batch_autotune": tune}, chosen
 
 
-def section_served(ccs, engines, n_req=2048, lam=2000.0):
+def section_served(ccs, engines, n_req=2048, lam=2000.0, batch_tuning=None):
     """Poisson arrivals of uneven range requests: continuous-batching server
     versus a plain first-come-first-served loop; p50/p99 request latency."""
     import random
@@ -316,6 +321,8 @@ def section_served(ccs, engines, n_req=2048, lam=2000.0):
 
     # served
     srv = ccs.Server(engines, max_active=256, chunk_tiles=1 << 19, mem_cap_bytes=120 << 30)
+    if batch_tuning:
+        srv.set_batch_tuning(**batch_tuning)
     ids = [None] * n_req
     base = time.monotonic() + 0.05
 
@@ -499,12 +506,13 @@ def run_ours(args):
                 extra["autotune_depth_profiles"] = autotune_engines(ccs, depth_engines, SEED + 5)
             except Exception as ex:
                 extra["autotune_depth_profiles"] = {"error": repr(ex)}
+        btune = None
         try:
-            extra["batched"] = section_batched(ccs, depth_engines, args.batch_ranges)
+            extra["batched"], btune = section_batched(ccs, depth_engines, args.batch_ranges)
         except Exception as ex:
             extra["batched"] = {"error": repr(ex)}
         try:
-            extra["served"] = section_served(ccs, depth_engines, args.served_requests)
+            extra["served"] = section_served(ccs, depth_engines, args.served_requests, batch_tuning=btune)
         except Exception as ex:
             extra["served"] = {"error": repr(ex)}
         for e in depth_engines:

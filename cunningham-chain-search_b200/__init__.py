@@ -139,6 +139,11 @@ class _TunePoint(C.Structure):
 TUNE_LATTICE, TUNE_STAGES, TUNE_UNITS, TUNE_SHAPE, TUNE_ALL = 1, 2, 4, 8, 15
 
 
+class _BatchTuning(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("unit_words", C.c_uint32),
+                ("_pad", C.c_uint32)]
+
+
 # exported symbols of include/ccs.h, with their ctypes signatures
 _vp = C.c_void_p
 _u64 = C.c_uint64
@@ -179,6 +184,11 @@ _SIGS = {
     "ccs_set_tuning": (C.c_int, [_vp, C.POINTER(_Tuning)]),
     "ccs_autotune": (C.c_int, [_vp, _u64, _u64, _u64, C.c_uint32, C.POINTER(_TunePoint), C.c_uint32,
                                C.POINTER(C.c_uint32), C.POINTER(_Tuning)]),
+    "ccs_batch_get_tuning": (C.c_int, [_vp, C.POINTER(_BatchTuning)]),
+    "ccs_server_set_batch_tuning": (C.c_int, [_vp, C.POINTER(_BatchTuning)]),
+    "ccs_batch_set_tuning": (C.c_int, [_vp, C.POINTER(_BatchTuning)]),
+    "ccs_batch_autotune": (C.c_int, [_vp, _vp, C.c_uint32, C.POINTER(_TunePoint), C.c_uint32,
+                                     C.POINTER(C.c_uint32), C.POINTER(_BatchTuning)]),
 }
 
 _LIB = None
@@ -553,6 +563,40 @@ class Batch:
         _check(load_library().ccs_batch_last_ms(self.h, C.byref(ms)))
         return ms.value
 
+    @staticmethod
+    def _ranges(ranges):
+        rr = (_Range * max(len(ranges), 1))()
+        for i, (ts, nt, prof, bits) in enumerate(ranges):
+            lo, hi = _split128(ts)
+            rr[i].tile_start_lo, rr[i].tile_start_hi = lo, hi
+            rr[i].n_tiles = nt
+            rr[i].profile = prof
+            rr[i].bits = bits
+        return rr
+
+    def tuning(self):
+        t = _BatchTuning()
+        _check(load_library().ccs_batch_get_tuning(self.h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in _BatchTuning._fields_ if not f.startswith("_")}
+
+    def set_tuning(self, **kw):
+        t = _BatchTuning()
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _check(load_library().ccs_batch_set_tuning(self.h, C.byref(t)), "ccs_batch_set_tuning")
+
+    def autotune(self, ranges, cap=64):
+        """Batch autotuner over a sample of ranges: block shape and unit
+        length; returns (chosen dict, [(tuning dict, ms), ...])."""
+        pts = (_TunePoint * cap)()
+        n = C.c_uint32(0)
+        t = _BatchTuning()
+        _check(load_library().ccs_batch_autotune(self.h, self._ranges(ranges), len(ranges), pts, cap,
+                                                 C.byref(n), C.byref(t)), "ccs_batch_autotune")
+        pick = ("block_threads", "blocks_per_sm", "unit_words")
+        return ({f: getattr(t, f) for f in pick},
+                [({f: getattr(p.tuning, f) for f in pick}, p.ms) for p in pts[:min(n.value, cap)]])
+
 
 # ---------------------------------------------------------------------------
 # range planning (v13:411-518, 3480-3573): bit range, binary prefix, lanes
@@ -677,6 +721,12 @@ class Server:
 
     def cancel(self, rid):
         _check(load_library().ccs_cancel(self.h, rid), "ccs_cancel")
+
+    def set_batch_tuning(self, block_threads=0, blocks_per_sm=0, unit_words=0):
+        """Tuning of the server's batch executor (from Batch.autotune),
+        applied before its next tick."""
+        t = _BatchTuning(block_threads, blocks_per_sm, unit_words, 0)
+        _check(load_library().ccs_server_set_batch_tuning(self.h, C.byref(t)), "ccs_server_set_batch_tuning")
 
     def stats(self):
         out = (_u64 * 6)()

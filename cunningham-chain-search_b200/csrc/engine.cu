@@ -159,6 +159,11 @@ struct ccs_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0;
     uint32_t grid = 0;
+    uint32_t nc = 0;                     // counters in d_counts
+    // batch tuning: sweep block shape (captured in the graph) and the work
+    // unit length of every range (0: each engine's own)
+    uint32_t block_threads = 0, blocks_per_sm = 0, unit_words = 0;
+    uint32_t req_blocks_per_sm = 0;      // requested (0: as many as fit)
 };
 
 // ---------------------------------------------------------------------------
@@ -1096,6 +1101,8 @@ ccs_status ccs_batch_destroy(ccs_batch* b) {
     return CCS_OK;
 }
 
+static ccs_status batch_capture(ccs_batch* b);
+
 ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, uint32_t max_ranges,
                             uint64_t surv_cap, uint64_t chain_cap, ccs_batch** out) {
     if (!out || !profiles || !n_profiles || !max_ranges) return fail(CCS_ERR_INVALID, "bad argument");
@@ -1151,12 +1158,30 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     CU(cudaEventCreate(&b->ev0));
     CU(cudaEventCreate(&b->ev1));
-    const uint32_t bt = b->prof[0]->tune.block_threads;
-    int bps = sweep_blocks_per_sm(b->b_stride, bt);
-    b->grid = (uint32_t)b->prof[0]->sms * (uint32_t)std::max(bps, 1);
+    b->nc = (uint32_t)nc;
+    b->block_threads = kSweepThreads;
+    {
+        ccs_status s = batch_capture(b);
+        if (s != CCS_OK) { ccs_batch_destroy(b); return s; }
+    }
+    *out = b;
+    return CCS_OK;
+}
 
-    // record the whole batch once: H2D descriptors, setup, sweep, level C,
-    // prove, D2H counters.  Replays read the per-submission header on device.
+// Records the whole batch once: H2D descriptors, setup, sweep (with the
+// batch's block shape), prove, D2H counters.  Replays read the
+// per-submission header on the device.
+static ccs_status batch_capture(ccs_batch* b) {
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    const uint32_t bt = b->block_threads;
+    const int mx = sweep_blocks_per_sm(b->b_stride, bt);
+    if (mx <= 0) return fail(CCS_ERR_INVALID, "sweep does not fit the SM at this block size");
+    b->blocks_per_sm = (b->req_blocks_per_sm == 0 || b->req_blocks_per_sm > (uint32_t)mx)
+                           ? (uint32_t)mx : b->req_blocks_per_sm;
+    b->grid = (uint32_t)b->prof[0]->sms * b->blocks_per_sm;
+    const uint32_t max_ranges = b->max_ranges;
+    const size_t nc = b->nc;
     cudaStream_t st = b->stream;
     CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(b->d_ranges.p, b->h_ranges, sizeof(RangeDev) * max_ranges, cudaMemcpyHostToDevice, st);
@@ -1181,10 +1206,35 @@ ccs_status ccs_batch_create(ccs_engine* const* profiles, uint32_t n_profiles, ui
     launch_prove(pa, (uint32_t)b->prof[0]->sms * 16, st);
     cudaMemcpyAsync(b->h_counts, b->d_counts.p, 4 * nc, cudaMemcpyDeviceToHost, st);
     cudaError_t ce = cudaStreamEndCapture(st, &b->graph);
-    if (ce != cudaSuccess) { ccs_batch_destroy(b); return fail(CCS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)); }
+    if (ce != cudaSuccess) return fail(CCS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
     ce = cudaGraphInstantiate(&b->gexec, b->graph, 0);
-    if (ce != cudaSuccess) { ccs_batch_destroy(b); return fail(CCS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce)); }
-    *out = b;
+    if (ce != cudaSuccess) return fail(CCS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    return CCS_OK;
+}
+
+ccs_status ccs_batch_get_tuning(const ccs_batch* b, ccs_batch_tuning* t) {
+    if (!b || !t) return fail(CCS_ERR_INVALID, "null argument");
+    t->block_threads = b->block_threads;
+    t->blocks_per_sm = b->blocks_per_sm;
+    t->unit_words = b->unit_words;
+    t->_pad = 0;
+    return CCS_OK;
+}
+
+ccs_status ccs_batch_set_tuning(ccs_batch* b, const ccs_batch_tuning* t) {
+    if (!b || !t) return fail(CCS_ERR_INVALID, "null argument");
+    if (t->block_threads && t->block_threads != 128 && t->block_threads != 256)
+        return fail(CCS_ERR_INVALID, "block_threads must be 128 or 256");
+    if (t->unit_words > (1u << 20)) return fail(CCS_ERR_INVALID, "unit_words too large");
+    CU(cudaSetDevice(b->device));
+    b->unit_words = t->unit_words;
+    const uint32_t bt = t->block_threads ? t->block_threads : b->block_threads;
+    if (bt != b->block_threads || t->blocks_per_sm != b->req_blocks_per_sm) {
+        CU(cudaStreamSynchronize(b->stream));
+        b->block_threads = bt;
+        b->req_blocks_per_sm = t->blocks_per_sm;
+        return batch_capture(b);
+    }
     return CCS_OK;
 }
 
@@ -1198,14 +1248,27 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
     uint64_t total = 0;
     uint32_t* cnt = b->d_counts.p;
     for (uint32_t i = 0; i < n_ranges; i++) {
+        if (ranges[i].profile >= b->prof.size()) return fail(CCS_ERR_INVALID, "bad profile index");
+        if (ranges[i].n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
+    }
+    // work units are laid out profile by profile, longest range first, so the
+    // persistent sweep works through one profile's tables at a time and ends
+    // on short units; records still carry the caller's range index
+    std::vector<uint32_t> order(n_ranges);
+    for (uint32_t i = 0; i < n_ranges; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        if (ranges[x].profile != ranges[y].profile) return ranges[x].profile < ranges[y].profile;
+        return ranges[x].n_tiles > ranges[y].n_tiles;
+    });
+    for (uint32_t k = 0; k < n_ranges; k++) {
+        const uint32_t i = order[k];
         const ccs_range& rg = ranges[i];
-        if (rg.profile >= b->prof.size()) return fail(CCS_ERR_INVALID, "bad profile index");
-        if (rg.n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
         ccs_engine* E = b->prof[rg.profile];
         unsigned __int128 ts = mk128(rg.tile_start_lo, rg.tile_start_hi);
-        RangeDev& R = b->h_ranges[i];
+        RangeDev& R = b->h_ranges[k];
         memset(&R, 0, sizeof(R));
         const FilterSet& f = place_range(E, ts, rg.n_tiles, R, false);   // ranges share the GPU
+        if (b->unit_words) R.unit_words = std::max<uint32_t>(1, std::min(b->unit_words, R.n_words));
         R.prime_base = b->prime_base[2 * rg.profile + (&f == &E->fs[1] ? 1 : 0)];
         R.surv_cap = (uint32_t)b->surv_cap;
         R.surv_count = cnt;
@@ -1221,7 +1284,7 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
         P.target = E->hp.target;
         P.chain_count = cnt + 4 + 3 * i + 1;
         P.prime_count = cnt + 4 + 3 * i + 2;
-        b->h_prefix[i] = total;
+        b->h_prefix[k] = total;
         total += R.n_words ? units_of(f, R.n_words, R.unit_words) : 0;
     }
     b->h_prefix[n_ranges] = total;
@@ -1266,6 +1329,60 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
     if (chains_host && ccopy) CU(cudaMemcpy(chains_host, b->d_chains.p, 48 * ccopy, cudaMemcpyDeviceToHost));
     if (ns > b->surv_cap || nch > b->chain_cap) st = fail(CCS_OVERFLOW, "batch capacity exceeded");
     return st;
+}
+
+ccs_status ccs_batch_autotune(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
+                              ccs_tune_point* points, uint32_t cap, uint32_t* n_points,
+                              ccs_batch_tuning* chosen) {
+    if (!b || !ranges || !n_ranges) return fail(CCS_ERR_INVALID, "bad argument");
+    if (n_ranges > b->max_ranges) return fail(CCS_ERR_INVALID, "too many ranges for this batch");
+    if (cap && !points) return fail(CCS_ERR_INVALID, "points is null");
+    std::vector<ccs_range_result> res(n_ranges);
+    uint32_t n = 0;
+    float best_ms = -1.0f;
+    ccs_batch_tuning best{};
+    ccs_batch_get_tuning(b, &best);
+    auto measure = [&](const ccs_batch_tuning& t) -> ccs_status {
+        ccs_status s = ccs_batch_set_tuning(b, &t);
+        if (s != CCS_OK) return s;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            s = ccs_batch_run(b, ranges, n_ranges, res.data(), nullptr, nullptr, nullptr);
+            if (s != CCS_OK && s != CCS_OVERFLOW) return s;
+            ms = std::min(ms, b->last_ms);
+        }
+        if (n < cap) {
+            memset(&points[n], 0, sizeof(points[n]));
+            points[n].tuning.block_threads = b->block_threads;
+            points[n].tuning.blocks_per_sm = b->blocks_per_sm;
+            points[n].tuning.unit_words = b->unit_words;
+            points[n].ms = ms;
+        }
+        n++;
+        if (best_ms < 0 || ms < best_ms) {
+            best_ms = ms;
+            best = t;
+            best.block_threads = b->block_threads;
+        }
+        return CCS_OK;
+    };
+    // unit length at the default shape, then block shapes at that length
+    const uint32_t units[5] = {0, 1024, 2048, 4096, 8192};
+    for (uint32_t uw : units) {
+        ccs_status s = measure(ccs_batch_tuning{256u, 0u, uw, 0u});
+        if (s != CCS_OK) return s;
+    }
+    const uint32_t uw_best = best.unit_words;
+    const uint32_t shapes[5][2] = {{256, 1}, {256, 2}, {128, 2}, {128, 3}, {128, 4}};
+    for (const auto& sh : shapes) {
+        ccs_status s = measure(ccs_batch_tuning{sh[0], sh[1], uw_best, 0u});
+        if (s != CCS_OK) return s;
+    }
+    ccs_status s = ccs_batch_set_tuning(b, &best);
+    if (s != CCS_OK) return s;
+    if (n_points) *n_points = n;
+    if (chosen) ccs_batch_get_tuning(b, chosen);
+    return CCS_OK;
 }
 
 ccs_status ccs_batch_last_ms(const ccs_batch* b, float* ms) {

@@ -63,6 +63,8 @@ struct ccs_server {
     std::vector<ccs_chain> tick_chains;
     uint64_t surv_cap = 0, chain_cap = 0;
     std::string err;
+    bool tune_pending = false;          // batch tuning to apply before the next tick
+    ccs_batch_tuning tune{};
 };
 
 namespace {
@@ -135,9 +137,14 @@ void worker_loop(ccs_server* s) {
             s->tick_off.push_back(r->done_tiles);
         }
         const uint32_t n = (uint32_t)s->tick_ranges.size();
+        const bool retune = s->tune_pending;
+        const ccs_batch_tuning tune = s->tune;
+        s->tune_pending = false;
         lk.unlock();
-        ccs_status st = ccs_batch_run(s->batch, s->tick_ranges.data(), n, s->tick_res.data(),
-                                      s->tick_surv.data(), s->tick_chains.data(), nullptr);
+        ccs_status st = retune ? ccs_batch_set_tuning(s->batch, &tune) : CCS_OK;
+        if (st == CCS_OK)
+            st = ccs_batch_run(s->batch, s->tick_ranges.data(), n, s->tick_res.data(),
+                               s->tick_surv.data(), s->tick_chains.data(), nullptr);
         lk.lock();
         s->st_ticks++;
         if (st != CCS_OK && st != CCS_OVERFLOW) {
@@ -305,6 +312,15 @@ ccs_status ccs_cancel(ccs_server* s, uint64_t id) {
     if (it == s->all.end()) return CCS_ERR_NOT_FOUND;
     if (it->second->state == CCS_PENDING) it->second->cancel = true;
     s->cv_work.notify_one();
+    return CCS_OK;
+}
+
+ccs_status ccs_server_set_batch_tuning(ccs_server* s, const ccs_batch_tuning* t) {
+    if (!s || !t) return CCS_ERR_INVALID;
+    if (t->block_threads && t->block_threads != 128 && t->block_threads != 256) return CCS_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->tune = *t;
+    s->tune_pending = true;
     return CCS_OK;
 }
 

@@ -244,6 +244,19 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
 /* device-side timing of the last ccs_batch_run: filter+prove milliseconds */
 ccs_status ccs_batch_last_ms(const ccs_batch* b, float* ms);
 
+/* Batch tuning: the sweep block shape of the recorded graph and the work
+ * unit length applied to every range (0: each engine's own unit_words). */
+typedef struct {
+    uint32_t block_threads;   /* 128 or 256 */
+    uint32_t blocks_per_sm;   /* 0: as many as fit */
+    uint32_t unit_words;
+    uint32_t _pad;
+} ccs_batch_tuning;
+
+ccs_status ccs_batch_get_tuning(const ccs_batch* b, ccs_batch_tuning* out);
+/* a new block shape re-records the batch graph */
+ccs_status ccs_batch_set_tuning(ccs_batch* b, const ccs_batch_tuning* t);
+
 /* ---- served path ------------------------------------------------------------ */
 
 /* A request server with continuous batching: requests (lattice ranges) are
@@ -281,6 +294,9 @@ ccs_status ccs_poll(ccs_server* s, uint64_t id, ccs_request_result* res, ccs_sur
 /* block until the request is done (or timeout_ms passes: CCS_ERR_TIMEOUT) */
 ccs_status ccs_wait(ccs_server* s, uint64_t id, uint32_t timeout_ms);
 ccs_status ccs_cancel(ccs_server* s, uint64_t id);
+/* batch tuning of the server's executor (ccs_batch_set_tuning), applied
+ * before its next tick */
+ccs_status ccs_server_set_batch_tuning(ccs_server* s, const ccs_batch_tuning* t);
 /* counters: [0] submitted [1] admitted [2] completed [3] cancelled [4] ticks [5] pending now */
 ccs_status ccs_server_stats(ccs_server* s, uint64_t* out6);
 
@@ -337,6 +353,15 @@ typedef struct {
 ccs_status ccs_autotune(ccs_engine* eng, uint64_t ts_lo, uint64_t ts_hi, uint64_t n_tiles,
                         uint32_t what, ccs_tune_point* points, uint32_t cap, uint32_t* n_points,
                         ccs_tuning* chosen);
+
+/* Batch autotuner: runs the batch on the given ranges (results discarded)
+ * for each block shape (256 and 128 threads, as many blocks as fit) and unit
+ * length (each engine's own, 1024, 2048, 4096, 8192 words), keeps the one
+ * with the shortest device time and leaves it set on the batch.  Points
+ * carry block_threads, blocks_per_sm and unit_words in their tuning. */
+ccs_status ccs_batch_autotune(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
+                              ccs_tune_point* points, uint32_t cap, uint32_t* n_points,
+                              ccs_batch_tuning* chosen);
 
 /* ---- diagnostics ----------------------------------------------------------- */
 

@@ -36,3 +36,33 @@ def test_batch_equals_plain(ccs):
     batch.close()
     for e in engines:
         e.close()
+
+
+def test_batch_tuning_keeps_results(ccs):
+    """Every batch block shape and unit length gives the same per-range
+    survivor sets; the batch autotuner leaves one of them set."""
+    engines = [ccs.Engine(target=16, depth=16, bits=64), ccs.Engine(target=18, bits=64)]
+    batch = ccs.Batch(engines, max_ranges=32, surv_cap=1 << 20, chain_cap=1 << 18)
+    r = random.Random(17)
+    ranges = [((1 << 63) // (20677 * 1616615) + r.randint(0, 10**7), r.choice([3, 70, 900, 20000]), i % 2, 64)
+              for i in range(16)]
+
+    def sets():
+        res, surv, _ = batch.run(ranges)
+        by = {}
+        for rec in surv:
+            by.setdefault(int(rec["_pad"]), []).append(
+                (int(rec["base_idx"]), int(rec["k_offset"]), int(rec["tile_idx"])))
+        return [sorted(by.get(i, [])) for i in range(len(ranges))], [x["n_primes"] for x in res]
+
+    want = sets()
+    for bt, uw in [(128, 0), (256, 2), (128, 4096), (256, 1024)]:
+        batch.set_tuning(block_threads=bt, unit_words=uw)
+        assert batch.tuning()["block_threads"] == bt
+        assert sets() == want
+    chosen, points = batch.autotune(ranges)
+    assert len(points) == 10 and chosen == batch.tuning()
+    assert sets() == want
+    batch.close()
+    for e in engines:
+        e.close()

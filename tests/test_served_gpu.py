@@ -29,6 +29,8 @@ def test_served_results_equal_alone_and_in_the_mix(ccs):
         ids.append(srv.submit(ts, nt, p, bits))
         if i % 7 == 3:
             time.sleep(0.002)          # arrivals while earlier requests run
+        if i == 20:                    # executor re-tuned between ticks
+            srv.set_batch_tuning(block_threads=128, unit_words=2048)
     mixed = {}
     for rid in ids:
         srv.wait(rid)
