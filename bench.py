@@ -469,6 +469,19 @@ def run_ours(args):
     filt_ms = ev0.elapsed_time(ev1)
     int_peak = ccs.measure_int32_peak(local)
     E = info["expected_tests"]
+    # DRAM traffic per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum
+    # of a 2^22-tile launch of this profile on the extended lattice (158.1 MB
+    # for 287,469 work units = one per 32-line group), scaled by the work units
+    # of this launch (the line table is read once per unit)
+    tune_now = eng.tuning()
+    span = (TILES + 5) // 6 + 1
+    n_words = ((span + 36) // 37 + 63) // 64
+    traffic, traffic_note = None, None
+    if n_words >= tune_now["ext_min_words"]:
+        chunks = -(-n_words // max(1, min(tune_now["unit_words"], n_words)))
+        traffic = 158.1e6 * chunks
+        traffic_note = (f"ncu DRAM bytes of a 2^22-tile launch (158.1 MB, one unit per line group) "
+                        f"x {chunks} units per group at {TILES} tiles")
     achieved = cand_step * 4.0 * E / (filt_ms * 1e-3) / 1e12
 
     # end to end through the host-buffer C-ABI call (copies inside)
@@ -530,7 +543,8 @@ def run_ours(args):
             "survivors": n_surv, "chains": n_chain, "primes": n_prime,
             "survivor_rate": n_surv / (args.steps * cand_step),
             "roofline": {"bound": "int32", "achieved": achieved, "peak": int_peak, "unit": "TOPS",
-                         "frac": achieved / int_peak, "traffic": None,
+                         "frac": achieved / int_peak, "traffic": traffic,
+                         "traffic_source": traffic_note,
                          "kernel": "sweep_kernel (+ range setup, deferred stage)",
                          "work_per_candidate": f"4 x E[tests] = {4 * E:.3f} int32 ops",
                          "filter_ms_per_launch_group": filt_ms,
