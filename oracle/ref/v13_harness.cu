@@ -162,3 +162,45 @@ int ref13_prove_cpu(const unsigned* surv, int count, unsigned long long ts_lo,
 }
 
 }  /* extern "C" */
+
+/* ---- campaign shell pins: generator and checkpoint file (v13:540-722) ---- */
+extern "C" {
+
+/* n outputs of the reference generator rng_next after rng_seed(seed) */
+void ref13_rng(unsigned long long seed, int n, unsigned long long* out) {
+    rng_seed(seed);
+    for (int i = 0; i < n; i++) out[i] = rng_next();
+}
+
+static void ref13_set_prefix(const char* prefix, int lanes, int lane_id) {
+    g_use_prefix = (prefix && prefix[0] && strcmp(prefix, "none") != 0);
+    snprintf(g_prefix_str, sizeof(g_prefix_str), "%s", g_use_prefix ? prefix : "");
+    g_prefix_lanes = lanes;
+    g_prefix_lane_id = lane_id;
+}
+
+/* reference checkpoint_save with the given campaign identity and cursor */
+int ref13_checkpoint_save(const char* path, int bits, int target, int depth, const char* prefix,
+                          int lanes, int lane_id, unsigned long long tile_hi, unsigned long long tile_lo,
+                          unsigned long long tiles, unsigned long long primes, unsigned long long chains,
+                          int best) {
+    ref13_set_prefix(prefix, lanes, lane_id);
+    u128 t = ((u128)tile_hi << 64) | tile_lo;
+    return checkpoint_save(path, bits, target, depth, t, tiles, primes, chains, best);
+}
+
+/* reference checkpoint_load; out = {tile_hi, tile_lo, tiles, primes, chains, best} */
+int ref13_checkpoint_load(const char* path, int bits, int target, int depth, const char* prefix,
+                          int lanes, int lane_id, unsigned long long* out) {
+    ref13_set_prefix(prefix, lanes, lane_id);
+    u128 t = 0;
+    u64 tiles = 0, primes = 0, chains = 0;
+    int best = 0;
+    int r = checkpoint_load(path, bits, target, depth, &t, &tiles, &primes, &chains, &best);
+    out[0] = (unsigned long long)(t >> 64);
+    out[1] = (unsigned long long)t;
+    out[2] = tiles; out[3] = primes; out[4] = chains; out[5] = (unsigned long long)best;
+    return r;
+}
+
+}  // extern "C"
