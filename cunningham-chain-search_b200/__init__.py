@@ -256,8 +256,12 @@ def format_chain_line(chain_len, root, target, is_root=True):
     return f"{tag}CC{chain_len} 0x{root:X} {root.bit_length()}"
 
 
+FLAG_REVERSE_PROVE = 1     # CCS_FLAG_REVERSE_PROVE: v15 --prove-order reverse (roots mode)
+
+
 def _make_params(target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, stages=None,
-                 max_bases=0, witnesses=V13_WITNESSES, primality=PRIME_BPSW, prove_mode=PROVE_FULL):
+                 max_bases=0, witnesses=V13_WITNESSES, primality=PRIME_BPSW, prove_mode=PROVE_FULL,
+                 reverse_prove=False):
     """ccs_params plus the buffers it points to (keep both alive)."""
     if stages is None:
         stages = reference_stages()
@@ -289,6 +293,7 @@ def _make_params(target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, s
     p.n_witnesses = len(witnesses)
     p.primality = primality
     p.prove_mode = prove_mode
+    p.flags = FLAG_REVERSE_PROVE if reverse_prove else 0
     return p, keep
 
 
@@ -324,12 +329,12 @@ class Engine:
 
     def __init__(self, target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, stages=None,
                  max_bases=0, witnesses=V13_WITNESSES, primality=PRIME_BPSW,
-                 prove_mode=PROVE_FULL, device=0):
+                 prove_mode=PROVE_FULL, device=0, reverse_prove=False):
         lib = load_library()
         if stages is None:
             stages = reference_stages()
         p, self._keep = _make_params(target, depth, bits, crt, wheel, stages, max_bases, witnesses,
-                                     primality, prove_mode)
+                                     primality, prove_mode, reverse_prove)
         h = _vp()
         _check(lib.ccs_create(C.byref(p), device, C.byref(h)), "ccs_create")
         self.h = h

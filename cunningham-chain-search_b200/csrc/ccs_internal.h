@@ -129,6 +129,7 @@ struct HostProfile {
     uint32_t max_bases = 0;
     std::vector<uint64_t> witnesses;
     uint32_t primality = 1, prove_mode = 1;
+    uint32_t reverse_prove = 0;      // CCS_FLAG_REVERSE_PROVE
     uint32_t q0 = 1;                 // filter prime absorbed into the modulus (1: none)
     uint32_t t_count = 0;            // table-window primes wanted (0: by the admission rule)
 

@@ -269,6 +269,7 @@ ccs_status upload_prove(ccs_engine* E, cudaStream_t st) {
     pv.M = (uint32_t)hp.M;
     pv.primality = hp.primality;
     pv.prove_mode = hp.prove_mode;
+    pv.reverse = hp.reverse_prove;
     pv.n_wit = (uint32_t)std::min<size_t>(hp.witnesses.size(), 32);
     for (uint32_t i = 0; i < pv.n_wit; i++) pv.wit[i] = (uint32_t)hp.witnesses[i];
     CU(upload_prove_const(E->slot, pv, st));
@@ -306,6 +307,7 @@ ccs_status build_filters(ccs_engine* E, uint32_t split, uint32_t t_count) {
         d.crt = s.crt; d.wheel = s.wheel; d.stages = s.stages;
         d.max_bases = s.max_bases; d.witnesses = s.witnesses;
         d.primality = s.primality; d.prove_mode = s.prove_mode;
+        d.reverse_prove = s.reverse_prove;
         d.t_count = t_count;
     };
     params_of(nh[0]);
@@ -447,6 +449,10 @@ static ccs_status params_to_profile(const ccs_params* params, HostProfile& hp) {
     hp.primality = p.primality;
     hp.prove_mode = p.prove_mode;
     if (hp.primality > 1 || hp.prove_mode > 1) return fail(CCS_ERR_INVALID, "bad primality / prove_mode");
+    if (p.flags & ~CCS_FLAG_REVERSE_PROVE) return fail(CCS_ERR_INVALID, "unknown flags");
+    hp.reverse_prove = (p.flags & CCS_FLAG_REVERSE_PROVE) ? 1u : 0u;
+    if (hp.reverse_prove && hp.prove_mode != CCS_PROVE_ROOTS)
+        return fail(CCS_ERR_INVALID, "reverse prove order is a CCS_PROVE_ROOTS option (the reference K2's)");
     std::string err = build_profile(hp, 1024);
     if (!err.empty()) return fail(CCS_ERR_INVALID, err);
     if (hp.primesB.size() > (size_t)kMaxLevelB) return fail(CCS_ERR_INVALID, "too many level-B primes");

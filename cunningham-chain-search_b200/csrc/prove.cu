@@ -632,6 +632,34 @@ prove_kernel(ProveArgs a) {
         for (int t = 0; t < ntd && !comp; t++) comp = big_mod_small(nb, c_screen[t]) == 0;
         if (comp) continue;
         uint32_t mm = 0;
+        if (pc.reverse) {
+            // chain position target - 1 first: ((n + 1) << pos) - 1, the
+            // largest member and the likeliest composite (v15:1704-1708)
+            const int pos = R.target - 1 < 63 ? (int)R.target - 1 : 63;
+            if (pos > 0 && big_bits(nb) + pos < 32 * kMaxLimbs) {
+                Big top = nb;
+                uint32_t c = 1;
+#pragma unroll
+                for (int w = 0; w < kMaxLimbs; w++) {            // n + 1
+                    const uint64_t v = (uint64_t)top.w[w] + c;
+                    top.w[w] = (uint32_t)v;
+                    c = (uint32_t)(v >> 32);
+                }
+                for (int k = 0; k < pos; k++) {                  // << pos
+#pragma unroll
+                    for (int w = kMaxLimbs - 1; w > 0; w--) top.w[w] = (top.w[w] << 1) | (top.w[w - 1] >> 31);
+                    top.w[0] <<= 1;
+                }
+                uint32_t br = 1;
+#pragma unroll
+                for (int w = 0; w < kMaxLimbs; w++) {            // - 1
+                    const uint32_t nv = top.w[w] - br;
+                    br = (br && top.w[w] == 0) ? 1u : 0u;
+                    top.w[w] = nv;
+                }
+                if (!is_prime_dev(top, pc, mm)) continue;
+            }
+        }
         if (!is_prime_dev(nb, pc, mm)) continue;
         if (R.prime_count) atomicAdd(R.prime_count, 1u);
         Big root = nb;

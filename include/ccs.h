@@ -89,8 +89,14 @@ typedef struct {
     uint32_t n_witnesses;
     uint32_t primality;            /* CCS_PRIME_MR | CCS_PRIME_BPSW */
     uint32_t prove_mode;           /* CCS_PROVE_ROOTS | CCS_PROVE_FULL */
-    uint32_t flags;                /* reserved, 0 */
+    uint32_t flags;                /* CCS_FLAG_* */
 } ccs_params;
+
+/* ccs_params.flags */
+#define CCS_FLAG_REVERSE_PROVE 1u  /* with CCS_PROVE_ROOTS: test chain position target - 1 first
+                                      and drop the survivor when it is composite, then prove as
+                                      usual (v15 --prove-order reverse, v15:1686-1730); exact
+                                      arithmetic where the reference wraps at 2^128 */
 
 /* Filter output: the reference's Survivor record (v13:207-212), 16 bytes.
  * tile_idx is relative to the tile_start of the call. */

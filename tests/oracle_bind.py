@@ -230,6 +230,20 @@ def ref33():
     return lib
 
 
+def ref15():
+    """The reference v15 engine harness (its K1 and K2 in either prove
+    order), or None."""
+    path = os.path.join(REF_DIR, "libref15.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    lib.ref15_filter.restype = C.c_uint
+    lib.ref15_filter.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_uint, C.c_int, _u32p, C.c_uint]
+    lib.ref15_prove_gpu.restype = C.c_uint
+    lib.ref15_prove_gpu.argtypes = [C.c_ulonglong, C.c_ulonglong, _u32p, C.c_uint, C.POINTER(C.c_uint)]
+    return lib
+
+
 def ref13():
     """The reference v13 engine harness (GMP + its CUDA kernels), or None."""
     path = os.path.join(REF_DIR, "libref13.so")

@@ -175,3 +175,41 @@ def test_walk_rounds_across_chunks(ccs, ob, eng_bpsw):
     assert (L == L[0]).all()
     for i in r.sample(range(len(distinct)), 300):
         assert L[0, i] == ob.chain_from(distinct[i], ob.PRIME_BPSW), distinct[i]
+
+
+REF15 = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                     "libref15.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF15), reason="reference harness not built")
+@pytest.mark.parametrize("reverse", [False, True])
+def test_matches_reference_v15_filter_and_prove_order(ccs, ob, reverse):
+    """The reference v15 engine (the throughput kernel): its K1 survivor set
+    equals ours, and its K2 in forward and in reverse order (--prove-order,
+    chain position target - 1 tested first) gives our ChainResult set and
+    prime count (bits 61, target 18: no 2^128 wrap)."""
+    import ctypes as C
+    import torch
+    r15 = ob.ref15()
+    r15.ref15_setup(18, 18)
+    r15.ref15_upload(18, 61, 18, 0 if reverse else 1)
+    eng = ccs.Engine(bits=61, primality=ccs.PRIME_MR, prove_mode=ccs.PROVE_ROOTS, reverse_prove=reverse)
+    rr = random.Random(15 + reverse)
+    for n_tiles in (1, 700, 3000):
+        ts = (1 << 60) // (20677 * 1616615) + rr.randint(0, 10**6)
+        cap = 1 << 20
+        out = np.zeros(4 * cap, dtype=np.uint32)
+        cnt = r15.ref15_filter(ts & (2**64 - 1), ts >> 64, n_tiles, 12, out, cap)
+        ref_surv = sorted(map(tuple, out[: 4 * cnt].reshape(-1, 4)[:, :3].astype(np.int64).tolist()))
+        ours = eng.filter_range(ts, n_tiles, cap=cap)
+        assert sorted(map(tuple, (ours.cpu().numpy()[:, :3].astype(np.int64) & 0xFFFFFFFF).tolist())) == ref_surv
+        res = np.zeros(4 * 65536, dtype=np.uint32)
+        pr = C.c_uint(0)
+        nres = r15.ref15_prove_gpu(ts & (2**64 - 1), ts >> 64, res, 65536, C.byref(pr))
+        ref = sorted(map(tuple, res[: 4 * nres].reshape(-1, 4).astype(np.int64).tolist()))
+        surv = torch.tensor(out[: 4 * cnt].view(np.int32), device="cuda").reshape(-1, 4)
+        chains, primes = eng.prove(surv, ts)
+        got = sorted(map(tuple, (chains.cpu().numpy()[:, :4].astype(np.int64) & 0xFFFFFFFF).tolist()))
+        assert got == ref, (reverse, n_tiles)
+        assert primes == pr.value
+    eng.close()
