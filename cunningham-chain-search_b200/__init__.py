@@ -249,6 +249,9 @@ def chain_root_int(rec):
     return sum(int(x) << (32 * i) for i, x in enumerate(rec["root"]))
 
 
+KIND_FIRST, KIND_SECOND = 1, 2
+
+
 def format_chain_line(chain_len, root, target, is_root=True):
     """Reference output line "[TARGET ][NON-ROOT ]CC<len> 0x<HEX> <bits>"
     (v13:2030-2033)."""
@@ -261,7 +264,7 @@ FLAG_REVERSE_PROVE = 1     # CCS_FLAG_REVERSE_PROVE: v15 --prove-order reverse (
 
 def _make_params(target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, stages=None,
                  max_bases=0, witnesses=V13_WITNESSES, primality=PRIME_BPSW, prove_mode=PROVE_FULL,
-                 reverse_prove=False):
+                 reverse_prove=False, kind=1):
     """ccs_params plus the buffers it points to (keep both alive)."""
     if stages is None:
         stages = reference_stages()
@@ -278,7 +281,7 @@ def _make_params(target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, s
     wit = (C.c_uint64 * max(len(witnesses), 1))(*witnesses)
     keep += [crt_a, wheel_a, st, wit]
     p = _Params()
-    p.kind = 1
+    p.kind = kind
     p.target = target
     p.depth = depth if depth is not None else target
     p.bits = bits
@@ -329,12 +332,12 @@ class Engine:
 
     def __init__(self, target=18, depth=None, bits=89, crt=REF_CRT, wheel=REF_WHEEL, stages=None,
                  max_bases=0, witnesses=V13_WITNESSES, primality=PRIME_BPSW,
-                 prove_mode=PROVE_FULL, device=0, reverse_prove=False):
+                 prove_mode=PROVE_FULL, device=0, reverse_prove=False, kind=1):
         lib = load_library()
         if stages is None:
             stages = reference_stages()
         p, self._keep = _make_params(target, depth, bits, crt, wheel, stages, max_bases, witnesses,
-                                     primality, prove_mode, reverse_prove)
+                                     primality, prove_mode, reverse_prove, kind)
         h = _vp()
         _check(lib.ccs_create(C.byref(p), device, C.byref(h)), "ccs_create")
         self.h = h

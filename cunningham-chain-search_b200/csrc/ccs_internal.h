@@ -130,6 +130,7 @@ struct HostProfile {
     std::vector<uint64_t> witnesses;
     uint32_t primality = 1, prove_mode = 1;
     uint32_t reverse_prove = 0;      // CCS_FLAG_REVERSE_PROVE
+    uint32_t kind = 1;               // 1: p -> 2p + 1, 2: p -> 2p - 1
     uint32_t q0 = 1;                 // filter prime absorbed into the modulus (1: none)
     uint32_t t_count = 0;            // table-window primes wanted (0: by the admission rule)
 

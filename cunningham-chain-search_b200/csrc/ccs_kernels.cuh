@@ -68,6 +68,7 @@ struct ProveConst {
     uint32_t primality;      // CCS_PRIME_MR / CCS_PRIME_BPSW
     uint32_t prove_mode;     // CCS_PROVE_ROOTS / CCS_PROVE_FULL
     uint32_t reverse;        // 1: test chain position target - 1 first (v15 --prove-order reverse)
+    uint32_t kind;           // 1: p -> 2p + 1, 2: p -> 2p - 1 (v13b)
     uint32_t n_wit;
     uint32_t wit[32];
 };

@@ -270,6 +270,7 @@ ccs_status upload_prove(ccs_engine* E, cudaStream_t st) {
     pv.primality = hp.primality;
     pv.prove_mode = hp.prove_mode;
     pv.reverse = hp.reverse_prove;
+    pv.kind = hp.kind;
     pv.n_wit = (uint32_t)std::min<size_t>(hp.witnesses.size(), 32);
     for (uint32_t i = 0; i < pv.n_wit; i++) pv.wit[i] = (uint32_t)hp.witnesses[i];
     CU(upload_prove_const(E->slot, pv, st));
@@ -308,6 +309,7 @@ ccs_status build_filters(ccs_engine* E, uint32_t split, uint32_t t_count) {
         d.max_bases = s.max_bases; d.witnesses = s.witnesses;
         d.primality = s.primality; d.prove_mode = s.prove_mode;
         d.reverse_prove = s.reverse_prove;
+        d.kind = s.kind;
         d.t_count = t_count;
     };
     params_of(nh[0]);
@@ -408,8 +410,9 @@ static ccs_status params_to_profile(const ccs_params* params, HostProfile& hp) {
     ccs_params def;
     memset(&def, 0, sizeof(def));
     const ccs_params& p = params ? *params : def;
-    if (p.kind != 0 && p.kind != CCS_KIND_FIRST)
-        return fail(CCS_ERR_INVALID, "only first-kind chains are supported");
+    if (p.kind != 0 && p.kind != CCS_KIND_FIRST && p.kind != CCS_KIND_SECOND)
+        return fail(CCS_ERR_INVALID, "kind must be CCS_KIND_FIRST or CCS_KIND_SECOND");
+    hp.kind = p.kind == CCS_KIND_SECOND ? 2u : 1u;
     hp.target = p.target ? p.target : 18;
     hp.depth = p.depth ? p.depth : hp.target;
     hp.bits = p.bits ? p.bits : 89;

@@ -50,14 +50,15 @@ uint32_t mod_inverse_u32(uint32_t a, uint32_t q) {
 }
 
 // Residues n mod q with q | p_i = 2^i (n+1) - 1 for some i in [pos_lo, min(L, q)):
-// n = 2^{-i} - 1.  Walk x = 2^{-i} by repeated multiplication with 2^{-1}.
-static std::vector<uint32_t> forbidden_set(uint32_t q, uint32_t L, uint32_t pos_lo) {
+// n = 2^{-i} - 1; second kind, p_i = 2^i (n-1) + 1: n = 1 - 2^{-i} (v13b:779).
+// Walk x = 2^{-i} by repeated multiplication with 2^{-1}.
+static std::vector<uint32_t> forbidden_set(uint32_t q, uint32_t L, uint32_t pos_lo, uint32_t kind) {
     std::set<uint32_t> s;
     uint64_t inv2 = (q + 1) / 2;                 // 2^{-1} mod odd q
     uint64_t x = 1;                               // 2^{-0}
     uint32_t hi = std::min<uint32_t>(L, q);
     for (uint32_t i = 0; i < hi; i++) {
-        if (i >= pos_lo) s.insert((uint32_t)((x + q - 1) % q));
+        if (i >= pos_lo) s.insert((uint32_t)(kind == 2 ? (1 + q - x) % q : (x + q - 1) % q));
         x = x * inv2 % q;
     }
     return std::vector<uint32_t>(s.begin(), s.end());
@@ -96,7 +97,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
     std::vector<uint64_t> combos = {0};
     uint64_t mod = 1;
     for (uint32_t q : hp.crt) {
-        std::vector<uint32_t> f = forbidden_set(q, hp.target, 0);
+        std::vector<uint32_t> f = forbidden_set(q, hp.target, 0, hp.kind);
         std::vector<uint64_t> next;
         uint64_t inv = mod_inverse_u32((uint32_t)(mod % q), q);   // mod^{-1} mod q
         for (uint64_t a : combos) {
@@ -118,7 +119,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
     const uint32_t inv_m6 = (m6 == 1) ? 1 : 5;             // units mod 6 are self-inverse
     const uint32_t wp6 = hp.WP % 6;
     std::vector<std::vector<uint32_t>> wf;
-    for (uint32_t q : hp.wheel) wf.push_back(forbidden_set(q, hp.target, 0));
+    for (uint32_t q : hp.wheel) wf.push_back(forbidden_set(q, hp.target, 0, hp.kind));
     hp.bases.clear(); hp.tkm6.clear(); hp.wheel_total.clear(); hp.lines.clear();
     for (int c = 0; c < 6; c++) hp.lines_per_class[c] = 0;
     for (uint64_t base : combos) {
@@ -142,7 +143,9 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
         if (ks.empty()) continue;
         uint32_t bidx = (uint32_t)hp.bases.size();
         if (bidx >= 65536) return "too many bases (> 65535)";
-        uint32_t t6 = (uint32_t)(((5 + 6 - base % 6) % 6) * inv_m6 % 6);
+        // n == 5 (mod 6) for the first kind, n == 1 for the second (v13b:983)
+        const uint32_t nres = hp.kind == 2 ? 1u : 5u;
+        uint32_t t6 = (uint32_t)(((nres + 6 - base % 6) % 6) * inv_m6 % 6);
         hp.bases.push_back(base);
         hp.tkm6.push_back(t6);
         hp.wheel_total.push_back((uint32_t)ks.size());
@@ -172,7 +175,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             if (!is_prime_u32(q) || q < 5) return "filter primes must be primes >= 5";
             if (lattice_primes.count(q)) return "filter prime divides the lattice modulus";
             if (q >= (1u << 24)) return "filter primes must be < 2^24";
-            std::vector<uint32_t> f = forbidden_set(q, hp.depth, st.pos_lo);
+            std::vector<uint32_t> f = forbidden_set(q, hp.depth, st.pos_lo, hp.kind);
             // reference test order: stage by stage, prime by prime
             hp.expected_tests += surv;
             surv *= 1.0 - (double)f.size() / q;

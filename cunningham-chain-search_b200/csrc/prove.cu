@@ -86,11 +86,42 @@ __device__ __forceinline__ uint32_t big_shl1_inc(Big& a) {
     return carry;
 }
 
-// a = (a - 1) / 2 for odd a
-__device__ __forceinline__ void big_pred(Big& a) {
+// next chain member: 2a + 1 (first kind) or 2a - 1 (second kind, a >= 1)
+__device__ __forceinline__ void big_next(Big& a, uint32_t kind) {
+    if (kind != 2) { big_shl1_inc(a); return; }
+    uint32_t carry = 0;
 #pragma unroll
     for (int i = 0; i < kMaxLimbs; i++) {
-        uint32_t hi = (i + 1 < kMaxLimbs) ? a.w[i + 1] : 0;
+        const uint32_t nc = a.w[i] >> 31;
+        a.w[i] = (a.w[i] << 1) | carry;
+        carry = nc;
+    }
+    uint32_t br = 1;
+#pragma unroll
+    for (int i = 0; i < kMaxLimbs; i++) {
+        const uint32_t v = a.w[i];
+        a.w[i] = v - br;
+        br = (br && v == 0) ? 1u : 0u;
+    }
+}
+
+// predecessor of an odd chain member: (a - 1) / 2 (first kind) or
+// (a + 1) / 2 (second kind, v13b:1522)
+__device__ __forceinline__ void big_prev(Big& a, uint32_t kind) {
+    uint32_t top = 0;
+    if (kind == 2) {
+        uint32_t c = 1;
+#pragma unroll
+        for (int i = 0; i < kMaxLimbs; i++) {
+            const uint64_t v = (uint64_t)a.w[i] + c;
+            a.w[i] = (uint32_t)v;
+            c = (uint32_t)(v >> 32);
+        }
+        top = c;
+    }
+#pragma unroll
+    for (int i = 0; i < kMaxLimbs; i++) {
+        const uint32_t hi = (i + 1 < kMaxLimbs) ? a.w[i + 1] : top;
         a.w[i] = (a.w[i] >> 1) | (hi << 31);
     }
 }
@@ -564,13 +595,14 @@ __device__ bool is_prime_dev(const Big& nb, const ProveConst& pc, uint32_t& mm) 
     }
 }
 
-// forward walk p -> 2p + 1 while prime, counting p (v13:1519-1528, 1873-1881)
+// forward walk p -> 2p + 1 (second kind 2p - 1) while prime, counting p
+// (v13:1519-1528, 1873-1881; v13b:1527-1535, 1878-1886)
 __device__ int walk_forward(Big cur, const ProveConst& pc, uint32_t& mm) {
     int len = 1;
     while (len < kMaxChain) {
         if (big_bits(cur) >= 32 * kMaxLimbs) break;   // next member would exceed 192 bits
         Big nx = cur;
-        big_shl1_inc(nx);
+        big_next(nx, pc.kind);
         if (!is_prime_dev(nx, pc, mm)) break;
         len++;
         cur = nx;
@@ -633,30 +665,13 @@ prove_kernel(ProveArgs a) {
         if (comp) continue;
         uint32_t mm = 0;
         if (pc.reverse) {
-            // chain position target - 1 first: ((n + 1) << pos) - 1, the
-            // largest member and the likeliest composite (v15:1704-1708)
+            // chain position target - 1 first (the largest member, the
+            // likeliest composite; v15:1704-1708): pos applications of
+            // p -> 2p + 1 (second kind 2p - 1)
             const int pos = R.target - 1 < 63 ? (int)R.target - 1 : 63;
             if (pos > 0 && big_bits(nb) + pos < 32 * kMaxLimbs) {
                 Big top = nb;
-                uint32_t c = 1;
-#pragma unroll
-                for (int w = 0; w < kMaxLimbs; w++) {            // n + 1
-                    const uint64_t v = (uint64_t)top.w[w] + c;
-                    top.w[w] = (uint32_t)v;
-                    c = (uint32_t)(v >> 32);
-                }
-                for (int k = 0; k < pos; k++) {                  // << pos
-#pragma unroll
-                    for (int w = kMaxLimbs - 1; w > 0; w--) top.w[w] = (top.w[w] << 1) | (top.w[w - 1] >> 31);
-                    top.w[0] <<= 1;
-                }
-                uint32_t br = 1;
-#pragma unroll
-                for (int w = 0; w < kMaxLimbs; w++) {            // - 1
-                    const uint32_t nv = top.w[w] - br;
-                    br = (br && top.w[w] == 0) ? 1u : 0u;
-                    top.w[w] = nv;
-                }
+                for (int k = 0; k < pos; k++) big_next(top, pc.kind);
                 if (!is_prime_dev(top, pc, mm)) continue;
             }
         }
@@ -665,14 +680,14 @@ prove_kernel(ProveArgs a) {
         Big root = nb;
         bool is_root = true;
         Big pred = nb;
-        big_pred(pred);
+        big_prev(pred, pc.kind);
         if (!big_lt_u32(pred, 2) && is_prime_dev(pred, pc, mm)) {
             is_root = false;
             if (pc.prove_mode == CCS_PROVE_ROOTS) continue;              // v13:1513-1516
             root = pred;
             for (int back = 0; back < kMaxChain; back++) {            // v13:1855-1866
                 Big p2 = root;
-                big_pred(p2);
+                big_prev(p2, pc.kind);
                 if (big_lt_u32(p2, 2)) break;
                 if (!is_prime_dev(p2, pc, mm)) break;
                 root = p2;
@@ -726,20 +741,20 @@ __device__ __forceinline__ void walk_count_mm(uint32_t mm, uint32_t words) {
 
 // member found prime: count it, continue with 2p + 1 or end the walk
 // (MAX_CHAIN, or a next member beyond 192 bits; v13:1519-1528, 1873-1881)
-__device__ __forceinline__ void walk_advance(const WalkItem& it, int nbits, bool live, WalkArgs& a) {
+__device__ __forceinline__ void walk_advance(const WalkItem& it, int nbits, bool live, WalkArgs& a,
+                                             uint32_t kind) {
     const uint32_t len = it.len + 1;
     const bool more = live && len < (uint32_t)kMaxChain && nbits < 32 * kMaxLimbs;
     const uint32_t pos = warp_append(&a.st->n_next, more);
     if (!live) return;
     if (more) {
         WalkItem nx = it;
-        uint32_t carry = 1;
+        Big b;
 #pragma unroll
-        for (int i = 0; i < kMaxLimbs; i++) {
-            const uint32_t nc = nx.x[i] >> 31;
-            nx.x[i] = (nx.x[i] << 1) | carry;
-            carry = nc;
-        }
+        for (int i = 0; i < kMaxLimbs; i++) b.w[i] = nx.x[i];
+        big_next(b, kind);
+#pragma unroll
+        for (int i = 0; i < kMaxLimbs; i++) nx.x[i] = b.w[i];
         nx.len = len;
         a.next[pos] = nx;
     } else {
@@ -780,7 +795,7 @@ walk_screen_kernel(WalkArgs a) {
             a.code[i] = (uint8_t)v;
             if (v == 0) a.lengths[it.idx] = it.len;
         }
-        walk_advance(it, nbits, live && v == 1, a);
+        walk_advance(it, nbits, live && v == 1, a, pc.kind);
 #pragma unroll
         for (int nl = 2; nl <= kMaxLimbs; nl++) {
             const uint32_t m = __ballot_sync(0xFFFFFFFFu, live && v == nl);
@@ -854,7 +869,7 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
             const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas);
             if (to_lucas) a.lucas[off + pos] = it;
         }
-        walk_advance(it, nbits, prime, a);
+        walk_advance(it, nbits, prime, a, pc.kind);
     }
 }
 

@@ -54,7 +54,11 @@ typedef struct {
     uint32_t pos_lo;
 } ccs_stage;
 
-enum { CCS_KIND_FIRST = 1 };
+/* Chain kind.  First kind: p, 2p + 1, 4p + 3, ... (v13).  Second kind:
+ * p, 2p - 1, 4p - 3, ...: forbidden residues 1 - 2^-i instead of 2^-i - 1,
+ * n == 1 (mod 6) instead of 5, predecessor (n + 1) / 2 (the reference's
+ * v13b, v13b:6-14). */
+enum { CCS_KIND_FIRST = 1, CCS_KIND_SECOND = 2 };
 
 /* Primality predicate used by the prover. */
 enum {
@@ -74,7 +78,7 @@ enum {
  * 101..863 (line sieve from position 1), target 18, depth = target, bits 89,
  * v13's 20 witnesses {2..71}, BPSW, full prove. */
 typedef struct {
-    uint32_t kind;                 /* CCS_KIND_FIRST */
+    uint32_t kind;                 /* CCS_KIND_FIRST (0 = first) | CCS_KIND_SECOND */
     uint32_t target;               /* chain length for CRT/wheel admissibility (v13 generate_bases) */
     uint32_t depth;                /* filter depth, clamped to [1, min(target, 32)] (v13:3238-3252) */
     uint32_t bits;                 /* bit width gate of the prover (v13:1495, 1828) */

@@ -55,8 +55,15 @@ static u64 powmod_u64(u64 b, u64 e, u64 m) {
 /* inverse of a mod prime q via Fermat (q prime, a != 0 mod q) */
 static u64 inv_mod_prime(u64 a, u64 q) { return powmod_u64(a % q, q - 2, q); }
 
+/* Chain kind: 1 = first kind (p -> 2p + 1), 2 = second kind (p -> 2p - 1,
+ * the reference's v13b).  Process-wide setting of the test oracle. */
+static int g_kind = 1;
+void orc_set_kind(int kind) { g_kind = (kind == 2) ? 2 : 1; }
+int orc_get_kind(void) { return g_kind; }
+
 /* Forbidden residues of n mod q for positions i in [pos_lo, min(L, q)):
- * p_i = 2^i (n + 1) - 1 == 0 (mod q)  <=>  n == 2^{-i} - 1 (mod q).
+ * p_i = 2^i (n + 1) - 1 == 0 (mod q)  <=>  n == 2^{-i} - 1 (mod q);
+ * second kind: p_i = 2^i (n - 1) + 1 == 0  <=>  n == 1 - 2^{-i} (v13b:779-850).
  * For pos_lo = 0 the reference caps at min(L, q - 1) (v13:774); position
  * q - 1 yields residue 0, the same as position 0, so the set is identical.
  * For pos_lo = 1 the reference caps at min(L, q) (v13:838, "pos < q"). */
@@ -64,7 +71,8 @@ int orc_forbidden(u32 q, int L, int pos_lo, u32* out) {
     int cnt = 0;
     int hi = L < (int)q ? L : (int)q;
     for (int i = pos_lo; i < hi; i++) {
-        u64 r = (inv_mod_prime(powmod_u64(2, (u64)i, q), q) + q - 1) % q;
+        u64 inv = inv_mod_prime(powmod_u64(2, (u64)i, q), q);
+        u64 r = (g_kind == 2) ? (1 + q - inv) % q : (inv + q - 1) % q;
         int dup = 0;
         for (int k = 0; k < cnt; k++) if (out[k] == (u32)r) { dup = 1; break; }
         if (!dup) out[cnt++] = (u32)r;
@@ -138,7 +146,9 @@ orc_lattice* orc_lattice_create(const u32* crt, int n_crt, const u32* wheel, int
         }
         if (nw == 0) { free(wl); continue; }
         L->bases[b] = r;
-        L->tkm6[b] = (u32)(((5 + 6 - r % 6) % 6) * inv_m6 % 6);
+        /* n == 5 (mod 6) for the first kind, n == 1 for the second (v13b:983) */
+        const u32 nres = (g_kind == 2) ? 1 : 5;
+        L->tkm6[b] = (u32)(((nres + 6 - r % 6) % 6) * inv_m6 % 6);
         for (int i = 0; i < nw; i++) tmp[wl[i] % 6]++;
         for (int m = 0; m < 6; m++) {
             L->bucket[b][m] = (u32*)malloc(sizeof(u32) * (tmp[m] ? tmp[m] : 1));
@@ -613,14 +623,16 @@ static int is_prime_p(const big* n, const orc_pred* p) {
     return is_prime_mr(n, p->wit, p->n_wit);
 }
 
-/* forward walk p -> 2p + 1 while prime, counting p itself (v13:1873-1881) */
+/* forward walk p -> 2p + 1 (second kind: 2p - 1) while prime, counting p
+ * itself (v13:1873-1881, v13b:1878-1886) */
 static int walk_forward(const big* root, const orc_pred* p) {
     int len = 1;
     big cur = *root, nx;
     while (len < ORC_MAX_CHAIN) {
         nx = cur;
         big_shl1(&nx);
-        big_add_u64(&nx, &nx, 1);
+        if (g_kind == 2) big_sub_u64(&nx, &nx, 1);
+        else big_add_u64(&nx, &nx, 1);
         if (!is_prime_p(&nx, p)) break;
         len++;
         cur = nx;
@@ -668,7 +680,8 @@ int orc_prove_n(const u64* n_words, int nw, int bits, int mode, int primality,
     *is_prime_out = 1;
     big pred, root = n, two;
     big_set_u64(&two, 2);
-    big_sub_u64(&pred, &n, 1);
+    /* predecessor (n - 1) / 2; second kind (n + 1) / 2 (v13b:1522, 1860) */
+    if (g_kind == 2) big_add_u64(&pred, &n, 1); else big_sub_u64(&pred, &n, 1);
     big_shr1(&pred);
     int is_root = 1;
     if (big_cmp(&pred, &two) >= 0 && is_prime_p(&pred, &p)) {
@@ -677,7 +690,7 @@ int orc_prove_n(const u64* n_words, int nw, int bits, int mode, int primality,
         root = pred;
         int back = 0;
         while (back < ORC_MAX_CHAIN) {
-            big_sub_u64(&pred, &root, 1);
+            if (g_kind == 2) big_add_u64(&pred, &root, 1); else big_sub_u64(&pred, &root, 1);
             big_shr1(&pred);
             if (big_cmp(&pred, &two) < 0) break;
             if (!is_prime_p(&pred, &p)) break;

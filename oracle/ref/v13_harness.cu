@@ -8,8 +8,13 @@
  * v13:3764-3815, and read the results back.  Built into oracle/_ref/ by
  * oracle/Makefile; never part of the product.
  */
+/* The same harness builds over the second-kind variant v13b
+ * (-DREF13_SOURCE='"cc18_filter_cuda_CpC_v13b.cu"', oracle/Makefile). */
+#ifndef REF13_SOURCE
+#define REF13_SOURCE "cc18_filter_cuda_CpC_v13.cu"
+#endif
 #define main v13_reference_main
-#include "cc18_filter_cuda_CpC_v13.cu"
+#include REF13_SOURCE
 #undef main
 
 extern "C" {

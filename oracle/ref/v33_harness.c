@@ -127,3 +127,24 @@ int ref_gmp_forward_chain(const char* hex) {
     mpz_clear(cur); mpz_clear(t);
     return len;
 }
+
+/* The same walk for second-kind chains (p -> 2p - 1), the v13b CPU prover's
+ * loop (v13b:1878-1888): count n, then 2p - 1 while mpz_probab_prime_p(., 1)
+ * != 0, up to MAX_CHAIN.  Returns 0 when n itself is not prime. */
+int ref_gmp_forward_chain2(const char* hex) {
+    mpz_t cur, t; mpz_init(cur); mpz_init(t);
+    mpz_set_str(cur, hex, 16);
+    int len = 0;
+    if (mpz_probab_prime_p(cur, 1) != 0) {
+        len = 1;
+        while (len < MAX_CHAIN) {
+            mpz_mul_2exp(t, cur, 1);
+            mpz_sub_ui(t, t, 1);
+            if (mpz_probab_prime_p(t, 1) == 0) break;
+            len++;
+            mpz_set(cur, t);
+        }
+    }
+    mpz_clear(cur); mpz_clear(t);
+    return len;
+}

@@ -19,8 +19,12 @@ reference itself (run in the container that holds the reference tree):
   * walk_roots.json    -- seeded 80..110-bit odd roots with GMP forward chain
                           lengths (the prove-batch workload)
 
-Usage: python tests/golden/make_golden.py   (needs oracle/_ref built by
-`make -C oracle`).
+  * second_kind.json   -- the same for second-kind chains (v13b): self-test
+                          vectors with GMP 2p - 1 walks and the v13b CPU
+                          prover's output lines
+
+Usage: python tests/golden/make_golden.py [--second-kind]   (needs oracle/_ref
+built by `make -C oracle`).
 """
 import json
 import os
@@ -181,10 +185,52 @@ def main():
                              "roots": walks})
 
 
+def second_kind():
+    """second_kind.json: the reference v13b self-test vectors (read from its
+    source, v13b:2095-2112) and seeded survivors of its filter, with GMP
+    2p - 1 walk lengths (the v13b CPU prover's loop), plus the v13b CPU
+    prover's output lines on survivors of seeded ranges."""
+    r33 = ob.ref33()
+    r13b = ob.ref13b()
+    assert r33 is not None and r13b is not None, "build oracle/_ref first (make -C oracle)"
+    src = open(os.path.join(REF, "src/cuda/cc18_filter_cuda_CpC_v13b.cu")).read()
+    table = src[src.index("Known second-kind Cunningham chain test vectors"):]
+    table = table[:table.index("};")]
+    vecs = re.findall(r'\{\s*"(\d+)",\s*(\d+),', table)
+    known = [{"root": v, "selftest_len": int(n), "forward": r33.ref_gmp_forward_chain2(hex(int(v))[2:].encode())}
+             for v, n in vecs]
+    prover = []
+    import ctypes as C
+    for (target, bits, ts, nt) in [(18, 61, (1 << 60) // (20677 * 1616615) + 5151, 600),
+                                   (16, 64, (1 << 63) // (20677 * 1616615) + 99, 300)]:
+        r13b.ref13_setup(target, target)
+        lat = ob.Lattice(lattice_len=target, depth=target, kind_=2)
+        surv = lat.filter_range(ts, nt)
+        if target < 18:
+            surv = surv[surv[:, 0] < r13b.ref13_num_bases()]
+        s_ = np.ascontiguousarray(surv.astype(np.uint32))
+        path = tempfile.mktemp(suffix=".txt")
+        pr, ch = C.c_ulonglong(0), C.c_ulonglong(0)
+        r13b.ref13_prove_cpu(s_.reshape(-1), len(s_), ts & (2**64 - 1), ts >> 64, target, bits,
+                             path.encode(), C.byref(pr), C.byref(ch))
+        lines = [ln.strip() for ln in open(path) if ln.strip()]
+        os.unlink(path)
+        prover.append({"target": target, "bits": bits, "tile_start": str(ts), "n_tiles": nt,
+                       "primes": pr.value, "chains": ch.value, "lines": sorted(lines),
+                       "survivors": surv.astype(np.int64).tolist()})
+    dump("second_kind.json", {"source": "v13b self-test vectors (v13b:2095-2112), GMP 2p-1 walks; "
+                                        "prove_survivors_mt of v13b via oracle/_ref",
+                              "chains": known, "prover": prover})
+
+
 def C_buf():
     import ctypes as C
     return C.create_string_buffer(256)
 
 
 if __name__ == "__main__":
-    main()
+    if "--second-kind" in sys.argv:
+        second_kind()
+    else:
+        main()
+        second_kind()

@@ -86,9 +86,23 @@ def words_to_int(w):
     return sum(int(x) << (64 * i) for i, x in enumerate(w))
 
 
-def forbidden(q, L, pos_lo=0):
+class kind:
+    """Context manager: run oracle calls for chain kind k (1 first, 2 second)."""
+
+    def __init__(self, k):
+        self.k = k
+
+    def __enter__(self):
+        oracle().orc_set_kind(self.k)
+
+    def __exit__(self, *a):
+        oracle().orc_set_kind(1)
+
+
+def forbidden(q, L, pos_lo=0, kind_=1):
     out = np.zeros(64, dtype=np.uint32)
-    n = oracle().orc_forbidden(q, L, pos_lo, out)
+    with kind(kind_):
+        n = oracle().orc_forbidden(q, L, pos_lo, out)
     return sorted(int(x) for x in out[:n])
 
 
@@ -111,12 +125,13 @@ def powmod(b, e, m):
     return words_to_int(out)
 
 
-def chain_from(n, primality=PRIME_BPSW, witnesses=V13_WITNESSES):
+def chain_from(n, primality=PRIME_BPSW, witnesses=V13_WITNESSES, kind_=1):
     w = np.array(witnesses, dtype=np.uint64)
-    return oracle().orc_chain_from(int_to_words(n), 4, primality, w, len(w))
+    with kind(kind_):
+        return oracle().orc_chain_from(int_to_words(n), 4, primality, w, len(w))
 
 
-def prove_n(n, bits, mode=1, primality=PRIME_BPSW, witnesses=V13_WITNESSES):
+def prove_n(n, bits, mode=1, primality=PRIME_BPSW, witnesses=V13_WITNESSES, kind_=1):
     """Reference prove semantics for one candidate n.  mode 0 = GPU K2
     (roots only), mode 1 = CPU GMP prover (backward walk).  Returns None
     or (chain_len, root, is_root), plus whether n itself tested prime."""
@@ -124,8 +139,9 @@ def prove_n(n, bits, mode=1, primality=PRIME_BPSW, witnesses=V13_WITNESSES):
     root = np.zeros(4, dtype=np.uint64)
     flags = C.c_int(0)
     isp = C.c_int(0)
-    r = oracle().orc_prove_n(int_to_words(n), 4, bits, mode, primality, w, len(w), root,
-                             C.byref(flags), C.byref(isp))
+    with kind(kind_):
+        r = oracle().orc_prove_n(int_to_words(n), 4, bits, mode, primality, w, len(w), root,
+                                 C.byref(flags), C.byref(isp))
     if r < 0:
         return None, bool(isp.value)
     return (r, words_to_int(root), bool(flags.value & 1)), bool(isp.value)
@@ -135,8 +151,10 @@ class Lattice:
     """Oracle lattice + filter stages.  stages: list of (primes, pos_lo)."""
 
     def __init__(self, crt=CRT_PRIMES, wheel=WHEEL_PRIMES, lattice_len=18, depth=18,
-                 stages=None, max_bases=0):
+                 stages=None, max_bases=0, kind_=1):
         lib = oracle()
+        lib.orc_set_kind(kind_)
+        self.kind = kind_
         self.crt = list(crt)
         self.wheel = list(wheel)
         self.M = int(np.prod(self.crt, dtype=object))
@@ -151,6 +169,7 @@ class Lattice:
             a = np.array(primes, dtype=np.uint32)
             lib.orc_add_stage(self.h, a, len(a), pos_lo, depth)
         self.n_bases = lib.orc_num_bases(self.h)
+        lib.orc_set_kind(1)
 
     def __del__(self):
         try:
@@ -227,6 +246,7 @@ def ref33():
     lib.ref33_forward_chain.argtypes = [C.c_char_p]
     lib.ref33_is_root.argtypes = [C.c_char_p]
     lib.ref_gmp_forward_chain.argtypes = [C.c_char_p]
+    lib.ref_gmp_forward_chain2.argtypes = [C.c_char_p]
     return lib
 
 
@@ -244,12 +264,23 @@ def ref15():
     return lib
 
 
+def ref13b():
+    """The reference second-kind engine v13b through the same harness, or None."""
+    path = os.path.join(REF_DIR, "libref13b.so")
+    if not os.path.exists(path):
+        return None
+    return _bind13(C.CDLL(path))
+
+
 def ref13():
     """The reference v13 engine harness (GMP + its CUDA kernels), or None."""
     path = os.path.join(REF_DIR, "libref13.so")
     if not os.path.exists(path):
         return None
-    lib = C.CDLL(path)
+    return _bind13(C.CDLL(path))
+
+
+def _bind13(lib):
     lib.ref13_base.restype = C.c_ulonglong
     lib.ref13_tkm6.restype = C.c_uint
     lib.ref13_bucket.argtypes = [C.c_int, C.c_int, _u32p]
