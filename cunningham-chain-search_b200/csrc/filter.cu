@@ -280,6 +280,15 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         const uint32_t* jm = a.jmod + (uint64_t)cur_range * a.jmod_stride;
         const uint32_t li = g * 32 + lane;
         const bool has_line = li < P.n_lines;
+        if (P.ptab && has_line) {
+            // start pulling this line's phase-table row toward L2 now; it is
+            // read after the pattern copies and range offsets below
+            const char* rp = reinterpret_cast<const char*>(P.ptab + (size_t)li * P.ptab_stride);
+            const uint32_t bytes = P.ptab_stride * 2u;
+            for (uint32_t off = 0; off < bytes; off += 128)
+                asm volatile("prefetch.global.L2 [%0];" :: "l"(rp + off));
+            asm volatile("prefetch.global.L2 [%0];" :: "l"(rp + bytes - 1));
+        }
         const Line ln = has_line ? P.lines[li] : Line{0, 0, 0, 0};
         const uint32_t c = (ln.bc >> 16) & 7u;
         const uint32_t d = ln.bc >> 19;
