@@ -268,6 +268,54 @@ def autotune_engines(ccs, engines, seed):
     return {"seconds": time.time() - t0, "engines": out}
 
 
+def section_reference_runs(ccs, torch, dev, local, tiles=1 << 22, steps=4):
+    """The reference's own GPU run configurations on this engine: v13
+    defaults (target = depth = 18, 89-bit roots, K2 roots-only prove with the
+    v13 witnesses) and the v15 CC19 configuration (target = depth = 19, 88-107
+    bit shells, reverse prove order), filter + prove per 2^22-tile batch,
+    device-timed on the engine stream."""
+    import random
+    out = {}
+    for name, kw, bits_list in [
+            ("v13_defaults_cc18", dict(target=18, bits=89), [89]),
+            ("v15_cc19_reverse", dict(target=19, depth=19, reverse_prove=True), list(range(88, 108)))]:
+        eng = ccs.Engine(device=local, primality=ccs.PRIME_MR, prove_mode=ccs.PROVE_ROOTS, **kw)
+        info = eng.info
+        bases = eng.bases()
+        r = random.Random(SEED + 41)
+        stream = torch.cuda.Stream(device=dev)
+        surv = torch.empty((1 << 22, 4), dtype=torch.int32, device=dev)
+        chains = torch.empty((1 << 18, 12), dtype=torch.int32, device=dev)
+        plan = []
+        for i in range(steps + 1):
+            bits = bits_list[i % len(bits_list)]
+            lo, hi = ccs.bit_tile_range(bits, bases, info["lattice_m"], info["wheel_period"])
+            plan.append((bits, r.randint(lo, hi - tiles - 1)))
+        ms = 0.0
+        n_s = n_c = n_p = 0
+        for i, (bits, ts) in enumerate(plan):
+            eng.set_bits(bits)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s_ = eng.filter_range(ts, tiles, out=surv, stream=stream)
+            c_, p_ = eng.prove(s_, ts, out=chains, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i == 0:
+                continue                                   # warm-up batch
+            ms += e0.elapsed_time(e1)
+            n_s += s_.shape[0]
+            n_c += c_.shape[0]
+            n_p += p_
+        cand = steps * tiles * info["candidates_per_tile"]
+        out[name] = {"candidates_per_s": cand / (ms * 1e-3), "survivors": n_s, "chains": n_c,
+                     "primes": n_p, "ms": ms, "tiles_per_batch": tiles, "batches": steps,
+                     "candidates_per_tile": info["candidates_per_tile"]}
+        eng.close()
+    return out
+
+
 def section_batched(ccs, engines, n_ranges=4096):
     """Uneven ranges: one batched graph replay versus per-range plain calls."""
     ranges = ccs.mixed_ranges(engines, n_ranges, SEED + 11)
@@ -513,6 +561,10 @@ def run_ours(args):
             extra["prove"] = section_prove(ccs, torch, eng, dev, local)
         except Exception as ex:                       # report, keep the headline
             extra["prove"] = {"error": repr(ex)}
+        try:
+            extra["reference_runs"] = section_reference_runs(ccs, torch, dev, local)
+        except Exception as ex:
+            extra["reference_runs"] = {"error": repr(ex)}
         depth_engines = [ccs.Engine(device=local, **ccs.config_depth_profile(d)) for d in range(14, 20)]
         if not args.no_autotune:
             try:

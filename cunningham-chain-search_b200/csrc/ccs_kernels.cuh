@@ -100,6 +100,7 @@ struct WalkState {
     uint32_t n_lucas[kMaxLimbs + 1];     // base-2 probable primes per limb count
 };
 struct WalkArgs {
+    uint32_t max_len;                    // walks end at this length (chain lengths cap)
     WalkState* st;
     const WalkItem* act;
     WalkItem* sorted;                    // act, grouped by limb count
@@ -111,7 +112,29 @@ struct WalkArgs {
 };
 cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
                              WalkItem* out, cudaStream_t st);
-cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, uint32_t primality, cudaStream_t st);
+cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, cudaStream_t st);
+
+// staged prove of one range's survivors (prove.cu)
+struct StagedProve {
+    const ProveRange* range;
+    const uint32_t* surv;                // survivor records (4 x u32)
+    uint32_t first, n_surv;              // this chunk: records [first, first + n_surv)
+    uint32_t* nval;                      // [n_surv][kMaxLimbs] survivor numbers
+    uint32_t* root;                      // [n_surv][kMaxLimbs] current root
+    uint32_t* flags;                     // [n_surv] CCS_CHAIN_IS_ROOT
+    uint32_t* lengths;                   // [n_surv] verdict of the last stage / chain length
+    WalkItem* out;                       // members for the next primality stage
+    uint32_t* count;
+    WalkItem* fwd;                       // roots ready for the forward walk
+    uint32_t* fwd_count;
+    uint32_t* primes;
+    uint32_t* chains;
+    uint32_t* chain_count;
+    uint32_t chain_cap;
+};
+// which: -1 seed, 0 after the top member, 1 after n, 2 after a predecessor, 3 emit
+cudaError_t launch_prove_stage(int which, const StagedProve& p, const WalkItem* in, uint32_t n,
+                               cudaStream_t st);
 int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads);
 cudaError_t modmul_count(uint64_t* out, uint64_t* words, bool reset);
 

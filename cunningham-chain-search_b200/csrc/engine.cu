@@ -36,6 +36,9 @@ ccs_status fail(ccs_status st, const std::string& msg) {
                         std::string(#call) + ": " + cudaGetErrorString(e_));              \
     } while (0)
 
+// survivor counts from which ccs_prove runs the staged (breadth-first) prove
+constexpr uint64_t kStagedProveMin = 256;
+
 // constant-memory profile slots, per device
 std::mutex g_slot_mu;
 uint32_t g_slots_used[64] = {0};
@@ -125,6 +128,9 @@ struct ccs_engine {
     DevBuf<WalkItem> w_act, w_next, w_sorted, w_lucas;
     DevBuf<uint8_t> w_code;
     DevBuf<WalkState> w_state;
+    // staged prove: per-survivor numbers, roots, flags, verdicts; item lists
+    DevBuf<uint32_t> p_nval, p_root, p_flags, p_len, p_ctr;
+    DevBuf<WalkItem> p_items0, p_items1, p_fwd;
     // pinned staging
     void* h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -550,6 +556,8 @@ ccs_status ccs_destroy(ccs_engine* E) {
     E->d_surv_scratch.free_(); E->d_chain_scratch.free_();
     E->w_act.free_(); E->w_next.free_(); E->w_sorted.free_(); E->w_lucas.free_();
     E->w_code.free_(); E->w_state.free_();
+    E->p_nval.free_(); E->p_root.free_(); E->p_flags.free_(); E->p_len.free_(); E->p_ctr.free_();
+    E->p_items0.free_(); E->p_items1.free_(); E->p_fwd.free_();
     if (E->h_stage) cudaFreeHost(E->h_stage);
     if (E->own_stream) cudaStreamDestroy(E->own_stream);
     for (auto& f : E->fs) free_slot(E->device, f.slot);
@@ -667,6 +675,10 @@ ccs_status ccs_filter_range(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint6
     return CCS_OK;
 }
 
+static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
+                               const ProveRange* pr_dev, ccs_chain* out_dev, uint64_t cap,
+                               uint64_t* n_out, uint64_t* primes_out, cudaStream_t st);
+
 ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv, uint64_t ts_lo,
                      uint64_t ts_hi, ccs_chain* out_dev, uint64_t cap, uint64_t* n_out,
                      uint64_t* primes_out, void* stream) {
@@ -685,6 +697,8 @@ ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_sur
     pr->chain_count = nullptr;
     pr->prime_count = E->d_counters.p + 3;
     CU(cudaMemcpyAsync(E->d_prange.p, pr, sizeof(ProveRange), cudaMemcpyHostToDevice, st));
+    if (n_surv >= kStagedProveMin)
+        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, out_dev, cap, n_out, primes_out, st);
     CU(cudaMemsetAsync(E->d_counters.p + 2, 0, 8, st));
     ProveArgs a;
     a.ranges = E->d_prange.p;
@@ -748,6 +762,59 @@ ccs_status ccs_search_range_host(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, 
     return s != CCS_OK ? s : s2;
 }
 
+// capacity for n items of per-batch scratch: the next power of two, so that
+// batches of slightly varying size do not reallocate
+static uint64_t scratch_items(uint64_t n) {
+    uint64_t c = 1024;
+    while (c < n) c <<= 1;
+    return c;
+}
+
+// walk scratch for up to n items
+static ccs_status walk_reserve(ccs_engine* E, uint64_t n) {
+    n = scratch_items(n);
+    if (E->w_act.n < n) {
+        CU(E->w_act.alloc(n)); CU(E->w_next.alloc(n));
+        CU(E->w_sorted.alloc(n)); CU(E->w_lucas.alloc(n));
+        CU(E->w_code.alloc(n));
+    }
+    if (!E->w_state.p) CU(E->w_state.alloc(1));
+    return CCS_OK;
+}
+
+// Breadth-first walk rounds over the n items already in E->w_act: every walk
+// ends at its first composite member or at max_len; lengths[idx] receives
+// the count (the items' len included).
+static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint32_t max_len, cudaStream_t st) {
+    WalkState* hs = (WalkState*)((char*)E->h_stage + 12288);
+    const bool two_stage = E->hp.primality == CCS_PRIME_BPSW || E->hp.witnesses.size() > 1;
+    WalkItem* act = E->w_act.p;
+    WalkItem* nxt = E->w_next.p;
+    uint32_t n_act = n;
+    for (int round = 0; n_act && round <= kMaxChain; round++) {
+        memset(hs, 0, sizeof(WalkState));
+        hs->n_act = n_act;
+        CU(cudaMemcpyAsync(E->w_state.p, hs, sizeof(WalkState), cudaMemcpyHostToDevice, st));
+        WalkArgs a;
+        a.max_len = max_len;
+        a.st = E->w_state.p;
+        a.act = act;
+        a.sorted = E->w_sorted.p;
+        a.lucas = E->w_lucas.p;
+        a.next = nxt;
+        a.code = E->w_code.p;
+        a.lengths = lengths;
+        a.profile = E->slot;
+        CU(launch_walk_round(a, n_act, two_stage, st));
+        E->launches += two_stage ? 5 : 4;
+        CU(cudaMemcpyAsync(hs, &E->w_state.p->n_next, 4, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        n_act = hs->n_act;
+        std::swap(act, nxt);
+    }
+    return CCS_OK;
+}
+
 ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t n, uint32_t limbs,
                             uint32_t* lengths_dev, void* stream) {
     if (!E) return fail(CCS_ERR_INVALID, "null engine");
@@ -759,42 +826,101 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
     // numbers are walked in chunks of up to 2^22, each in rounds until every
     // walk has ended (at most MAX_CHAIN rounds)
     const uint64_t chunk = std::min<uint64_t>(n, 1ull << 22);
-    if (E->w_act.n < chunk) {
-        CU(E->w_act.alloc(chunk)); CU(E->w_next.alloc(chunk));
-        CU(E->w_sorted.alloc(chunk)); CU(E->w_lucas.alloc(chunk));
-        CU(E->w_code.alloc(chunk));
+    {
+        ccs_status s = walk_reserve(E, chunk);
+        if (s != CCS_OK) return s;
     }
-    if (!E->w_state.p) CU(E->w_state.alloc(1));
-    WalkState* hs = (WalkState*)((char*)E->h_stage + 12288);
     for (uint64_t first = 0; first < n; first += chunk) {
         const uint32_t cn = (uint32_t)std::min<uint64_t>(chunk, n - first);
         CU(launch_walk_load(numbers_dev, first, cn, limbs, E->w_act.p, st));
         E->launches += 1;
-        WalkItem* act = E->w_act.p;
-        WalkItem* nxt = E->w_next.p;
-        uint32_t n_act = cn;
-        for (int round = 0; n_act && round <= kMaxChain; round++) {
-            memset(hs, 0, sizeof(WalkState));
-            hs->n_act = n_act;
-            CU(cudaMemcpyAsync(E->w_state.p, hs, sizeof(WalkState), cudaMemcpyHostToDevice, st));
-            WalkArgs a;
-            a.st = E->w_state.p;
-            a.act = act;
-            a.sorted = E->w_sorted.p;
-            a.lucas = E->w_lucas.p;
-            a.next = nxt;
-            a.code = E->w_code.p;
-            a.lengths = lengths_dev;
-            a.profile = E->slot;
-            CU(launch_walk_round(a, n_act, E->hp.primality, st));
-            E->launches += E->hp.primality == CCS_PRIME_BPSW ? 5 : 4;
-            CU(cudaMemcpyAsync(hs, &E->w_state.p->n_next, 4, cudaMemcpyDeviceToHost, st));
-            CU(cudaStreamSynchronize(st));
-            n_act = hs->n_act;
-            std::swap(act, nxt);
-        }
+        ccs_status s = walk_rounds(E, cn, lengths_dev, kMaxChain, st);
+        if (s != CCS_OK) return s;
     }
     CU(cudaStreamSynchronize(st));
+    return CCS_OK;
+}
+
+// Staged prove of n survivors of one range (the prove_kernel semantics, in
+// breadth-first stages; see prove.cu).  pr_dev: the range's ProveRange on
+// the device; counters: chains at hc[0], primes at hc[1].
+static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
+                               const ProveRange* pr_dev, ccs_chain* out_dev, uint64_t cap,
+                               uint64_t* n_out, uint64_t* primes_out, cudaStream_t st) {
+    const uint64_t chunk = std::min<uint64_t>(n_surv, 1ull << 22);
+    {
+        ccs_status s = walk_reserve(E, chunk);
+        if (s != CCS_OK) return s;
+    }
+    const uint64_t cap_items = scratch_items(chunk);
+    if (E->p_len.n < cap_items) {
+        CU(E->p_nval.alloc(cap_items * kMaxLimbs)); CU(E->p_root.alloc(cap_items * kMaxLimbs));
+        CU(E->p_flags.alloc(cap_items)); CU(E->p_len.alloc(cap_items));
+        CU(E->p_items0.alloc(cap_items)); CU(E->p_items1.alloc(cap_items)); CU(E->p_fwd.alloc(cap_items));
+    }
+    if (!E->p_ctr.p) CU(E->p_ctr.alloc(8));
+    uint32_t* hc = (uint32_t*)((char*)E->h_stage + 16384);
+    uint32_t* ctr = E->p_ctr.p;                   // [0] items [1] roots [2] primes [3] chains
+    CU(cudaMemsetAsync(ctr, 0, 32, st));
+    StagedProve p;
+    p.range = pr_dev;
+    p.surv = (const uint32_t*)surv_dev;
+    p.nval = E->p_nval.p;
+    p.root = E->p_root.p;
+    p.flags = E->p_flags.p;
+    p.lengths = E->p_len.p;
+    p.count = ctr;
+    p.fwd = E->p_fwd.p;
+    p.fwd_count = ctr + 1;
+    p.primes = ctr + 2;
+    p.chains = (uint32_t*)out_dev;
+    p.chain_count = ctr + 3;
+    p.chain_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
+    auto read_ctr = [&](int i) -> uint32_t {
+        cudaMemcpyAsync(hc, ctr + i, 4, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        return *hc;
+    };
+    for (uint64_t first = 0; first < n_surv; first += chunk) {
+        p.first = (uint32_t)first;
+        p.n_surv = (uint32_t)std::min<uint64_t>(chunk, n_surv - first);
+        CU(cudaMemsetAsync(ctr, 0, 8, st));                       // items, roots
+        WalkItem* lists[2] = {E->p_items0.p, E->p_items1.p};
+        int cur = 0;
+        p.out = lists[cur];
+        CU(launch_prove_stage(-1, p, nullptr, p.n_surv, st));
+        uint32_t n = read_ctr(0);
+        // primality stages: the top member (reverse order), n, then predecessors
+        int stage = E->hp.reverse_prove ? 0 : 1;
+        while (n) {
+            CU(cudaMemcpyAsync(E->w_act.p, lists[cur], sizeof(WalkItem) * n, cudaMemcpyDeviceToDevice, st));
+            {
+                ccs_status s = walk_rounds(E, n, p.lengths, 1, st);
+                if (s != CCS_OK) return s;
+            }
+            CU(cudaMemsetAsync(ctr, 0, 4, st));
+            p.out = lists[cur ^ 1];
+            CU(launch_prove_stage(stage, p, lists[cur], n, st));
+            E->launches += 1;
+            n = read_ctr(0);
+            cur ^= 1;
+            if (stage < 2) stage++;
+        }
+        // forward walks from the roots, then their records
+        const uint32_t nr = read_ctr(1);
+        if (nr) {
+            CU(cudaMemcpyAsync(E->w_act.p, E->p_fwd.p, sizeof(WalkItem) * nr, cudaMemcpyDeviceToDevice, st));
+            ccs_status s = walk_rounds(E, nr, p.lengths, kMaxChain, st);
+            if (s != CCS_OK) return s;
+            CU(launch_prove_stage(3, p, E->p_fwd.p, nr, st));
+            E->launches += 1;
+        }
+    }
+    CU(cudaMemcpyAsync(hc, ctr + 2, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    *n_out = hc[1];
+    if (primes_out) *primes_out = hc[0];
+    if (hc[1] > cap) return fail(CCS_OVERFLOW, "chain capacity exceeded");
     return CCS_OK;
 }
 

@@ -623,6 +623,35 @@ __constant__ uint32_t c_screen[132] = {
 // ---------------------------------------------------------------------------
 // prove kernel: one thread per survivor
 // ---------------------------------------------------------------------------
+// n = ((T0 + tile_idx) * WP + k) * M + base   (v13:1479-1492)
+__device__ __forceinline__ Big survivor_number(const uint4 s, const ProveRange& R, const ProveConst& pc) {
+    Big nb;
+    uint64_t c = s.z;
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        const uint64_t v = (uint64_t)R.T0[w] + c;
+        nb.w[w] = (uint32_t)v;
+        c = v >> 32;
+    }
+    nb.w[4] = (uint32_t)c;
+    nb.w[5] = 0;
+    c = s.y;
+#pragma unroll
+    for (int w = 0; w < kMaxLimbs; w++) {
+        const uint64_t v = (uint64_t)nb.w[w] * pc.WP + c;
+        nb.w[w] = (uint32_t)v;
+        c = v >> 32;
+    }
+    c = (s.x < pc.n_bases) ? pc.bases[s.x] : 0;
+#pragma unroll
+    for (int w = 0; w < kMaxLimbs; w++) {
+        const uint64_t v = (uint64_t)nb.w[w] * pc.M + c;
+        nb.w[w] = (uint32_t)v;
+        c = v >> 32;
+    }
+    return nb;
+}
+
 __global__ void __launch_bounds__(128)
 prove_kernel(ProveArgs a) {
     uint32_t n = a.n_surv_dev ? *a.n_surv_dev : a.n_surv;
@@ -744,7 +773,7 @@ __device__ __forceinline__ void walk_count_mm(uint32_t mm, uint32_t words) {
 __device__ __forceinline__ void walk_advance(const WalkItem& it, int nbits, bool live, WalkArgs& a,
                                              uint32_t kind) {
     const uint32_t len = it.len + 1;
-    const bool more = live && len < (uint32_t)kMaxChain && nbits < 32 * kMaxLimbs;
+    const bool more = live && len < a.max_len && nbits < 32 * kMaxLimbs;
     const uint32_t pos = warp_append(&a.st->n_next, more);
     if (!live) return;
     if (more) {
@@ -850,15 +879,21 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
             Mont<NL> M;
             mont_setup<NL>(M, b, nbits);
             M.count = 0;
-                    if (stage == 0) {
+            if (stage == 0) {
+                // the first test for every member; the rest only for its
+                // probable primes, in a second launch of uniform warps
                 if (pc.primality == CCS_PRIME_BPSW) {
                     to_lucas = strong_prp<NL>(M, b, 2);
+                } else if (pc.n_wit <= 1) {
+                    prime = pc.n_wit == 0 || strong_prp<NL>(M, b, pc.wit[0]);
                 } else {
-                    prime = true;
-                    for (uint32_t k = 0; k < pc.n_wit && prime; k++) prime = strong_prp<NL>(M, b, pc.wit[k]);
+                    to_lucas = strong_prp<NL>(M, b, pc.wit[0]);
                 }
-            } else {
+            } else if (pc.primality == CCS_PRIME_BPSW) {
                 prime = strong_lucas<NL>(M, b);
+            } else {
+                prime = true;
+                for (uint32_t k = 1; k < pc.n_wit && prime; k++) prime = strong_prp<NL>(M, b, pc.wit[k]);
             }
             mm = M.count;
             words = M.count * (2 * NL * NL + NL);
@@ -873,8 +908,8 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
     }
 }
 
-// blockIdx.y selects the limb count (2 + y); stage 0 = base-2 strong test (or
-// the witness list), stage 1 = strong Lucas test
+// blockIdx.y selects the limb count (2 + y); stage 0 = base-2 strong test
+// (first witness), stage 1 = strong Lucas test (the other witnesses)
 __global__ void __launch_bounds__(128, 4)
 walk_test_kernel(WalkArgs a, int stage) {
     const ProveConst& pc = c_prove[a.profile];
@@ -894,14 +929,176 @@ cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n
     return cudaGetLastError();
 }
 
-cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, uint32_t primality, cudaStream_t st) {
+cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, cudaStream_t st) {
     const uint32_t blocks = std::min<uint32_t>((n_act + 255) / 256, 148 * 8);
     walk_screen_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(a);
     walk_regions_kernel<<<1, 32, 0, st>>>(a.st);
     walk_scatter_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(a);
     const uint32_t tb = std::min<uint32_t>((n_act + 127) / 128, 148 * 16);
     walk_test_kernel<<<dim3(tb ? tb : 1, kMaxLimbs - 1), 128, 0, st>>>(a, 0);
-    if (primality == CCS_PRIME_BPSW) walk_test_kernel<<<dim3(tb ? tb : 1, kMaxLimbs - 1), 128, 0, st>>>(a, 1);
+    if (two_stage) walk_test_kernel<<<dim3(tb ? tb : 1, kMaxLimbs - 1), 128, 0, st>>>(a, 1);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// staged prove of a filter launch's survivors
+//
+// The same semantics as prove_kernel, run as breadth-first stages over all
+// survivors so warps do one kind of test at a time: seed (reconstruction,
+// bit gate, trial division; with the reverse order the top member), then
+// primality of the members each stage asks for through the walk rounds
+// above (max length 1), then the forward walk from every root.  Per survivor
+// index: its number, its current root, and the stage's verdict in
+// lengths[idx].
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void big_store(uint32_t* dst, const Big& b) {
+#pragma unroll
+    for (int w = 0; w < kMaxLimbs; w++) dst[w] = b.w[w];
+}
+__device__ __forceinline__ Big big_load(const uint32_t* src) {
+    Big b;
+#pragma unroll
+    for (int w = 0; w < kMaxLimbs; w++) b.w[w] = src[w];
+    return b;
+}
+__device__ __forceinline__ void item_put(WalkItem* out, uint32_t pos, const Big& x, uint32_t idx, uint32_t len) {
+    WalkItem it;
+#pragma unroll
+    for (int w = 0; w < kMaxLimbs; w++) it.x[w] = x.w[w];
+    it.idx = idx;
+    it.len = len;
+    out[pos] = it;
+}
+
+__global__ void __launch_bounds__(256)
+prove_seed_kernel(StagedProve p) {
+    const ProveConst& pc = c_prove[p.range->profile];
+    const ProveRange& R = *p.range;
+    const uint32_t ntd = (pc.prove_mode == CCS_PROVE_ROOTS) ? 132 : 62;        // v13:1499 / 1832
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < p.n_surv; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        bool keep = false;
+        Big nb, x;
+        if (i < p.n_surv) {
+            const uint4 sv = reinterpret_cast<const uint4*>(p.surv)[p.first + i];
+            nb = survivor_number(sv, R, pc);
+            keep = big_bits(nb) == (int)R.bits;                                  // v13:1495, 1828
+            for (uint32_t t = 0; t < ntd && keep; t++) keep = big_mod_small(nb, c_screen[t]) != 0;
+            x = nb;
+            if (keep) {
+                big_store(p.nval + (size_t)i * kMaxLimbs, nb);
+                if (pc.reverse) {
+                    // chain position target - 1 first (v15:1704-1708)
+                    const int pos = R.target - 1 < 63 ? (int)R.target - 1 : 63;
+                    if (pos > 0 && big_bits(nb) + pos < 32 * kMaxLimbs)
+                        for (int k = 0; k < pos; k++) big_next(x, pc.kind);
+                }
+            }
+        }
+        const uint32_t pos = warp_append(p.count, keep);
+        if (keep) item_put(p.out, pos, x, i, 0);
+    }
+}
+
+// after a primality stage over the items of `in` (len: backward steps so far)
+//   stage 0: the reverse order's top member -> test n itself
+//   stage 1: n itself  -> count the prime; test its predecessor (or it is a root)
+//   stage 2: a predecessor -> prime: not a root (roots-only mode drops it,
+//            otherwise it becomes the root candidate and its own predecessor is
+//            tested next); composite: the current root is final
+__global__ void __launch_bounds__(256)
+prove_select_kernel(StagedProve p, const WalkItem* in, uint32_t n_in, int stage) {
+    const ProveConst& pc = c_prove[p.range->profile];
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n_in; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        bool emit = false, to_fwd = false;
+        Big x;
+        uint32_t idx = 0;
+        if (i < n_in) {
+            const WalkItem it = in[i];
+            idx = it.idx;
+            // the walk of one member leaves len + 1 when it is prime, len otherwise
+            const bool prime = p.lengths[idx] == it.len + 1;
+            if (stage == 0) {
+                if (prime) { x = big_load(p.nval + (size_t)idx * kMaxLimbs); emit = true; }
+            } else if (stage == 1) {
+                if (prime) {
+                    atomicAdd(p.primes, 1u);
+                    const Big nb = big_load(p.nval + (size_t)idx * kMaxLimbs);
+                    big_store(p.root + (size_t)idx * kMaxLimbs, nb);
+                    p.flags[idx] = CCS_CHAIN_IS_ROOT;
+                    x = nb;
+                    big_prev(x, pc.kind);
+                    if (big_lt_u32(x, 2)) to_fwd = true; else emit = true;
+                }
+            } else {
+                if (prime) {
+                    if (pc.prove_mode != CCS_PROVE_ROOTS) {                       // v13:1855-1866
+                        Big r;
+#pragma unroll
+                        for (int w = 0; w < kMaxLimbs; w++) r.w[w] = it.x[w];
+                        big_store(p.root + (size_t)idx * kMaxLimbs, r);
+                        p.flags[idx] = 0;
+                        if (it.len >= (uint32_t)kMaxChain) {
+                            to_fwd = true;                 // the backward walk's step cap
+                        } else {
+                            x = r;
+                            big_prev(x, pc.kind);
+                            if (big_lt_u32(x, 2)) to_fwd = true; else emit = true;
+                        }
+                    }                                        // roots-only: dropped (v13:1513-1516)
+                } else {
+                    to_fwd = true;
+                }
+            }
+        }
+        const uint32_t pos = warp_append(p.count, emit);
+        if (emit) item_put(p.out, pos, x, idx, stage == 2 ? in[i].len + 1 : 0);
+        const uint32_t fpos = warp_append(p.fwd_count, to_fwd);
+        if (to_fwd) {
+            // forward walk from the root: its next member, the root counted;
+            // a root of 192 bits has no next member (0 ends the walk at 1)
+            const Big r = big_load(p.root + (size_t)idx * kMaxLimbs);
+            Big nx = r;
+            if (big_bits(r) >= 32 * kMaxLimbs) {
+#pragma unroll
+                for (int w = 0; w < kMaxLimbs; w++) nx.w[w] = 0;
+            } else {
+                big_next(nx, pc.kind);
+            }
+            item_put(p.fwd, fpos, nx, idx, 1u);
+        }
+    }
+}
+
+// records of the walked roots: lengths[idx] = chain length
+__global__ void __launch_bounds__(256)
+prove_emit_kernel(StagedProve p, const WalkItem* roots, uint32_t n_roots) {
+    const ProveRange& R = *p.range;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_roots; i += gridDim.x * blockDim.x) {
+        const uint32_t idx = roots[i].idx;
+        const uint32_t len = p.lengths[idx];
+        const uint4 sv = reinterpret_cast<const uint4*>(p.surv)[p.first + idx];
+        const uint32_t slot = atomicAdd(p.chain_count, 1u);
+        if (slot < p.chain_cap) {
+            uint32_t* o = p.chains + (size_t)slot * 12;
+            o[0] = sv.x; o[1] = sv.y; o[2] = sv.z; o[3] = len;
+#pragma unroll
+            for (int w = 0; w < 6; w++) o[4 + w] = p.root[(size_t)idx * kMaxLimbs + w];
+            o[10] = p.flags[idx] | (len >= R.target ? CCS_CHAIN_TARGET : 0u);
+            o[11] = p.first + idx;
+        }
+    }
+}
+
+cudaError_t launch_prove_stage(int which, const StagedProve& p, const WalkItem* in, uint32_t n,
+                               cudaStream_t st) {
+    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 255) / 256, 148 * 8));
+    switch (which) {
+        case -1: prove_seed_kernel<<<blocks, 256, 0, st>>>(p); break;
+        case 0: case 1: case 2: prove_select_kernel<<<blocks, 256, 0, st>>>(p, in, n, which); break;
+        default: prove_emit_kernel<<<blocks, 256, 0, st>>>(p, in, n); break;
+    }
     return cudaGetLastError();
 }
 

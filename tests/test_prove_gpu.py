@@ -213,3 +213,41 @@ def test_matches_reference_v15_filter_and_prove_order(ccs, ob, reverse):
         assert got == ref, (reverse, n_tiles)
         assert primes == pr.value
     eng.close()
+
+
+@pytest.mark.parametrize("cfg", [
+    dict(bits=89, primality="MR", prove_mode="ROOTS"),
+    dict(bits=89, primality="BPSW", prove_mode="FULL"),
+    dict(bits=61, primality="MR", prove_mode="ROOTS", reverse_prove=True),
+    dict(bits=70, primality="BPSW", prove_mode="ROOTS", reverse_prove=True),
+    dict(bits=80, primality="BPSW", prove_mode="FULL", kind=2),
+])
+def test_staged_prove_equals_per_survivor_prove(ccs, cfg):
+    """ccs_prove runs a breadth-first staged prove from 256 survivors up and
+    the one-thread-per-survivor kernel below that: the whole survivor set in
+    one call must give the records of the same set proved in slices of 200
+    (survivor index shifted by the slice start), and the same prime count."""
+    import torch
+    kw = dict(cfg)
+    kw["primality"] = getattr(ccs, "PRIME_" + kw["primality"])
+    kw["prove_mode"] = getattr(ccs, "PROVE_" + kw["prove_mode"])
+    eng = ccs.Engine(**kw)
+    info = eng.info
+    lo, hi = ccs.bit_tile_range(cfg["bits"], eng.bases(), info["lattice_m"], info["wheel_period"])
+    r = random.Random(cfg["bits"] * 7 + cfg.get("kind", 1))
+    ts = r.randint(lo, max(lo, hi - 40000))
+    surv = eng.filter_range(ts, min(20000, hi - ts), cap=1 << 20)
+    assert surv.shape[0] >= 600
+    whole, p_whole = eng.prove(surv, ts, cap=1 << 18)
+    parts, p_parts = [], 0
+    for s0 in range(0, surv.shape[0], 200):
+        c, p = eng.prove(surv[s0:s0 + 200], ts, cap=1 << 16)
+        c = c.clone()
+        c[:, 11] += s0
+        parts.append(c)
+        p_parts += p
+    parts = torch.cat(parts)
+    key = lambda t: sorted(map(tuple, (t.cpu().numpy().astype(np.int64) & 0xFFFFFFFF).tolist()))
+    assert p_whole == p_parts
+    assert key(whole) == key(parts) and whole.shape[0] > 0
+    eng.close()
