@@ -147,6 +147,17 @@ class _BatchTuning(C.Structure):
 # exported symbols of include/ccs.h, with their ctypes signatures
 _vp = C.c_void_p
 _u64 = C.c_uint64
+class _QIterParams(C.Structure):
+    _fields_ = [("n_variants", C.c_uint32), ("dv", C.POINTER(C.c_uint32)), ("exp_start", C.c_uint32),
+                ("depth", C.c_uint32), ("target", C.c_uint32), ("n_primes", C.c_uint32),
+                ("primes", C.POINTER(C.c_uint32)), ("primality", C.c_uint32), ("prove_mode", C.c_uint32),
+                ("flags", C.c_uint32)]
+
+
+class _QSeg(C.Structure):
+    _fields_ = [("q_base", C.c_uint32 * 4), ("n_q", C.c_uint32), ("variant", C.c_uint32)]
+
+
 _SIGS = {
     "ccs_describe": (C.c_int, [C.POINTER(_Params), C.POINTER(_Info), C.POINTER(_u64), C.c_uint32]),
     "ccs_create": (C.c_int, [C.POINTER(_Params), C.c_int, C.POINTER(_vp)]),
@@ -189,6 +200,12 @@ _SIGS = {
     "ccs_batch_set_tuning": (C.c_int, [_vp, C.POINTER(_BatchTuning)]),
     "ccs_batch_autotune": (C.c_int, [_vp, _vp, C.c_uint32, C.POINTER(_TunePoint), C.c_uint32,
                                      C.POINTER(C.c_uint32), C.POINTER(_BatchTuning)]),
+    "ccs_qiter_create": (C.c_int, [C.POINTER(_QIterParams), C.c_int, C.POINTER(_vp)]),
+    "ccs_qiter_destroy": (C.c_int, [_vp]),
+    "ccs_qiter_filter": (C.c_int, [_vp, C.POINTER(_QSeg), C.c_uint32, _vp, _u64, C.POINTER(_u64), _vp]),
+    "ccs_qiter_prove": (C.c_int, [_vp, C.POINTER(_QSeg), C.c_uint32, _vp, _u64, _vp, _u64,
+                                  C.POINTER(_u64), C.POINTER(_u64), _vp]),
+    "ccs_qiter_forbidden_count": (C.c_int, [_vp, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
 }
 
 _LIB = None
@@ -771,3 +788,7 @@ def mixed_ranges(engines, n, seed, min_log2=20, max_log2=34, width_lo=64, width_
         ts = r.randint(t0, max(t0, t1 - nt - 1))
         out.append((ts, nt, p, bits))
     return out
+
+
+from .qiter import (QIter, parse_pool, parse_pool_spec, parse_pool_specs, pool_from_text,  # noqa: E402
+                    qiter_sieve_primes, q_window, V16_EXT_PRIMES, format_hit_line)

@@ -2,11 +2,29 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include "../../include/ccs.h"
 #include "ccs_internal.h"
 
 namespace ccs {
 
 constexpr int kSweepThreads = 256;
+
+// device buffer owned by a host object (freed explicitly)
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        free_();
+        n = count;
+        return cudaMalloc((void**)&p, sizeof(T) * (count ? count : 1));
+    }
+    void free_() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
 
 // One lattice range as the device sees it.
 struct RangeDev {
@@ -114,8 +132,18 @@ cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n
                              WalkItem* out, cudaStream_t st);
 cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, cudaStream_t st);
 
+// q-iteration survivors {offset, seg, variant} in a staged prove:
+// p_0 = (q_base[seg] + offset) * D_V * 2^E - 1
+struct QiterProve {
+    const uint32_t* seg;                 // [n_segs][6]: q_base limbs, n_q, variant (null: lattice survivors)
+    const uint32_t* dv;                  // [n_variants][4]
+    uint32_t exp_start;
+    uint32_t n_segs;                     // survivors naming another segment are skipped
+};
+
 // staged prove of one range's survivors (prove.cu)
 struct StagedProve {
+    QiterProve q;
     const ProveRange* range;
     const uint32_t* surv;                // survivor records (4 x u32)
     uint32_t first, n_surv;              // this chunk: records [first, first + n_surv)
@@ -136,6 +164,17 @@ struct StagedProve {
 cudaError_t launch_prove_stage(int which, const StagedProve& p, const WalkItem* in, uint32_t n,
                                cudaStream_t st);
 int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads);
+
+// engine services used by the q-iteration object (engine.cu); set_error
+// records the message ccs_last_error returns
+ccs_status set_error(ccs_status st, const char* msg);
+ccs_status engine_create_prover(int device, uint32_t primality, uint32_t prove_mode, bool reverse,
+                                uint32_t target, ccs_engine** out);
+ccs_status engine_prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
+                               const ProveRange& pr, const QiterProve* q, ccs_chain* out_dev,
+                               uint64_t cap, uint64_t* n_out, uint64_t* primes_out, cudaStream_t st);
+cudaStream_t engine_stream(ccs_engine* E);
+int engine_slot(const ccs_engine* E);
 cudaError_t modmul_count(uint64_t* out, uint64_t* words, bool reset);
 
 }  // namespace ccs

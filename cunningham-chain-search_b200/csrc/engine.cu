@@ -61,22 +61,6 @@ const uint32_t kRefL2[] = {37, 41, 43, 47, 53, 59, 61};
 const uint32_t kRefExt[] = {67, 71, 73, 79, 83, 89, 97};
 const uint64_t kRefWit[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71};
 
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    cudaError_t alloc(size_t count) {
-        free_();
-        n = count;
-        return cudaMalloc((void**)&p, sizeof(T) * (count ? count : 1));
-    }
-    void free_() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-};
-
 // One filter variant of a profile: the lattice lines and the per-prime tables
 // the sweep reads, plus the constant-memory slot they are registered in.
 struct FilterSet {
@@ -676,8 +660,8 @@ ccs_status ccs_filter_range(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint6
 }
 
 static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
-                               const ProveRange* pr_dev, ccs_chain* out_dev, uint64_t cap,
-                               uint64_t* n_out, uint64_t* primes_out, cudaStream_t st);
+                               const ProveRange* pr_dev, const QiterProve* q, ccs_chain* out_dev,
+                               uint64_t cap, uint64_t* n_out, uint64_t* primes_out, cudaStream_t st);
 
 ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv, uint64_t ts_lo,
                      uint64_t ts_hi, ccs_chain* out_dev, uint64_t cap, uint64_t* n_out,
@@ -698,7 +682,7 @@ ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_sur
     pr->prime_count = E->d_counters.p + 3;
     CU(cudaMemcpyAsync(E->d_prange.p, pr, sizeof(ProveRange), cudaMemcpyHostToDevice, st));
     if (n_surv >= kStagedProveMin)
-        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, out_dev, cap, n_out, primes_out, st);
+        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, nullptr, out_dev, cap, n_out, primes_out, st);
     CU(cudaMemsetAsync(E->d_counters.p + 2, 0, 8, st));
     ProveArgs a;
     a.ranges = E->d_prange.p;
@@ -845,8 +829,13 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
 // breadth-first stages; see prove.cu).  pr_dev: the range's ProveRange on
 // the device; counters: chains at hc[0], primes at hc[1].
 static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
-                               const ProveRange* pr_dev, ccs_chain* out_dev, uint64_t cap,
-                               uint64_t* n_out, uint64_t* primes_out, cudaStream_t st) {
+                               const ProveRange* pr_dev, const QiterProve* q, ccs_chain* out_dev,
+                               uint64_t cap, uint64_t* n_out, uint64_t* primes_out, cudaStream_t st) {
+    if (n_surv == 0) {
+        *n_out = 0;
+        if (primes_out) *primes_out = 0;
+        return CCS_OK;
+    }
     const uint64_t chunk = std::min<uint64_t>(n_surv, 1ull << 22);
     {
         ccs_status s = walk_reserve(E, chunk);
@@ -863,6 +852,7 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
     uint32_t* ctr = E->p_ctr.p;                   // [0] items [1] roots [2] primes [3] chains
     CU(cudaMemsetAsync(ctr, 0, 32, st));
     StagedProve p;
+    p.q = q ? *q : QiterProve{nullptr, nullptr, 0, 0};
     p.range = pr_dev;
     p.surv = (const uint32_t*)surv_dev;
     p.nval = E->p_nval.p;
@@ -923,6 +913,74 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
     if (hc[1] > cap) return fail(CCS_OVERFLOW, "chain capacity exceeded");
     return CCS_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// engine services for the q-iteration object
+// ---------------------------------------------------------------------------
+namespace ccs {
+
+ccs_status set_error(ccs_status st, const char* msg) { return fail(st, msg); }
+
+// An engine with no filter tables: one prove-constant slot (the predicate,
+// prove mode and order; no lattice), the walk scratch and the staging.
+ccs_status engine_create_prover(int device, uint32_t primality, uint32_t prove_mode, bool reverse,
+                                uint32_t target, ccs_engine** out) {
+    *out = nullptr;
+    if (primality > 1 || prove_mode > 1) return fail(CCS_ERR_INVALID, "bad primality / prove_mode");
+    if (reverse && prove_mode != CCS_PROVE_ROOTS)
+        return fail(CCS_ERR_INVALID, "reverse prove order is a CCS_PROVE_ROOTS option");
+    CU(cudaSetDevice(device));
+    ccs_engine* E = new ccs_engine();
+    E->device = device;
+    HostProfile& hp = E->hp;
+    hp.target = target;
+    hp.depth = target;
+    hp.bits = 0;
+    hp.primality = primality;
+    hp.prove_mode = prove_mode;
+    hp.reverse_prove = reverse ? 1u : 0u;
+    hp.kind = 1;
+    hp.witnesses.assign(kRefWit, kRefWit + 20);
+    E->fs[0].slot = alloc_slot(device);
+    if (E->fs[0].slot < 0) { delete E; return fail(CCS_ERR_INVALID, "no free constant-memory slot"); }
+    E->slot = E->fs[0].slot;
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    E->sms = prop.multiProcessorCount;
+    CU(cudaStreamCreateWithFlags(&E->own_stream, cudaStreamNonBlocking));
+    ccs_status st = upload_prove(E, E->own_stream);
+    if (st != CCS_OK) { ccs_destroy(E); return st; }
+    if (E->d_prange.alloc(1) || E->d_counters.alloc(8)) {
+        ccs_destroy(E);
+        return fail(CCS_ERR_NOMEM, "device allocation failed");
+    }
+    E->h_stage_bytes = 1 << 16;
+    if (cudaMallocHost(&E->h_stage, E->h_stage_bytes) != cudaSuccess) {
+        ccs_destroy(E);
+        return fail(CCS_ERR_NOMEM, "pinned allocation failed");
+    }
+    *out = E;
+    return CCS_OK;
+}
+
+ccs_status engine_prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
+                               const ProveRange& pr, const QiterProve* q, ccs_chain* out_dev,
+                               uint64_t cap, uint64_t* n_out, uint64_t* primes_out, cudaStream_t st) {
+    ProveRange* h = (ProveRange*)((char*)E->h_stage + 4096);
+    *h = pr;
+    h->profile = (uint32_t)E->slot;
+    CU(cudaMemcpyAsync(E->d_prange.p, h, sizeof(ProveRange), cudaMemcpyHostToDevice, st));
+    return prove_staged(E, surv_dev, n_surv, E->d_prange.p, q, out_dev, cap, n_out, primes_out, st);
+}
+
+cudaStream_t engine_stream(ccs_engine* E) { return E->own_stream; }
+int engine_slot(const ccs_engine* E) { return E->slot; }
+
+}  // namespace ccs
+
+extern "C" {
 
 ccs_status ccs_walk_modmuls(ccs_engine* E, uint64_t* count, int reset) {
     if (!E || !count) return fail(CCS_ERR_INVALID, "null argument");

@@ -393,6 +393,79 @@ ccs_status ccs_walk_modmuls(ccs_engine* eng, uint64_t* count, int reset);
  * word product is one IMAD lo/hi pair. */
 ccs_status ccs_walk_word_products(ccs_engine* eng, uint64_t* modmuls, uint64_t* words, int reset);
 
+/* ------------------------------------------------------------------------
+ * Fingerprint-pool Q iteration (the reference's v16 engine,
+ * experimental/cc20_first_kind_immune_v16.cu).
+ *
+ * Candidates are p_0 = Q * D_V * 2^E - 1 for the variants V of a pool of
+ * fingerprints D_V and consecutive Q.  Chain position j is
+ * p_j = 2^(E+j) * Q * D_V - 1, so a prime q not dividing D_V divides p_j
+ * exactly when Q = (D_V * 2^(E+j))^-1 (mod q); a Q is a survivor when no
+ * sieve prime divides any of p_0 .. p_(depth-1) (v16:1244-1266, the
+ * per-(V, q) forbid mask of v16:5104-5178 and its probe in
+ * v16_q_iter_kernel, v16:2038-2153).  Primes that divide D_V sieve nothing
+ * for V (the reference's active-prime pruning, v16:5229-5299).
+ * ------------------------------------------------------------------------ */
+typedef struct ccs_qiter ccs_qiter;
+
+typedef struct {
+    uint32_t n_variants;
+    const uint32_t* dv;        /* [n_variants][4]: D_V as little-endian 32-bit limbs (< 2^128) */
+    uint32_t exp_start;        /* E (--exp-start) */
+    uint32_t depth;            /* sieved chain positions 0 .. depth-1 (--depth) */
+    uint32_t target;           /* chain length of interest (--target): reverse prove order, TARGET flag */
+    uint32_t n_primes;
+    const uint32_t* primes;    /* sieve primes, ascending, odd, < 8192: the reference's q-iter list
+                                  (7..sieve-max, v16:4680-4720) and, optionally, its CPU-side
+                                  extended primes 509..1009 (v16:174-187, 2595-2616) */
+    uint32_t primality;        /* CCS_PRIME_BPSW = mpz_probab_prime_p (v16:2677-2722) */
+    uint32_t prove_mode;       /* CCS_PROVE_ROOTS: the reference's q-iter prover reports roots only */
+    uint32_t flags;            /* CCS_FLAG_REVERSE_PROVE: position target - 1 first (the default
+                                  --prove-order reverse, v16:2658-2673) */
+} ccs_qiter_params;
+
+/* One run of consecutive Q: Q = q_base + offset for offset < n_q, one variant. */
+typedef struct {
+    uint32_t q_base[4];        /* little-endian 32-bit limbs */
+    uint32_t n_q;              /* Q values (the reference's --q-chunk per launch) */
+    uint32_t variant;
+} ccs_qseg;
+
+/* Filter output: the reference's QSurvivor {thread_offset, seed_idx}
+ * (v16:2140-2150) with the segment index; 16 bytes. */
+typedef struct {
+    uint32_t offset;           /* Q - q_base of the segment */
+    uint32_t seg;
+    uint32_t variant;
+    uint32_t _pad;             /* written as 0 */
+} ccs_qsurvivor;
+
+/* Builds the per-variant forbidden-Q windows and uploads them. */
+ccs_status ccs_qiter_create(const ccs_qiter_params* params, int device, ccs_qiter** out);
+ccs_status ccs_qiter_destroy(ccs_qiter* qe);
+
+/* Survivors of all segments (host array, n_segs <= 2^20) into a
+ * caller-owned device buffer; CCS_OVERFLOW with the exact count in *n_out
+ * when cap is too small.  Replaces v16_q_iter_kernel launched once per
+ * (variant, chunk) (v16:5837-5881). */
+ccs_status ccs_qiter_filter(ccs_qiter* qe, const ccs_qseg* segs, uint32_t n_segs, ccs_qsurvivor* out_dev,
+                            uint64_t cap, uint64_t* n_out, void* stream);
+
+/* Proves survivors on the device (BPSW predicate, reverse order, roots
+ * only: the q-iter path of cpu_prove_worker, v16:2540-2722).  Records are
+ * ccs_chain with base_idx = offset, k_offset = seg, tile_idx = variant and
+ * root = p_0.  Every (Q + n_q) * D_V * 2^E of the segments must stay below
+ * 2^160.  *primes_out counts survivors whose p_0 tested prime (after the
+ * reverse gate). */
+ccs_status ccs_qiter_prove(ccs_qiter* qe, const ccs_qseg* segs, uint32_t n_segs,
+                           const ccs_qsurvivor* surv_dev, uint64_t n_surv, ccs_chain* out_dev,
+                           uint64_t cap, uint64_t* n_out, uint64_t* primes_out, void* stream);
+
+/* For variant v: counts[i] = how many residues of Q mod primes[i] are
+ * forbidden (0 when primes[i] divides D_V: the prime is pruned), as the
+ * uploaded windows hold them. */
+ccs_status ccs_qiter_forbidden_count(const ccs_qiter* qe, uint32_t variant, uint32_t* counts, uint32_t cap);
+
 #ifdef __cplusplus
 }
 #endif

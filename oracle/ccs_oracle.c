@@ -730,3 +730,136 @@ void orc_reconstruct(const orc_lattice* L, u64 ts_lo, u64 ts_hi, u32 base_idx, u
     big_add_u64(&prod, &prod, L->bases[base_idx]);
     memcpy(out, prod.w, sizeof(u64) * ORC_LIMBS);
 }
+
+/* ------------------------------------------------------------------------
+ * Fingerprint-pool Q iteration (experimental/cc20_first_kind_immune_v16.cu)
+ *   p_0 = Q * D_V * 2^E - 1,  p_j = 2^(E+j) * Q * D_V - 1.
+ * ------------------------------------------------------------------------ */
+static u32 orc_inv_mod(u32 a, u32 q) {
+    long long t = 0, nt = 1, r = q, nr = a % q;
+    while (nr) {
+        long long f = r / nr, x;
+        x = t - f * nt; t = nt; nt = x;
+        x = r - f * nr; r = nr; nr = x;
+    }
+    return (u32)(t < 0 ? t + q : t);
+}
+
+static u32 orc_pow2_mod(int e, u32 q) {
+    u64 r = 1 % q;
+    for (int i = 0; i < e; i++) r = (r * 2) % q;
+    return (u32)r;
+}
+
+/* Forbidden residues of Q mod q (v16:1244-1266): inv(D mod q) * inv(2^(E+j))
+ * for j < depth, deduplicated, in order of first appearance.  Returns the
+ * count, 0 when q divides D (immune: the prime sieves nothing). */
+int orc_qiter_forbidden(u32 q, u64 d_lo, u64 d_hi, int E, int depth, u32* out) {
+    u128 D = ((u128)d_hi << 64) | d_lo;
+    u32 dm = (u32)(D % q);
+    if (dm == 0) return 0;
+    u32 inv_d = orc_inv_mod(dm, q);
+    int n = 0;
+    for (int j = 0; j < depth; j++) {
+        u32 r = (u32)((u64)inv_d * orc_inv_mod(orc_pow2_mod(E + j, q), q) % q);
+        int dup = 0;
+        for (int k = 0; k < n; k++) if (out[k] == r) { dup = 1; break; }
+        if (!dup) out[n++] = r;
+    }
+    return n;
+}
+
+/* Survivors of one segment Q = q_base + off, off < n_q, in increasing off
+ * (the per-Q probe of v16_q_iter_kernel, v16:2104-2134, every prime whose
+ * mask is non-empty).  Residues are advanced by one per Q.  Returns the
+ * survivor count; offsets beyond cap are counted, not written. */
+u64 orc_qiter_filter_seg(u64 qb_lo, u64 qb_hi, u32 n_q, u64 d_lo, u64 d_hi, int E, int depth,
+                         const u32* primes, int n_primes, u32* out, u64 cap) {
+    u128 qb = ((u128)qb_hi << 64) | qb_lo;
+    unsigned char** bad = calloc((size_t)n_primes, sizeof(unsigned char*));
+    u32* res = calloc((size_t)n_primes, sizeof(u32));
+    u32* fb = malloc(sizeof(u32) * (size_t)(depth > 0 ? depth : 1));
+    int* act = malloc(sizeof(int) * (size_t)(n_primes > 0 ? n_primes : 1));
+    int n_act = 0;
+    for (int i = 0; i < n_primes; i++) {
+        int n = orc_qiter_forbidden(primes[i], d_lo, d_hi, E, depth, fb);
+        if (n == 0) continue;
+        bad[i] = calloc(primes[i], 1);
+        for (int k = 0; k < n; k++) bad[i][fb[k]] = 1;
+        res[i] = (u32)(qb % primes[i]);
+        act[n_act++] = i;
+    }
+    u64 cnt = 0;
+    for (u64 off = 0; off < n_q; off++) {
+        int ok = 1;
+        for (int a = 0; a < n_act; a++) {
+            int i = act[a];
+            if (bad[i][res[i]]) { ok = 0; break; }
+        }
+        if (ok) {
+            if (cnt < cap) out[cnt] = (u32)off;
+            cnt++;
+        }
+        for (int a = 0; a < n_act; a++) {
+            int i = act[a];
+            if (++res[i] == primes[i]) res[i] = 0;
+        }
+    }
+    for (int i = 0; i < n_primes; i++) free(bad[i]);
+    free(bad); free(res); free(fb); free(act);
+    return cnt;
+}
+
+/* Prove one q-iteration survivor (the q-iter path of cpu_prove_worker,
+ * v16:2540-2722): p_0 from (Q, D_V, E); with reverse != 0 chain position
+ * target - 1 must be prime first (v16:2658-2673); p_0 prime (counted in
+ * *is_prime_out); root check on (p_0 - 1)/2 (v16:2693-2711; the birth
+ * certificate there only skips a test whose answer is already known);
+ * mode 0 drops non-roots, mode 1 walks back to the true root; forward walk.
+ * Returns the chain length or -1 when there is no record. */
+int orc_qiter_prove(u64 q_lo, u64 q_hi, u64 d_lo, u64 d_hi, int E, int target, int reverse, int mode,
+                    int primality, const u64* wit, int n_wit, u64* root_out, int* flags,
+                    int* is_prime_out) {
+    orc_pred pr = {primality, wit, n_wit};
+    big Q, D, n, two;
+    memset(&Q, 0, sizeof(Q)); memset(&D, 0, sizeof(D));
+    Q.w[0] = q_lo; Q.w[1] = q_hi;
+    D.w[0] = d_lo; D.w[1] = d_hi;
+    big_set_u64(&n, 0);
+    for (int i = big_bits(&D) - 1; i >= 0; i--) {          /* n = Q * D, shift-add */
+        big_shl1(&n);
+        if (big_bit(&D, i)) big_add(&n, &n, &Q);
+    }
+    for (int i = 0; i < E; i++) big_shl1(&n);
+    big_sub_u64(&n, &n, 1);
+    *flags = 0;
+    *is_prime_out = 0;
+    if (reverse && target > 1) {
+        big top = n;
+        for (int k = 0; k < target - 1; k++) { big_shl1(&top); big_add_u64(&top, &top, 1); }
+        if (!is_prime_p(&top, &pr)) return -1;
+    }
+    if (!is_prime_p(&n, &pr)) return -1;
+    *is_prime_out = 1;
+    big pred, root = n;
+    big_set_u64(&two, 2);
+    big_sub_u64(&pred, &n, 1);
+    big_shr1(&pred);
+    int is_root = 1;
+    if (big_cmp(&pred, &two) >= 0 && is_prime_p(&pred, &pr)) {
+        is_root = 0;
+        if (mode == 0) return -1;
+        root = pred;
+        for (int back = 0; back < ORC_MAX_CHAIN; back++) {
+            big_sub_u64(&pred, &root, 1);
+            big_shr1(&pred);
+            if (big_cmp(&pred, &two) < 0) break;
+            if (!is_prime_p(&pred, &pr)) break;
+            root = pred;
+        }
+    }
+    int len = walk_forward(&root, &pr);
+    memcpy(root_out, root.w, sizeof(u64) * ORC_LIMBS);
+    *flags = is_root ? 1 : 0;
+    return len;
+}

@@ -66,6 +66,10 @@ void __gmpz_addmul_ui(mpz_ptr, mpz_srcptr, unsigned long);
 void __gmpz_sub(mpz_ptr, mpz_srcptr, mpz_srcptr);
 void __gmpz_sub_ui(mpz_ptr, mpz_srcptr, unsigned long);
 void __gmpz_mul_ui(mpz_ptr, mpz_srcptr, unsigned long);
+void __gmpz_mul(mpz_ptr, mpz_srcptr, mpz_srcptr);
+size_t __gmpz_out_str(FILE*, int, mpz_srcptr);
+int __gmpz_divisible_p(mpz_srcptr, mpz_srcptr);
+int __gmp_fprintf(FILE*, const char*, ...);
 void __gmpz_mul_2exp(mpz_ptr, mpz_srcptr, mp_bitcnt_t);
 size_t __gmpz_sizeinbase(mpz_srcptr, int);
 void __gmpz_ui_pow_ui(mpz_ptr, unsigned long, unsigned long);
@@ -110,6 +114,10 @@ int __gmp_printf(const char*, ...);
 #define mpz_sub __gmpz_sub
 #define mpz_sub_ui __gmpz_sub_ui
 #define mpz_mul_ui __gmpz_mul_ui
+#define mpz_mul __gmpz_mul
+#define mpz_out_str __gmpz_out_str
+#define mpz_divisible_p __gmpz_divisible_p
+#define gmp_fprintf __gmp_fprintf
 #define mpz_mul_2exp __gmpz_mul_2exp
 #define mpz_sizeinbase __gmpz_sizeinbase
 #define mpz_ui_pow_ui __gmpz_ui_pow_ui

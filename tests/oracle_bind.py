@@ -65,6 +65,13 @@ def _load_oracle():
                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.orc_reconstruct.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32,
                                     C.c_uint32, _u64p]
+    lib.orc_qiter_forbidden.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, C.c_int, C.c_int, _u32p]
+    lib.orc_qiter_filter_seg.restype = C.c_uint64
+    lib.orc_qiter_filter_seg.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64,
+                                         C.c_int, C.c_int, _u32p, C.c_int, _u32p, C.c_uint64]
+    lib.orc_qiter_prove.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, _u64p, C.c_int, _u64p,
+                                    C.POINTER(C.c_int), C.POINTER(C.c_int)]
     return lib
 
 
@@ -295,4 +302,55 @@ def _bind13(lib):
     lib.ref13_prove_cpu.argtypes = [_u32p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int,
                                     C.c_int, C.c_char_p, C.POINTER(C.c_ulonglong),
                                     C.POINTER(C.c_ulonglong)]
+    return lib
+
+
+# ---------------------------------------------------------------------------
+# fingerprint-pool Q iteration (v16)
+# ---------------------------------------------------------------------------
+M64 = 2**64 - 1
+
+
+def qiter_forbidden(q, D, E, depth):
+    """Forbidden residues of Q mod q, in first-appearance order ([] when q | D)."""
+    out = np.zeros(max(depth, 1), dtype=np.uint32)
+    n = oracle().orc_qiter_forbidden(q, D & M64, D >> 64, E, depth, out)
+    return [int(x) for x in out[:n]]
+
+
+def qiter_filter_seg(q_base, n_q, D, E, depth, primes, cap=1 << 22):
+    """Survivor offsets of one segment, increasing."""
+    pr = np.asarray(primes, dtype=np.uint32)
+    out = np.zeros(max(cap, 1), dtype=np.uint32)
+    n = oracle().orc_qiter_filter_seg(q_base & M64, q_base >> 64, n_q, D & M64, D >> 64, E, depth,
+                                      pr, len(pr), out, cap)
+    return [int(x) for x in out[: min(n, cap)]]
+
+
+def qiter_prove(Q, D, E, target, reverse=True, mode=0, primality=PRIME_BPSW, witnesses=V13_WITNESSES):
+    """(chain_len, root, is_root) or None, and whether p_0 tested prime."""
+    wit = np.asarray(witnesses, dtype=np.uint64)
+    root = np.zeros(4, dtype=np.uint64)
+    fl, isp = C.c_int(0), C.c_int(0)
+    L = oracle().orc_qiter_prove(Q & M64, Q >> 64, D & M64, D >> 64, E, target, 1 if reverse else 0, mode,
+                                 primality, wit, len(wit), root, C.byref(fl), C.byref(isp))
+    if L < 0:
+        return None, bool(isp.value)
+    return (L, words_to_int(root), bool(fl.value & 1)), bool(isp.value)
+
+
+def ref16():
+    """The reference v16 engine harness (its forbidden residues and its
+    q-iteration kernel), or None."""
+    path = os.path.join(REF_DIR, "libref16.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    lib.ref16_forbidden.argtypes = [C.c_uint, C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_int, _u32p, C.c_int]
+    lib.ref16_qiter_filter.restype = C.c_uint
+    lib.ref16_qiter_filter.argtypes = [_u32p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_int,
+                                       C.c_ulonglong, C.c_ulonglong, C.c_uint, _u32p, C.c_uint]
+    lib.ref16_qiter_time.restype = C.c_float
+    lib.ref16_qiter_time.argtypes = [_u32p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_int,
+                                     C.c_ulonglong, C.c_ulonglong, C.c_uint, C.c_int, C.POINTER(C.c_uint)]
     return lib
