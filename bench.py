@@ -124,6 +124,44 @@ def v33_sample(bits, target, seconds_goal=15.0):
             "rate": wc / max(secs, 1e-9)}
 
 
+def reference_qiter(segs_per_step=32):
+    """The reference's own v16_q_iter_kernel (through oracle/_ref/libref16.so,
+    launched as its dispatch loop launches it) on the first 32 chunks of the
+    q-iteration section's first timed step; its sieve on the GPU is 7..503
+    (the 509..1009 primes run on its CPU prove workers)."""
+    import ctypes as C
+    import importlib
+    import numpy as np
+    path = os.path.join(ROOT, "oracle", "_ref", "libref16.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libref16.so not built"}
+    lib = C.CDLL(path)
+    u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+    lib.ref16_qiter_time.restype = C.c_float
+    lib.ref16_qiter_time.argtypes = [u32p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_int,
+                                     C.c_ulonglong, C.c_ulonglong, C.c_uint, C.c_int, C.POINTER(C.c_uint)]
+    ccs = importlib.import_module("cunningham-chain-search_b200")
+
+    class _Plan(ccs.QIter):                   # windows and chunk draws only, no device state
+        def __init__(self, pool):
+            self.dv, self.exp_start = [p[1] for p in pool], 0
+
+    pool = ccs.synthetic_pool(QITER_CFG["pool"], SEED + 61)
+    segs = qiter_plan(ccs, _Plan(pool), 2, 256)[1][:segs_per_step]
+    primes = np.asarray(ccs.qiter_sieve_primes(ext=False), dtype=np.uint32)
+    ms = 0.0
+    n = 0
+    reps = 4
+    for qb, nq, v in segs:
+        D = pool[v][1]
+        c = C.c_uint(0)
+        ms += lib.ref16_qiter_time(primes, len(primes), D & (2**64 - 1), D >> 64, 0, QITER_CFG["depth"],
+                                   qb & (2**64 - 1), qb >> 64, nq, reps, C.byref(c))
+        n += reps * nq
+    return {"qv_per_s_filter": n / (ms * 1e-3), "ms": ms, "chunks": len(segs), "reps": reps,
+            "sieve": "7..503 on the GPU (its kernel's list)", "unit": "(Q, variant) pairs/s"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -147,6 +185,11 @@ def run_reference(args):
                              "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": "candidates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if not args.headline_only:
+        try:
+            line["qiter_reference_kernel"] = reference_qiter()
+        except Exception as ex:
+            line["qiter_reference_kernel"] = {"error": repr(ex)}
     print(json.dumps(line))
     return 0
 
@@ -314,6 +357,64 @@ def section_reference_runs(ccs, torch, dev, local, tiles=1 << 22, steps=4):
                      "candidates_per_tile": info["candidates_per_tile"]}
         eng.close()
     return out
+
+
+QITER_CFG = dict(target=21, depth=21, bits_min=90, bits_max=107, chunk=1 << 24, pool=4248)
+
+
+def qiter_plan(ccs, qi, steps, segs_per_step):
+    return [qi.random_segments(segs_per_step, QITER_CFG["chunk"], QITER_CFG["bits_min"],
+                               QITER_CFG["bits_max"], seed=SEED + 71 + i, start_variant=i * segs_per_step)
+            for i in range(steps)]
+
+
+def section_qiter(ccs, torch, dev, local, steps=8, segs_per_step=256):
+    """Fingerprint-pool Q iteration as the reference's v16 production run
+    (--immune-prime 5 --target 21 --depth 21 --sieve-max 503 --bits-min 90
+    --bits-max 107 --q-order random, extended sieve 509..1009 on): a seeded
+    4248-variant synthetic pool, 256 random 2^24-Q chunks per step
+    round-robin over the variants, filter then prove, device-timed on one
+    stream; e2e = QIter.run on host segment lists (packing, filter, prove
+    overlapped with the next filter, HIT lines), timed on the host."""
+    pool = ccs.synthetic_pool(QITER_CFG["pool"], SEED + 61)
+    qi = ccs.QIter(pool, target=QITER_CFG["target"], depth=QITER_CFG["depth"], device=local)
+    plan = [qi.pack(p) for p in qiter_plan(ccs, qi, steps + 1, segs_per_step)]
+    stream = torch.cuda.Stream(device=dev)
+    surv = torch.empty((1 << 22, 4), dtype=torch.int32, device=dev)
+    chains = torch.empty((1 << 16, 12), dtype=torch.int32, device=dev)
+    f_ms = p_ms = 0.0
+    n_s = n_c = n_p = 0
+    for i, segs in enumerate(plan):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        s_ = qi.filter(segs, out=surv, stream=stream)
+        ev[1].record(stream)
+        c_, p_ = qi.prove(segs, s_, out=chains, stream=stream)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        if i == 0:
+            continue                                       # warm-up step
+        f_ms += ev[0].elapsed_time(ev[1])
+        p_ms += ev[1].elapsed_time(ev[2])
+        n_s += s_.shape[0]
+        n_c += c_.shape[0]
+        n_p += p_
+    qv = steps * segs_per_step * QITER_CFG["chunk"]
+    raw = qiter_plan(ccs, qi, steps + 1, segs_per_step)
+    qi.run(raw[:1], min_report_len=10)                     # warm-up: buffers, prove thread
+    torch.cuda.synchronize()
+    t0 = time.time()
+    tot, hits = qi.run(raw[1:], min_report_len=10)
+    e2e_s = time.time() - t0
+    assert tot["survivors"] == n_s and tot["chains"] == n_c
+    qi.close()
+    return {"workload": f"{QITER_CFG['pool']}-variant seeded pool, target = depth = 21, sieve 7..1009, "
+                        f"bits 90..107, {steps} steps x {segs_per_step} chunks of 2^24 Q",
+            "qv_per_s_filter": qv / (f_ms * 1e-3), "qv_per_s_filter_prove": qv / ((f_ms + p_ms) * 1e-3),
+            "qv_per_s_e2e": qv / e2e_s, "filter_ms": f_ms, "prove_ms": p_ms, "survivors": n_s,
+            "chains": n_c, "primes": n_p, "hit_lines_len10": len(hits),
+            "unit": "(Q, variant) pairs/s, the reference's G(Q,V)/s x 1e9"}
 
 
 def section_batched(ccs, engines, n_ranges=4096):
@@ -565,6 +666,10 @@ def run_ours(args):
             extra["reference_runs"] = section_reference_runs(ccs, torch, dev, local)
         except Exception as ex:
             extra["reference_runs"] = {"error": repr(ex)}
+        try:
+            extra["qiter"] = section_qiter(ccs, torch, dev, local)
+        except Exception as ex:
+            extra["qiter"] = {"error": repr(ex)}
         depth_engines = [ccs.Engine(device=local, **ccs.config_depth_profile(d)) for d in range(14, 20)]
         if not args.no_autotune:
             try:
@@ -635,10 +740,21 @@ def main():
                     help="skip the prove-batch, batched and served sections")
     ap.add_argument("--batch-ranges", type=int, default=4096)
     ap.add_argument("--served-requests", type=int, default=2048)
+    ap.add_argument("--only", choices=["qiter"], default=None,
+                    help="run one section alone and print its JSON (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warmup raised to 3")
         args.warmup = 3
+    if args.only == "qiter":
+        import importlib
+        import torch
+        ccs = importlib.import_module("cunningham-chain-search_b200")
+        if args.impl == "reference":
+            print(json.dumps(reference_qiter()))
+        else:
+            print(json.dumps(section_qiter(ccs, torch, torch.device("cuda:0"), 0, steps=args.steps)))
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

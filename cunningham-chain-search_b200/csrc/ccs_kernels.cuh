@@ -64,6 +64,15 @@ struct ProveRange {
     uint32_t* prime_count;   // per-range prime counter
 };
 
+// q-iteration survivors {offset, seg, variant} in a staged prove:
+// p_0 = (q_base[seg] + offset) * D_V * 2^E - 1
+struct QiterProve {
+    const uint32_t* seg;                 // [n_segs][6]: q_base limbs, n_q, variant (null: lattice survivors)
+    const uint32_t* dv;                  // [n_variants][4]
+    uint32_t exp_start;
+    uint32_t n_segs;                     // survivors naming another segment are skipped
+};
+
 // Prove launch: survivors of one or many ranges in one flat array.
 struct ProveArgs {
     const ProveRange* ranges;
@@ -75,6 +84,7 @@ struct ProveArgs {
     uint32_t* chains;              // 12 x u32 records
     uint32_t* chain_count;         // global counter
     uint32_t chain_cap;
+    QiterProve q = {nullptr, nullptr, 0, 0};   // q-iteration survivors (seg null: lattice)
 };
 
 // Prover constants per profile (constant memory).
@@ -131,15 +141,6 @@ struct WalkArgs {
 cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
                              WalkItem* out, cudaStream_t st);
 cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, cudaStream_t st);
-
-// q-iteration survivors {offset, seg, variant} in a staged prove:
-// p_0 = (q_base[seg] + offset) * D_V * 2^E - 1
-struct QiterProve {
-    const uint32_t* seg;                 // [n_segs][6]: q_base limbs, n_q, variant (null: lattice survivors)
-    const uint32_t* dv;                  // [n_variants][4]
-    uint32_t exp_start;
-    uint32_t n_segs;                     // survivors naming another segment are skipped
-};
 
 // staged prove of one range's survivors (prove.cu)
 struct StagedProve {

@@ -971,8 +971,34 @@ ccs_status engine_prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
     ProveRange* h = (ProveRange*)((char*)E->h_stage + 4096);
     *h = pr;
     h->profile = (uint32_t)E->slot;
+    h->chain_count = nullptr;
+    h->prime_count = E->d_counters.p + 3;
     CU(cudaMemcpyAsync(E->d_prange.p, h, sizeof(ProveRange), cudaMemcpyHostToDevice, st));
-    return prove_staged(E, surv_dev, n_surv, E->d_prange.p, q, out_dev, cap, n_out, primes_out, st);
+    if (n_surv >= kStagedProveMin)
+        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, q, out_dev, cap, n_out, primes_out, st);
+    // few survivors: one thread each, one launch
+    CU(cudaMemsetAsync(E->d_counters.p + 2, 0, 8, st));
+    ProveArgs a;
+    a.ranges = E->d_prange.p;
+    a.surv = (const uint32_t*)surv_dev;
+    a.n_surv_dev = nullptr;
+    a.n_surv = (uint32_t)n_surv;
+    a.surv_cap = (uint32_t)n_surv;
+    a.range_from_pad = 0;
+    a.chains = (uint32_t*)out_dev;
+    a.chain_count = E->d_counters.p + 2;
+    a.chain_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
+    if (q) a.q = *q;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, (n_surv + 127) / 128);
+    CU(launch_prove(a, grid, st));
+    E->launches += 1;
+    uint32_t* hc = (uint32_t*)((char*)E->h_stage + 8192);
+    CU(cudaMemcpyAsync(hc, E->d_counters.p + 2, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    *n_out = hc[0];
+    if (primes_out) *primes_out = hc[1];
+    if (hc[0] > cap) return fail(CCS_OVERFLOW, "chain capacity exceeded");
+    return CCS_OK;
 }
 
 cudaStream_t engine_stream(ccs_engine* E) { return E->own_stream; }

@@ -652,6 +652,56 @@ __device__ __forceinline__ Big survivor_number(const uint4 s, const ProveRange& 
     return nb;
 }
 
+// p_0 = (q_base + offset) * D_V * 2^E - 1 for a q-iteration survivor
+// {offset, seg, variant} (v16:2576-2620); the caller keeps p_0 < 2^160
+__device__ __forceinline__ Big qiter_number(const uint4 s, const QiterProve& q) {
+    const uint32_t* sg = q.seg + (size_t)s.y * 6;
+    uint32_t Q[5];
+    uint64_t c = s.x;
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        const uint64_t v = (uint64_t)sg[w] + c;
+        Q[w] = (uint32_t)v;
+        c = v >> 32;
+    }
+    Q[4] = (uint32_t)c;
+    const uint32_t* d = q.dv + (size_t)sg[5] * 4;               // the segment's variant
+    uint32_t prod[kMaxLimbs];
+#pragma unroll
+    for (int w = 0; w < kMaxLimbs; w++) prod[w] = 0;
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        uint64_t carry = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (i + j < kMaxLimbs) {
+                const uint64_t v = (uint64_t)Q[i] * d[j] + prod[i + j] + carry;
+                prod[i + j] = (uint32_t)v;
+                carry = v >> 32;
+            }
+        }
+        if (i + 4 < kMaxLimbs) prod[i + 4] = (uint32_t)carry;
+    }
+    Big b;
+    const uint32_t E = q.exp_start;
+    const uint32_t ws = E >> 5, bs = E & 31;
+#pragma unroll
+    for (int w = kMaxLimbs - 1; w >= 0; w--) {
+        const int src = w - (int)ws;
+        const uint32_t lo = src >= 0 ? prod[src] : 0u;
+        const uint32_t lo2 = src >= 1 ? prod[src - 1] : 0u;
+        b.w[w] = bs ? (lo << bs) | (lo2 >> (32 - bs)) : lo;
+    }
+    // - 1 (p + 1 >= 2 always: Q >= 1, D_V >= 1)
+#pragma unroll
+    for (int w = 0; w < kMaxLimbs; w++) {
+        const uint32_t old = b.w[w];
+        b.w[w] = old - 1u;
+        if (old != 0u) break;
+    }
+    return b;
+}
+
 __global__ void __launch_bounds__(128)
 prove_kernel(ProveArgs a) {
     uint32_t n = a.n_surv_dev ? *a.n_surv_dev : a.n_surv;
@@ -660,9 +710,13 @@ prove_kernel(ProveArgs a) {
         const uint4 s = reinterpret_cast<const uint4*>(a.surv)[i];
         const ProveRange& R = a.ranges[a.range_from_pad ? s.w : 0u];
         const ProveConst& pc = c_prove[R.profile];
-        // n = ((T0 + tile_idx) * WP + k) * M + base   (v13:1479-1492)
+        // n = ((T0 + tile_idx) * WP + k) * M + base   (v13:1479-1492), or a
+        // q-iteration p_0 (no bit gate, v16:2620)
         Big nb;
-        {
+        if (a.q.seg) {
+            if (s.y >= a.q.n_segs) continue;
+            nb = qiter_number(s, a.q);
+        } else {
             uint64_t c = s.z;
 #pragma unroll
             for (int w = 0; w < 4; w++) {
@@ -687,7 +741,7 @@ prove_kernel(ProveArgs a) {
                 c = v >> 32;
             }
         }
-        if (big_bits(nb) != (int)R.bits) continue;                     // v13:1495, 1828
+        if (!a.q.seg && big_bits(nb) != (int)R.bits) continue;         // v13:1495, 1828
         const int ntd = (pc.prove_mode == CCS_PROVE_ROOTS) ? 132 : 62;  // v13:1499 / 1832
         bool comp = false;
         for (int t = 0; t < ntd && !comp; t++) comp = big_mod_small(nb, c_screen[t]) == 0;
@@ -968,56 +1022,6 @@ __device__ __forceinline__ void item_put(WalkItem* out, uint32_t pos, const Big&
     it.idx = idx;
     it.len = len;
     out[pos] = it;
-}
-
-// p_0 = (q_base + offset) * D_V * 2^E - 1 for a q-iteration survivor
-// {offset, seg, variant} (v16:2576-2620); the caller keeps p_0 < 2^160
-__device__ __forceinline__ Big qiter_number(const uint4 s, const QiterProve& q) {
-    const uint32_t* sg = q.seg + (size_t)s.y * 6;
-    uint32_t Q[5];
-    uint64_t c = s.x;
-#pragma unroll
-    for (int w = 0; w < 4; w++) {
-        const uint64_t v = (uint64_t)sg[w] + c;
-        Q[w] = (uint32_t)v;
-        c = v >> 32;
-    }
-    Q[4] = (uint32_t)c;
-    const uint32_t* d = q.dv + (size_t)sg[5] * 4;               // the segment's variant
-    uint32_t prod[kMaxLimbs];
-#pragma unroll
-    for (int w = 0; w < kMaxLimbs; w++) prod[w] = 0;
-#pragma unroll
-    for (int i = 0; i < 5; i++) {
-        uint64_t carry = 0;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if (i + j < kMaxLimbs) {
-                const uint64_t v = (uint64_t)Q[i] * d[j] + prod[i + j] + carry;
-                prod[i + j] = (uint32_t)v;
-                carry = v >> 32;
-            }
-        }
-        if (i + 4 < kMaxLimbs) prod[i + 4] = (uint32_t)carry;
-    }
-    Big b;
-    const uint32_t E = q.exp_start;
-    const uint32_t ws = E >> 5, bs = E & 31;
-#pragma unroll
-    for (int w = kMaxLimbs - 1; w >= 0; w--) {
-        const int src = w - (int)ws;
-        const uint32_t lo = src >= 0 ? prod[src] : 0u;
-        const uint32_t lo2 = src >= 1 ? prod[src - 1] : 0u;
-        b.w[w] = bs ? (lo << bs) | (lo2 >> (32 - bs)) : lo;
-    }
-    // - 1 (p + 1 >= 2 always: Q >= 1, D_V >= 1)
-#pragma unroll
-    for (int w = 0; w < kMaxLimbs; w++) {
-        const uint32_t old = b.w[w];
-        b.w[w] = old - 1u;
-        if (old != 0u) break;
-    }
-    return b;
 }
 
 __global__ void __launch_bounds__(256)

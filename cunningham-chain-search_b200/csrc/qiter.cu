@@ -198,11 +198,17 @@ struct ccs_qiter {
     DevBuf<uint4> d_vhdr;
     DevBuf<uint2> d_act;
     DevBuf<uint32_t> d_pat, d_primes, d_magic, d_dv, d_count;
-    DevBuf<ccs_qseg> d_segs;
-    DevBuf<uint64_t> d_prefix;
-    ccs_qseg* h_segs = nullptr;               // pinned
-    uint64_t* h_prefix = nullptr;
-    uint32_t h_cap = 0;
+    // segment staging, one set for filter calls and one for prove calls, so
+    // that a filter and a prove may run at the same time from two host
+    // threads (each on its own stream)
+    struct Staging {
+        DevBuf<ccs_qseg> d_segs;
+        DevBuf<uint64_t> d_prefix;
+        ccs_qseg* h_segs = nullptr;           // pinned
+        uint64_t* h_prefix = nullptr;
+        uint32_t h_cap = 0;
+    } fst, pst;
+    cudaStream_t fstream = nullptr;           // filter calls without a stream
     uint32_t* h_count = nullptr;
 };
 
@@ -247,32 +253,32 @@ int bits128(unsigned __int128 x) {
     return b;
 }
 
-ccs_status stage_segs(ccs_qiter* Q, const ccs_qseg* segs, uint32_t n_segs, cudaStream_t st) {
-    if (n_segs > Q->h_cap) {
+ccs_status stage_segs(ccs_qiter::Staging& S, const ccs_qseg* segs, uint32_t n_segs, cudaStream_t st) {
+    if (n_segs > S.h_cap) {
         uint32_t c = 1024;
         while (c < n_segs) c <<= 1;
-        if (Q->h_segs) cudaFreeHost(Q->h_segs);
-        if (Q->h_prefix) cudaFreeHost(Q->h_prefix);
-        Q->h_segs = nullptr; Q->h_prefix = nullptr; Q->h_cap = 0;
-        if (cudaMallocHost(&Q->h_segs, sizeof(ccs_qseg) * c) != cudaSuccess ||
-            cudaMallocHost(&Q->h_prefix, sizeof(uint64_t) * (c + 1)) != cudaSuccess)
+        if (S.h_segs) cudaFreeHost(S.h_segs);
+        if (S.h_prefix) cudaFreeHost(S.h_prefix);
+        S.h_segs = nullptr; S.h_prefix = nullptr; S.h_cap = 0;
+        if (cudaMallocHost(&S.h_segs, sizeof(ccs_qseg) * c) != cudaSuccess ||
+            cudaMallocHost(&S.h_prefix, sizeof(uint64_t) * (c + 1)) != cudaSuccess)
             return fail(CCS_ERR_NOMEM, "pinned allocation failed");
-        CU(Q->d_segs.alloc(c));
-        CU(Q->d_prefix.alloc(c + 1));
-        Q->h_cap = c;
+        CU(S.d_segs.alloc(c));
+        CU(S.d_prefix.alloc(c + 1));
+        S.h_cap = c;
     }
     cudaStreamSynchronize(st);                // staging buffers may still feed a copy
-    memcpy(Q->h_segs, segs, sizeof(ccs_qseg) * n_segs);
+    memcpy(S.h_segs, segs, sizeof(ccs_qseg) * n_segs);
     uint64_t acc = 0;
-    Q->h_prefix[0] = 0;
+    S.h_prefix[0] = 0;
     for (uint32_t s = 0; s < n_segs; s++) {
         const uint64_t words = ((uint64_t)segs[s].n_q + 63) >> 6;
         acc += (words + kQUnitWords - 1) / kQUnitWords;
-        Q->h_prefix[s + 1] = acc;
+        S.h_prefix[s + 1] = acc;
     }
     if (n_segs) {
-        CU(cudaMemcpyAsync(Q->d_segs.p, Q->h_segs, sizeof(ccs_qseg) * n_segs, cudaMemcpyHostToDevice, st));
-        CU(cudaMemcpyAsync(Q->d_prefix.p, Q->h_prefix, sizeof(uint64_t) * (n_segs + 1),
+        CU(cudaMemcpyAsync(S.d_segs.p, S.h_segs, sizeof(ccs_qseg) * n_segs, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(S.d_prefix.p, S.h_prefix, sizeof(uint64_t) * (n_segs + 1),
                            cudaMemcpyHostToDevice, st));
     }
     return CCS_OK;
@@ -342,6 +348,23 @@ ccs_status ccs_qiter_create(const ccs_qiter_params* p, int device, ccs_qiter** o
         }
         const uint32_t n_act = (uint32_t)Q->act.size() - act0;
         const uint32_t words = (uint32_t)Q->pat.size() - pat0;
+        // the survivor set does not depend on the order of the primes: test
+        // the ones that kill the largest share of Q first (fewest survivors
+        // per residue), so that words die after fewer primes
+        {
+            std::vector<std::pair<double, uint2>> ord;
+            for (uint32_t k = 0; k < n_act; k++) {
+                const uint2 e = Q->act[act0 + k];
+                const uint32_t q = Q->primes[e.x];
+                const uint32_t* w = Q->pat.data() + pat0 + e.y;
+                uint32_t c = 0;
+                for (uint32_t b = 0; b < q; b++) c += (w[b >> 5] >> (b & 31)) & 1u;
+                ord.push_back({(double)(q - c) / q, e});
+            }
+            std::stable_sort(ord.begin(), ord.end(),
+                             [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (uint32_t k = 0; k < n_act; k++) Q->act[act0 + k] = ord[k].second;
+        }
         if (words > kQSlabMax) { delete Q; return fail(CCS_ERR_INVALID, "sieve primes too large for one slab"); }
         Q->vhdr.push_back(make_uint4(act0, n_act, pat0, words));
         Q->act_max = std::max(Q->act_max, n_act);
@@ -368,6 +391,7 @@ ccs_status ccs_qiter_create(const ccs_qiter_params* p, int device, ccs_qiter** o
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, device));
     Q->sms = prop.multiProcessorCount;
+    CU(cudaStreamCreateWithFlags(&Q->fstream, cudaStreamNonBlocking));
     if (Q->smem > 48 * 1024)
         CU(cudaFuncSetAttribute(qiter_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Q->smem));
     int bps = 0;
@@ -382,10 +406,15 @@ ccs_status ccs_qiter_destroy(ccs_qiter* Q) {
     cudaSetDevice(Q->device);
     if (Q->pe) ccs_destroy(Q->pe);
     Q->d_vhdr.free_(); Q->d_act.free_(); Q->d_pat.free_(); Q->d_primes.free_(); Q->d_magic.free_();
-    Q->d_dv.free_(); Q->d_count.free_(); Q->d_segs.free_(); Q->d_prefix.free_();
-    if (Q->h_segs) cudaFreeHost(Q->h_segs);
-    if (Q->h_prefix) cudaFreeHost(Q->h_prefix);
+    Q->d_dv.free_(); Q->d_count.free_();
+    for (ccs_qiter::Staging* S : {&Q->fst, &Q->pst}) {
+        S->d_segs.free_();
+        S->d_prefix.free_();
+        if (S->h_segs) cudaFreeHost(S->h_segs);
+        if (S->h_prefix) cudaFreeHost(S->h_prefix);
+    }
     if (Q->h_count) cudaFreeHost(Q->h_count);
+    if (Q->fstream) { cudaStreamSynchronize(Q->fstream); cudaStreamDestroy(Q->fstream); }
     delete Q;
     return CCS_OK;
 }
@@ -399,14 +428,14 @@ ccs_status ccs_qiter_filter(ccs_qiter* Q, const ccs_qseg* segs, uint32_t n_segs,
         if (s != CCS_OK) return s;
     }
     CU(cudaSetDevice(Q->device));
-    cudaStream_t st = stream ? (cudaStream_t)stream : engine_stream(Q->pe);
+    cudaStream_t st = stream ? (cudaStream_t)stream : Q->fstream;
     *n_out = 0;
     if (!n_segs) return CCS_OK;
     {
-        ccs_status s = stage_segs(Q, segs, n_segs, st);
+        ccs_status s = stage_segs(Q->fst, segs, n_segs, st);
         if (s != CCS_OK) return s;
     }
-    const uint64_t units = Q->h_prefix[n_segs];
+    const uint64_t units = Q->fst.h_prefix[n_segs];
     CU(cudaMemsetAsync(Q->d_count.p, 0, 4, st));
     if (units) {
         QSweepArgs a;
@@ -415,8 +444,8 @@ ccs_status ccs_qiter_filter(ccs_qiter* Q, const ccs_qseg* segs, uint32_t n_segs,
         a.pat = Q->d_pat.p;
         a.primes = Q->d_primes.p;
         a.magic = Q->d_magic.p;
-        a.segs = Q->d_segs.p;
-        a.unit_prefix = Q->d_prefix.p;
+        a.segs = Q->fst.d_segs.p;
+        a.unit_prefix = Q->fst.d_prefix.p;
         a.n_segs = n_segs;
         a.unit_words = kQUnitWords;
         a.act_max = Q->act_max;
@@ -460,14 +489,14 @@ ccs_status ccs_qiter_prove(ccs_qiter* Q, const ccs_qseg* segs, uint32_t n_segs,
     CU(cudaSetDevice(Q->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : engine_stream(Q->pe);
     {
-        ccs_status s = stage_segs(Q, segs, n_segs, st);
+        ccs_status s = stage_segs(Q->pst, segs, n_segs, st);
         if (s != CCS_OK) return s;
     }
     ProveRange pr;
     memset(&pr, 0, sizeof(pr));
     pr.target = Q->target;
     QiterProve qp;
-    qp.seg = reinterpret_cast<const uint32_t*>(Q->d_segs.p);
+    qp.seg = reinterpret_cast<const uint32_t*>(Q->pst.d_segs.p);
     qp.dv = Q->d_dv.p;
     qp.exp_start = Q->exp_start;
     qp.n_segs = n_segs;

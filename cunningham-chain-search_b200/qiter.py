@@ -105,6 +105,32 @@ def q_window(D, E, bits_min, bits_max):
     return qmin, qmax
 
 
+def synthetic_pool(n=4248, seed=1, bits_lo=12.0, bits_hi=37.0):
+    """n distinct seeded fingerprints shaped like the reference's empirical
+    pools: the floor 2*3*5 times a random subset of the palette primes
+    7..61, small exponents on 2, 3 and 5, D_V between 2^bits_lo and
+    2^bits_hi.  A stand-in for pool files, which are data, not code."""
+    import math
+    import random
+    r = random.Random(seed)
+    palette = [7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61]
+    seen, out = set(), []
+    while len(out) < n:
+        fac = {2: r.choice([1, 1, 1, 2, 3]), 3: r.choice([1, 1, 2, 3]), 5: r.choice([1, 1, 1, 2])}
+        for q in palette:
+            if r.random() < 0.3:
+                fac[q] = 2 if r.random() < 0.05 else 1
+        D = 1
+        for q, e in fac.items():
+            D *= q ** e
+        if not bits_lo <= math.log2(D) <= bits_hi or D in seen:
+            continue
+        seen.add(D)
+        spec = "*".join(f"{q}^{e}" if e > 1 else str(q) for q, e in sorted(fac.items()))
+        out.append((spec, D, fac))
+    return out
+
+
 def format_hit_line(seed_name, chain_len, Q, p0, fp=None, pool=None):
     s = f"HIT seed={seed_name} len={chain_len} "
     if fp is not None:
@@ -169,18 +195,29 @@ class QIter:
 
     # ---------------------------------------------------------------- segments
     @staticmethod
-    def _segs(segs):
-        from . import _QSeg
-        arr = (_QSeg * max(len(segs), 1))()
+    def pack(segs):
+        """Segments [(q_base, n_q, variant)] as the C ABI's ccs_qseg array
+        (a [n, 6] uint32 array); filter and prove take either form."""
+        if isinstance(segs, np.ndarray):
+            return segs
+        arr = np.zeros((max(len(segs), 1), 6), dtype=np.uint32)
         for i, (qb, n_q, v) in enumerate(segs):
             qb = int(qb)
             if qb < 0 or qb >= 1 << 128 or not 0 <= int(n_q) < 1 << 32:
                 raise ValueError("segment out of range")
-            for w in range(4):
-                arr[i].q_base[w] = (qb >> (32 * w)) & 0xFFFFFFFF
-            arr[i].n_q = int(n_q)
-            arr[i].variant = int(v)
+            arr[i] = (qb & 0xFFFFFFFF, (qb >> 32) & 0xFFFFFFFF, (qb >> 64) & 0xFFFFFFFF, qb >> 96,
+                      int(n_q), int(v))
         return arr
+
+    @staticmethod
+    def _segs(segs):
+        from . import _QSeg
+        arr = QIter.pack(segs)
+        return arr, arr.ctypes.data_as(C.POINTER(_QSeg))
+
+    @staticmethod
+    def _nsegs(segs):
+        return segs.shape[0] if isinstance(segs, np.ndarray) else len(segs)
 
     def windows(self, bits_min, bits_max):
         return [q_window(d, self.exp_start, bits_min, bits_max) for d in self.dv]
@@ -215,9 +252,9 @@ class QIter:
         if out is None:
             out = torch.empty((cap, 4), dtype=torch.int32, device=f"cuda:{self.device}")
         cap = out.shape[0]
-        arr = self._segs(segs)
+        keep, arr = self._segs(segs)
         n = _u64(0)
-        st = load_library().ccs_qiter_filter(self.h, arr, len(segs), out.data_ptr(), cap, C.byref(n),
+        st = load_library().ccs_qiter_filter(self.h, arr, self._nsegs(segs), out.data_ptr(), cap, C.byref(n),
                                              stream.cuda_stream if stream is not None else None)
         if st == OVERFLOW:
             raise CCSError(st, f"{n.value} survivors > cap {cap}")
@@ -233,17 +270,73 @@ class QIter:
         if out is None:
             out = torch.empty((cap, 12), dtype=torch.int32, device=f"cuda:{self.device}")
         cap = out.shape[0]
-        arr = self._segs(segs)
+        keep, arr = self._segs(segs)
         sv = survivors.contiguous()
         n = _u64(0)
         pr = _u64(0)
-        st = load_library().ccs_qiter_prove(self.h, arr, len(segs), sv.data_ptr() if sv.numel() else None,
+        st = load_library().ccs_qiter_prove(self.h, arr, self._nsegs(segs), sv.data_ptr() if sv.numel() else None,
                                             sv.shape[0], out.data_ptr(), cap, C.byref(n), C.byref(pr),
                                             stream.cuda_stream if stream is not None else None)
         if st == OVERFLOW:
             raise CCSError(st, f"{n.value} chains > cap {cap}")
         _check(st, "ccs_qiter_prove")
         return out[: n.value], pr.value
+
+    def run(self, plan, min_report_len=8, surv_cap=1 << 22, chain_cap=1 << 16, pool_primes=None):
+        """Filters and proves a list of steps (each a segment list), the
+        prove of step i overlapping the filter of step i + 1 (two host
+        threads, two streams, two survivor buffers), as the reference
+        overlaps its sieve launches with its CPU prove pool (v16:5700-5800).
+        Returns the totals and the sorted HIT lines."""
+        import queue
+        import threading
+        from . import _torch
+        torch = _torch()
+        dev = f"cuda:{self.device}"
+        bufs = [torch.empty((surv_cap, 4), dtype=torch.int32, device=dev) for _ in range(2)]
+        chains = torch.empty((chain_cap, 12), dtype=torch.int32, device=dev)
+        free = [threading.Semaphore(1), threading.Semaphore(1)]
+        work = queue.Queue(maxsize=1)
+        tot = {"steps": 0, "q": 0, "survivors": 0, "chains": 0, "primes": 0}
+        lines, err = [], []
+
+        def prover():
+            while True:
+                item = work.get()
+                if item is None:
+                    return
+                i, segs, surv = item
+                try:
+                    if not err:
+                        c, pr = self.prove(segs, surv, out=chains)
+                        tot["chains"] += c.shape[0]
+                        tot["primes"] += pr
+                        lines.extend(self.hit_lines(segs, c, min_report_len, pool_primes))
+                except Exception as ex:                   # reported to the caller below
+                    err.append(ex)
+                finally:
+                    free[i % 2].release()
+
+        th = threading.Thread(target=prover, daemon=True)
+        th.start()
+        try:
+            for i, segs in enumerate(plan):
+                packed = self.pack(segs)
+                free[i % 2].acquire()
+                if err:
+                    free[i % 2].release()
+                    break
+                s_ = self.filter(packed, out=bufs[i % 2])
+                tot["steps"] += 1
+                tot["q"] += int(packed[: self._nsegs(segs), 4].astype(np.int64).sum())
+                tot["survivors"] += s_.shape[0]
+                work.put((i, packed, s_))
+        finally:
+            work.put(None)
+            th.join()
+        if err:
+            raise err[0]
+        return tot, sorted(lines)
 
     def forbidden_counts(self, variant):
         from . import _check, load_library
@@ -263,8 +356,9 @@ class QIter:
             L = int(r[3])
             if L < min_report_len:
                 continue
-            qb, _, v = segs[int(r[1])]
-            Q = int(qb) + int(r[0])
+            sg = segs[int(r[1])]
+            qb = sum(int(sg[w]) << (32 * w) for w in range(4)) if isinstance(segs, np.ndarray) else int(sg[0])
+            Q = qb + int(r[0])
             p0 = sum(int(x) << (32 * i) for i, x in enumerate(r[4:10]))
             fp = [q for q in pool_primes if (p0 + 1) % q == 0] if pool_primes else None
             pool = [self.names[i] for i, d in enumerate(self.dv) if (p0 + 1) % d == 0]

@@ -440,7 +440,9 @@ typedef struct {
     uint32_t _pad;             /* written as 0 */
 } ccs_qsurvivor;
 
-/* Builds the per-variant forbidden-Q windows and uploads them. */
+/* Builds the per-variant forbidden-Q windows and uploads them.  One filter
+ * call and one prove call may run at the same time on one object (two host
+ * threads): they stage segments and run on separate streams. */
 ccs_status ccs_qiter_create(const ccs_qiter_params* params, int device, ccs_qiter** out);
 ccs_status ccs_qiter_destroy(ccs_qiter* qe);
 

@@ -132,6 +132,15 @@ def test_prove_matches_oracle(ccs, ob, reverse, mode):
     flags = chains.cpu().numpy()[:, 10]
     lens = chains.cpu().numpy()[:, 3]
     assert (((flags & 2) != 0) == (lens >= target)).all()
+    # below 256 survivors the one-thread-per-survivor kernel proves them:
+    # the same records for the same survivors
+    part = surv[:200]
+    keys = set((int(o), int(sg)) for o, sg in part.cpu().numpy()[:, :2].astype(np.int64))
+    c2, p2 = qi.prove(segs, part)
+    got2 = sorted((int(c[1]), int(c[0]), int(c[3]), sum(int(x & 0xFFFFFFFF) << (32 * i) for i, x in
+                                                         enumerate(c[4:10])), int(c[10]) & 1)
+                  for c in c2.cpu().numpy().astype(np.int64))
+    assert got2 == sorted(w for w in want if (w[1], w[0]) in keys)
     qi.close()
 
 
@@ -144,4 +153,26 @@ def test_prove_rejects_wide_segments(ccs):
         qi.prove([((1 << 128) - 1000, 10, len(SHAPES) - 1)], surv)   # p_0 above 2^160
     with pytest.raises(ValueError):
         qi.prove([(1 << 150, 10, 0)], surv)                  # Q beyond 128 bits
+    qi.close()
+
+
+def test_pipelined_run_equals_sequential(ccs):
+    """QIter.run (prove of step i beside the filter of step i + 1, two
+    threads and streams) gives the totals and HIT lines of plain
+    filter-then-prove calls, step by step."""
+    pool = _pool(ccs)
+    qi = ccs.QIter(pool, target=8, depth=8, primes=ccs.qiter_sieve_primes(sieve_max=131, ext=False))
+    plan = [qi.random_segments(16, 1 << 18, 64, 80, seed=s, start_variant=s) for s in range(6)]
+    tot, lines = qi.run(plan, min_report_len=4)
+    want_lines, n_s, n_c, n_p = [], 0, 0, 0
+    for segs in plan:
+        s_ = qi.filter(segs)
+        c_, p_ = qi.prove(segs, s_, cap=1 << 18)
+        n_s += s_.shape[0]
+        n_c += c_.shape[0]
+        n_p += p_
+        want_lines += qi.hit_lines(segs, c_, min_report_len=4)
+    assert (tot["steps"], tot["survivors"], tot["chains"], tot["primes"]) == (6, n_s, n_c, n_p)
+    assert tot["q"] == 6 * 16 * (1 << 18)
+    assert lines == sorted(want_lines) and len(lines) > 0 and n_s > 1000
     qi.close()
