@@ -14,8 +14,9 @@
 // after a few dozen primes is the common case.
 //
 // Work units are runs of unit_words words of one segment (one variant, one
-// run of Q); blocks take units in a grid-stride loop and restage the pattern
-// slab only when the variant changes.
+// run of Q); blocks take units from a global counter and restage the pattern
+// slab only when the variant changes; warps take 32-word blocks of a unit
+// from a shared counter.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,7 +46,7 @@ constexpr uint32_t kQPrimeMax = 8192;        // sieve primes below this
 constexpr uint32_t kQMaxPrimes = 1024;
 constexpr uint32_t kQSlabMax = 16384;        // pattern words per variant (64 KB of shared memory)
 constexpr uint32_t kQThreads = 256;
-constexpr uint32_t kQUnitWords = 4096;       // 262,144 Q per work unit
+constexpr uint32_t kQUnitWords = 8192;       // 524,288 Q per work unit
 constexpr uint32_t kQMaxSegs = 1u << 20;
 
 inline uint32_t q_words(uint32_t q) { return (q - 1) / 32 + 3; }
@@ -62,7 +63,7 @@ struct QSweepArgs {
     uint32_t unit_words;
     uint32_t act_max;                        // shared-memory entries reserved
     uint32_t* out;                           // ccs_qsurvivor records
-    uint32_t* count;
+    uint32_t* count;                         // [0] survivors, [1] next work unit
     uint32_t cap;
 };
 
@@ -71,34 +72,49 @@ __device__ __forceinline__ uint32_t qmod(uint32_t x, uint32_t q, uint32_t m) {
     return r >= q ? r - q : r;
 }
 
+// unit u -> segment, first word, word count (binary search on the unit prefix)
+__device__ __forceinline__ void qiter_unit(const QSweepArgs& a, uint64_t u, uint32_t* info) {
+    uint32_t lo = 0, hi = a.n_segs;                                  // last seg with prefix <= u
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.unit_prefix[mid] <= u) lo = mid; else hi = mid;
+    }
+    const ccs_qseg& sg = a.segs[lo];
+    const uint32_t words = (uint32_t)(((uint64_t)sg.n_q + 63) >> 6);
+    const uint32_t w0 = (uint32_t)(u - a.unit_prefix[lo]) * a.unit_words;
+    info[0] = lo;
+    info[1] = sg.variant;
+    info[2] = w0;
+    info[3] = min(a.unit_words, words - w0);
+}
+
 __global__ void __launch_bounds__(kQThreads)
 qiter_sweep_kernel(QSweepArgs a) {
     extern __shared__ __align__(16) uint32_t qsm[];
     uint4* s_act = reinterpret_cast<uint4*>(qsm);                 // q, magic, phase, slab offset
     uint32_t* s_pat = qsm + 4 * a.act_max;
-    __shared__ uint32_t s_seg, s_v, s_w0, s_nw;
+    // units are taken from a global counter; thread 0 resolves the next one
+    // while the block sweeps the current one.  Inside a unit, warps take
+    // 32-word blocks from a shared counter, so no warp waits on a slow one
+    // at the next unit boundary for longer than one block.
+    __shared__ uint32_t s_cur[4], s_next[4];
+    __shared__ uint32_t s_blk;
     __shared__ uint32_t s_staged;
-    if (threadIdx.x == 0) s_staged = 0xFFFFFFFFu;
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    __shared__ int s_has_next;
+    const uint32_t lane = threadIdx.x & 31;
     const uint64_t total = a.unit_prefix[a.n_segs];
-    for (uint64_t u = blockIdx.x; u < total; u += gridDim.x) {
-        __syncthreads();                                            // previous unit done with shared memory
-        if (threadIdx.x == 0) {
-            uint32_t lo = 0, hi = a.n_segs;                          // last seg with prefix <= u
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (a.unit_prefix[mid] <= u) lo = mid; else hi = mid;
-            }
-            const ccs_qseg& sg = a.segs[lo];
-            const uint32_t words = (uint32_t)(((uint64_t)sg.n_q + 63) >> 6);
-            const uint32_t w0 = (uint32_t)(u - a.unit_prefix[lo]) * a.unit_words;
-            s_seg = lo;
-            s_v = sg.variant;
-            s_w0 = w0;
-            s_nw = min(a.unit_words, words - w0);
-        }
+    if (threadIdx.x == 0) {
+        s_staged = 0xFFFFFFFFu;
+        const uint64_t u = atomicAdd(a.count + 1, 1u);
+        s_has_next = u < total;
+        if (u < total) qiter_unit(a, u, s_next);
+    }
+    __syncthreads();
+    while (s_has_next) {
+        if (threadIdx.x < 4) s_cur[threadIdx.x] = s_next[threadIdx.x];
+        if (threadIdx.x == 0) s_blk = 0;
         __syncthreads();
-        const uint32_t seg = s_seg, v = s_v, w0 = s_w0, nw = s_nw;
+        const uint32_t seg = s_cur[0], v = s_cur[1], w0 = s_cur[2], nw = s_cur[3];
         const uint4 vh = a.vhdr[v];
         if (s_staged != v) {
             for (uint32_t i = threadIdx.x; i < vh.w; i += blockDim.x) s_pat[i] = a.pat[vh.z + i];
@@ -122,10 +138,20 @@ qiter_sweep_kernel(QSweepArgs a) {
             s_act[i] = make_uint4(q, a.magic[e.x], (uint32_t)r, e.y);
         }
         __syncthreads();
-        if (threadIdx.x == 0) s_staged = v;
+        if (threadIdx.x == 0) {
+            s_staged = v;
+            const uint64_t u = atomicAdd(a.count + 1, 1u);           // next unit, resolved
+            s_has_next = u < total;                                  // while the block sweeps
+            if (u < total) qiter_unit(a, u, s_next);
+        }
         const uint32_t n_act = vh.y;
         const uint32_t n_q = sg.n_q;
-        for (uint32_t blk = warp; blk * 32 < nw; blk += nwarps) {
+        const uint32_t n_blk = (nw + 31) >> 5;
+        for (;;) {
+            uint32_t blk = 0;
+            if (lane == 0) blk = atomicAdd(&s_blk, 1u);
+            blk = __shfl_sync(0xFFFFFFFFu, blk, 0);
+            if (blk >= n_blk) break;
             const uint32_t k = blk * 32 + lane;
             const uint32_t wg = w0 + k;                              // word index in the segment
             uint32_t klo = 0, khi = 0;
@@ -174,6 +200,7 @@ qiter_sweep_kernel(QSweepArgs a) {
                 base++;
             }
         }
+        __syncthreads();                                             // unit done: shared memory free
     }
 }
 
@@ -436,7 +463,8 @@ ccs_status ccs_qiter_filter(ccs_qiter* Q, const ccs_qseg* segs, uint32_t n_segs,
         if (s != CCS_OK) return s;
     }
     const uint64_t units = Q->fst.h_prefix[n_segs];
-    CU(cudaMemsetAsync(Q->d_count.p, 0, 4, st));
+    if (units >= (1ull << 31)) return fail(CCS_ERR_INVALID, "too many Q in one call (split the segments)");
+    CU(cudaMemsetAsync(Q->d_count.p, 0, 8, st));
     if (units) {
         QSweepArgs a;
         a.vhdr = Q->d_vhdr.p;
