@@ -6,12 +6,14 @@
 // exactly when Q = (D_V * 2^(E+j))^-1 (mod q) (v16:1244-1266); the reference
 // ORs these residues into one mask per (V, q) and probes Q mod q for every Q
 // of a launch, one thread per Q (v16:2038-2153).  Here a lane owns a word of
-// 64 consecutive Q and a prime kills a whole word at once: the variant's
-// window pattern for q (bit b set when b mod q is forbidden, b < q + 64 and
-// beyond) is staged in shared memory, and the 64-bit window starting at the
-// word's phase u = Q mod q is three shared loads and two funnel shifts.  A
-// warp leaves the prime loop as soon as all 32 words are fully killed, which
-// after a few dozen primes is the common case.
+// 64 consecutive Q and a window kills a whole word at once: per variant, the
+// primes (ordered by the share of Q they kill) are merged into runs whose
+// product P stays within 8192, and each run's pattern (bit b set when b mod q
+// is forbidden for some q of the run, b < P + 64 and beyond) is staged in
+// shared memory; the 64-bit window starting at the word's phase u = Q mod P
+// is three shared loads and two funnel shifts.  A warp leaves the window loop
+// as soon as all 32 words are fully killed, which after a dozen windows is the
+// common case.
 //
 // Work units are runs of unit_words words of one segment (one variant, one
 // run of Q); blocks take units from a global counter and restage the pattern
@@ -48,15 +50,14 @@ constexpr uint32_t kQSlabMax = 16384;        // pattern words per variant (64 KB
 constexpr uint32_t kQThreads = 256;
 constexpr uint32_t kQUnitWords = 8192;       // 524,288 Q per work unit
 constexpr uint32_t kQMaxSegs = 1u << 20;
+constexpr uint64_t kQGroupMax = 8192;        // largest period of a merged window
 
 inline uint32_t q_words(uint32_t q) { return (q - 1) / 32 + 3; }
 
 struct QSweepArgs {
     const uint4* vhdr;                       // per variant: act_start, n_act, pat_start, pat_words
-    const uint2* act;                        // per active entry: prime index, slab offset
+    const uint4* act;                        // per window: period, floor(2^32 / period), slab offset
     const uint32_t* pat;
-    const uint32_t* primes;
-    const uint32_t* magic;                   // floor(2^32 / q)
     const ccs_qseg* segs;
     const uint64_t* unit_prefix;             // [n_segs + 1]
     uint32_t n_segs;
@@ -121,8 +122,8 @@ qiter_sweep_kernel(QSweepArgs a) {
         }
         const ccs_qseg& sg = a.segs[seg];
         for (uint32_t i = threadIdx.x; i < vh.y; i += blockDim.x) {
-            const uint2 e = a.act[vh.x + i];
-            const uint32_t q = a.primes[e.x];
+            const uint4 e = a.act[vh.x + i];
+            const uint32_t q = e.x;
             // (q_base + 64 w0) mod q, limb by limb from the top
             uint32_t L[4];
             uint64_t c = (uint64_t)w0 << 6;
@@ -135,7 +136,7 @@ qiter_sweep_kernel(QSweepArgs a) {
             uint64_t r = c;                                          // a carry out of 2^128 is 1
 #pragma unroll
             for (int w = 3; w >= 0; w--) r = ((r << 32) | L[w]) % q;
-            s_act[i] = make_uint4(q, a.magic[e.x], (uint32_t)r, e.y);
+            s_act[i] = make_uint4(q, e.y, (uint32_t)r, e.z);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -217,14 +218,14 @@ struct ccs_qiter {
     std::vector<uint32_t> primes;
     std::vector<uint32_t> dv;                 // [n_variants][4]
     std::vector<uint4> vhdr;
-    std::vector<uint2> act;
+    std::vector<uint4> act;                   // window: period, floor(2^32 / period), slab offset
     std::vector<uint32_t> pat;
+    std::vector<uint32_t> fcount;             // [variant][prime] forbidden residues
     uint32_t act_max = 0, slab_max = 0;
     size_t smem = 0;
     int blocks_per_sm = 1;
-    DevBuf<uint4> d_vhdr;
-    DevBuf<uint2> d_act;
-    DevBuf<uint32_t> d_pat, d_primes, d_magic, d_dv, d_count;
+    DevBuf<uint4> d_vhdr, d_act;
+    DevBuf<uint32_t> d_pat, d_dv, d_count;
     // segment staging, one set for filter calls and one for prove calls, so
     // that a filter and a prove may run at the same time from two host
     // threads (each on its own stream)
@@ -351,54 +352,58 @@ ccs_status ccs_qiter_create(const ccs_qiter_params* p, int device, ccs_qiter** o
     Q->target = p->target;
     Q->primes.assign(p->primes, p->primes + p->n_primes);
     Q->dv.assign(p->dv, p->dv + 4 * (size_t)p->n_variants);
-    // windows: per variant the active primes and their patterns
-    std::vector<uint32_t> fb(p->depth);
+    // windows: per variant the active primes (q not dividing D_V) with their
+    // forbidden residues, ordered by the share of Q they kill (the survivor
+    // set does not depend on the order; words die after fewer tests), then
+    // runs of consecutive primes whose product stays within kQGroupMax
+    // merged into one window of that period: one lookup tests the run
+    Q->fcount.assign((size_t)Q->n_variants * p->n_primes, 0);
+    struct Pr { uint32_t q; double surv; std::vector<uint32_t> res; };
+    std::vector<Pr> ps;
+    std::vector<char> seen;
     for (uint32_t v = 0; v < Q->n_variants; v++) {
         const unsigned __int128 D = dv_of(Q, v);
         if (D == 0) { delete Q; return fail(CCS_ERR_INVALID, "D_V must be >= 1"); }
-        const uint32_t act0 = (uint32_t)Q->act.size();
-        const uint32_t pat0 = (uint32_t)Q->pat.size();
+        ps.clear();
         for (uint32_t i = 0; i < p->n_primes; i++) {
             const uint32_t q = Q->primes[i];
             const uint32_t d = (uint32_t)(D % q);
             if (d == 0) continue;                                    // q | D_V: immune (v16:1247)
-            const uint32_t off = (uint32_t)Q->pat.size() - pat0;
-            const uint32_t nw = q_words(q);
-            Q->pat.resize(Q->pat.size() + nw, 0u);
-            uint32_t* w = Q->pat.data() + pat0 + off;
+            Pr e{q, 0.0, {}};
+            seen.assign(q, 0);
             for (uint32_t j = 0; j < p->depth; j++) {
                 const uint32_t m = (uint32_t)((uint64_t)d * pow2_mod(p->exp_start + j, q) % q);
                 const uint32_t r = inv_mod(m, q);                    // v16:1256-1258
-                for (uint32_t b = r; b < 32 * nw; b += q) w[b >> 5] |= 1u << (b & 31);
+                if (!seen[r]) { seen[r] = 1; e.res.push_back(r); }
             }
-            Q->act.push_back(make_uint2(i, off));
+            Q->fcount[(size_t)v * p->n_primes + i] = (uint32_t)e.res.size();
+            e.surv = (double)(q - e.res.size()) / q;
+            ps.push_back(std::move(e));
+        }
+        std::stable_sort(ps.begin(), ps.end(), [](const Pr& a, const Pr& b) { return a.surv < b.surv; });
+        const uint32_t act0 = (uint32_t)Q->act.size();
+        const uint32_t pat0 = (uint32_t)Q->pat.size();
+        for (size_t k = 0; k < ps.size();) {
+            uint64_t P = ps[k].q;
+            size_t e = k + 1;
+            while (e < ps.size() && P * ps[e].q <= kQGroupMax) P *= ps[e++].q;
+            const uint32_t off = (uint32_t)Q->pat.size() - pat0;
+            const uint32_t nw = q_words((uint32_t)P);
+            Q->pat.resize(Q->pat.size() + nw, 0u);
+            uint32_t* w = Q->pat.data() + pat0 + off;
+            for (size_t t = k; t < e; t++)
+                for (uint32_t r : ps[t].res)
+                    for (uint32_t b = r; b < 32 * nw; b += ps[t].q) w[b >> 5] |= 1u << (b & 31);
+            Q->act.push_back(make_uint4((uint32_t)P, (uint32_t)(0xFFFFFFFFull / P), off, 0u));
+            k = e;
         }
         const uint32_t n_act = (uint32_t)Q->act.size() - act0;
         const uint32_t words = (uint32_t)Q->pat.size() - pat0;
-        // the survivor set does not depend on the order of the primes: test
-        // the ones that kill the largest share of Q first (fewest survivors
-        // per residue), so that words die after fewer primes
-        {
-            std::vector<std::pair<double, uint2>> ord;
-            for (uint32_t k = 0; k < n_act; k++) {
-                const uint2 e = Q->act[act0 + k];
-                const uint32_t q = Q->primes[e.x];
-                const uint32_t* w = Q->pat.data() + pat0 + e.y;
-                uint32_t c = 0;
-                for (uint32_t b = 0; b < q; b++) c += (w[b >> 5] >> (b & 31)) & 1u;
-                ord.push_back({(double)(q - c) / q, e});
-            }
-            std::stable_sort(ord.begin(), ord.end(),
-                             [](const auto& a, const auto& b) { return a.first < b.first; });
-            for (uint32_t k = 0; k < n_act; k++) Q->act[act0 + k] = ord[k].second;
-        }
         if (words > kQSlabMax) { delete Q; return fail(CCS_ERR_INVALID, "sieve primes too large for one slab"); }
         Q->vhdr.push_back(make_uint4(act0, n_act, pat0, words));
         Q->act_max = std::max(Q->act_max, n_act);
         Q->slab_max = std::max(Q->slab_max, words);
     }
-    std::vector<uint32_t> magic(p->n_primes);
-    for (uint32_t i = 0; i < p->n_primes; i++) magic[i] = (uint32_t)(0xFFFFFFFFull / Q->primes[i]);
     Q->act_max = std::max<uint32_t>(Q->act_max, 1);
     Q->smem = (size_t)Q->act_max * 16 + (size_t)std::max<uint32_t>(Q->slab_max, 1) * 4;
     ccs_status s = engine_create_prover(device, p->primality, p->prove_mode,
@@ -410,7 +415,7 @@ ccs_status ccs_qiter_create(const ccs_qiter_params* p, int device, ccs_qiter** o
                                          cudaMemcpyHostToDevice) == cudaSuccess;
     };
     if (!up(Q->d_vhdr, Q->vhdr) || !up(Q->d_act, Q->act) || !up(Q->d_pat, Q->pat) ||
-        !up(Q->d_primes, Q->primes) || !up(Q->d_magic, magic) || !up(Q->d_dv, Q->dv) ||
+        !up(Q->d_dv, Q->dv) ||
         Q->d_count.alloc(2) != cudaSuccess || cudaMallocHost(&Q->h_count, 8) != cudaSuccess) {
         ccs_qiter_destroy(Q);
         return fail(CCS_ERR_NOMEM, "device allocation failed");
@@ -432,7 +437,7 @@ ccs_status ccs_qiter_destroy(ccs_qiter* Q) {
     if (!Q) return CCS_OK;
     cudaSetDevice(Q->device);
     if (Q->pe) ccs_destroy(Q->pe);
-    Q->d_vhdr.free_(); Q->d_act.free_(); Q->d_pat.free_(); Q->d_primes.free_(); Q->d_magic.free_();
+    Q->d_vhdr.free_(); Q->d_act.free_(); Q->d_pat.free_();
     Q->d_dv.free_(); Q->d_count.free_();
     for (ccs_qiter::Staging* S : {&Q->fst, &Q->pst}) {
         S->d_segs.free_();
@@ -470,8 +475,6 @@ ccs_status ccs_qiter_filter(ccs_qiter* Q, const ccs_qseg* segs, uint32_t n_segs,
         a.vhdr = Q->d_vhdr.p;
         a.act = Q->d_act.p;
         a.pat = Q->d_pat.p;
-        a.primes = Q->d_primes.p;
-        a.magic = Q->d_magic.p;
         a.segs = Q->fst.d_segs.p;
         a.unit_prefix = Q->fst.d_prefix.p;
         a.n_segs = n_segs;
@@ -536,17 +539,7 @@ ccs_status ccs_qiter_forbidden_count(const ccs_qiter* Q, uint32_t v, uint32_t* c
     if (!Q || !counts) return fail(CCS_ERR_INVALID, "null argument");
     if (v >= Q->n_variants) return fail(CCS_ERR_INVALID, "variant out of range");
     const uint32_t n = (uint32_t)Q->primes.size();
-    for (uint32_t i = 0; i < std::min(n, cap); i++) counts[i] = 0;
-    const uint4 h = Q->vhdr[v];
-    for (uint32_t k = 0; k < h.y; k++) {
-        const uint2 e = Q->act[h.x + k];
-        if (e.x >= cap) continue;
-        const uint32_t q = Q->primes[e.x];
-        const uint32_t* w = Q->pat.data() + h.z + e.y;
-        uint32_t c = 0;
-        for (uint32_t b = 0; b < q; b++) c += (w[b >> 5] >> (b & 31)) & 1u;
-        counts[e.x] = c;
-    }
+    for (uint32_t i = 0; i < std::min(n, cap); i++) counts[i] = Q->fcount[(size_t)v * n + i];
     return CCS_OK;
 }
 
