@@ -949,7 +949,10 @@ ccs_status engine_create_prover(int device, uint32_t primality, uint32_t prove_m
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, device));
     E->sms = prop.multiProcessorCount;
-    CU(cudaStreamCreateWithFlags(&E->own_stream, cudaStreamNonBlocking));
+    // proves run beside long filter launches: their blocks go first
+    int lo_prio = 0, hi_prio = 0;
+    CU(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
+    CU(cudaStreamCreateWithPriority(&E->own_stream, cudaStreamNonBlocking, hi_prio));
     ccs_status st = upload_prove(E, E->own_stream);
     if (st != CCS_OK) { ccs_destroy(E); return st; }
     if (E->d_prange.alloc(1) || E->d_counters.alloc(8)) {

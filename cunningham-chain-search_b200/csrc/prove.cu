@@ -742,7 +742,10 @@ prove_kernel(ProveArgs a) {
             }
         }
         if (!a.q.seg && big_bits(nb) != (int)R.bits) continue;         // v13:1495, 1828
-        const int ntd = (pc.prove_mode == CCS_PROVE_ROOTS) ? 132 : 62;  // v13:1499 / 1832
+        // trial division only rejects composites that the primality test
+        // rejects too (n > 863); q-iteration survivors passed the sieve at
+        // position 0 already, so for them it is skipped
+        const int ntd = a.q.seg ? 0 : (pc.prove_mode == CCS_PROVE_ROOTS) ? 132 : 62;  // v13:1499 / 1832
         bool comp = false;
         for (int t = 0; t < ntd && !comp; t++) comp = big_mod_small(nb, c_screen[t]) == 0;
         if (comp) continue;
@@ -1028,7 +1031,7 @@ __global__ void __launch_bounds__(256)
 prove_seed_kernel(StagedProve p) {
     const ProveConst& pc = c_prove[p.range->profile];
     const ProveRange& R = *p.range;
-    const uint32_t ntd = (pc.prove_mode == CCS_PROVE_ROOTS) ? 132 : 62;        // v13:1499 / 1832
+    const uint32_t ntd = p.q.seg ? 0u : (pc.prove_mode == CCS_PROVE_ROOTS) ? 132u : 62u;  // v13:1499 / 1832
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < p.n_surv; i0 += gridDim.x * blockDim.x) {
         const uint32_t i = i0 + threadIdx.x;
         bool keep = false;

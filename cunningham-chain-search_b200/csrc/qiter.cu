@@ -483,7 +483,9 @@ ccs_status ccs_qiter_filter(ccs_qiter* Q, const ccs_qseg* segs, uint32_t n_segs,
         a.out = (uint32_t*)out_dev;
         a.count = Q->d_count.p;
         a.cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
-        const uint64_t grid = std::min<uint64_t>(units, (uint64_t)Q->sms * Q->blocks_per_sm);
+        // one block slot per SM stays free for a prove running beside the filter
+        const uint64_t per_sm = Q->blocks_per_sm > 2 ? Q->blocks_per_sm - 1 : Q->blocks_per_sm;
+        const uint64_t grid = std::min<uint64_t>(units, (uint64_t)Q->sms * per_sm);
         qiter_sweep_kernel<<<(uint32_t)grid, kQThreads, Q->smem, st>>>(a);
         CU(cudaGetLastError());
     }

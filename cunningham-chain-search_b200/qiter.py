@@ -282,7 +282,8 @@ class QIter:
         _check(st, "ccs_qiter_prove")
         return out[: n.value], pr.value
 
-    def run(self, plan, min_report_len=8, surv_cap=1 << 22, chain_cap=1 << 16, pool_primes=None):
+    def run(self, plan, min_report_len=8, surv_cap=1 << 22, chain_cap=1 << 16, pool_primes=None,
+            dedup_p0=True):
         """Filters and proves a list of steps (each a segment list), the
         prove of step i overlapping the filter of step i + 1 (two host
         threads, two streams, two survivor buffers), as the reference
@@ -299,6 +300,7 @@ class QIter:
         work = queue.Queue(maxsize=1)
         tot = {"steps": 0, "q": 0, "survivors": 0, "chains": 0, "primes": 0}
         lines, err = [], []
+        seen = set() if dedup_p0 else None
 
         def prover():
             while True:
@@ -311,7 +313,7 @@ class QIter:
                         c, pr = self.prove(segs, surv, out=chains)
                         tot["chains"] += c.shape[0]
                         tot["primes"] += pr
-                        lines.extend(self.hit_lines(segs, c, min_report_len, pool_primes))
+                        lines.extend(self.hit_lines(segs, c, min_report_len, pool_primes, seen))
                 except Exception as ex:                   # reported to the caller below
                     err.append(ex)
                 finally:
@@ -346,10 +348,13 @@ class QIter:
         return list(arr)
 
     # ---------------------------------------------------------------- output
-    def hit_lines(self, segs, chains, min_report_len=8, pool_primes=None):
+    def hit_lines(self, segs, chains, min_report_len=8, pool_primes=None, seen=None):
         """The reference's HIT lines for records of at least min_report_len,
         sorted; fp lists the pool primes dividing p_0 + 1 and pool the
-        variants whose D_V divides it (v16:2775-2848)."""
+        variants whose D_V divides it (v16:2775-2848).  With a set `seen`
+        (its --dedup-p0, v16:2826-2848), a p_0 already in it gives the short
+        "HIT-DUP seed=.. len=.. A=.. p_0=0x.." line instead, and new p_0 are
+        added."""
         recs = np.asarray(chains.cpu().numpy() if hasattr(chains, "cpu") else chains).astype(np.int64) & 0xFFFFFFFF
         lines = []
         for r in recs:
@@ -360,6 +365,11 @@ class QIter:
             qb = sum(int(sg[w]) << (32 * w) for w in range(4)) if isinstance(segs, np.ndarray) else int(sg[0])
             Q = qb + int(r[0])
             p0 = sum(int(x) << (32 * i) for i, x in enumerate(r[4:10]))
+            if seen is not None and p0 in seen:
+                lines.append(f"HIT-DUP seed={self.seed_name} len={L} A={Q} p_0=0x{p0:x}")
+                continue
+            if seen is not None:
+                seen.add(p0)
             fp = [q for q in pool_primes if (p0 + 1) % q == 0] if pool_primes else None
             pool = [self.names[i] for i, d in enumerate(self.dv) if (p0 + 1) % d == 0]
             lines.append(format_hit_line(self.seed_name, L, Q, p0, fp, pool))

@@ -163,7 +163,7 @@ def test_pipelined_run_equals_sequential(ccs):
     pool = _pool(ccs)
     qi = ccs.QIter(pool, target=8, depth=8, primes=ccs.qiter_sieve_primes(sieve_max=131, ext=False))
     plan = [qi.random_segments(16, 1 << 18, 64, 80, seed=s, start_variant=s) for s in range(6)]
-    tot, lines = qi.run(plan, min_report_len=4)
+    tot, lines = qi.run(plan, min_report_len=4, dedup_p0=False)
     want_lines, n_s, n_c, n_p = [], 0, 0, 0
     for segs in plan:
         s_ = qi.filter(segs)
@@ -175,4 +175,9 @@ def test_pipelined_run_equals_sequential(ccs):
     assert (tot["steps"], tot["survivors"], tot["chains"], tot["primes"]) == (6, n_s, n_c, n_p)
     assert tot["q"] == 6 * 16 * (1 << 18)
     assert lines == sorted(want_lines) and len(lines) > 0 and n_s > 1000
+    # the same plan twice with --dedup-p0: the second sighting of every p_0
+    # is a HIT-DUP line
+    _, lines2 = qi.run(plan + plan, min_report_len=4)
+    dups = [l for l in lines2 if l.startswith("HIT-DUP")]
+    assert len(dups) == len(lines) and len(lines2) == 2 * len(lines)
     qi.close()
