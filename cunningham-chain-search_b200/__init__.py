@@ -791,4 +791,5 @@ def mixed_ranges(engines, n, seed, min_log2=20, max_log2=34, width_lo=64, width_
 
 
 from .qiter import (QIter, parse_pool, parse_pool_spec, parse_pool_specs, pool_from_text,  # noqa: E402
-                    qiter_sieve_primes, q_window, V16_EXT_PRIMES, format_hit_line, synthetic_pool)
+                    qiter_sieve_primes, q_window, V16_EXT_PRIMES, format_hit_line, synthetic_pool,
+                    QCampaign, QITER_CHECKPOINT_VERSION, sieve_hash, pool_hash)

@@ -374,3 +374,216 @@ class QIter:
             pool = [self.names[i] for i, d in enumerate(self.dv) if (p0 + 1) % d == 0]
             lines.append(format_hit_line(self.seed_name, L, Q, p0, fp, pool))
         return sorted(lines)
+
+
+# ---------------------------------------------------------------------------
+# campaign: Q walkers, checkpoint/resume, HIT log
+# ---------------------------------------------------------------------------
+QITER_CHECKPOINT_VERSION = "v16.0.3-drained-cursor"
+_FNV_OFFSET, _FNV_PRIME, _M64 = 0xCBF29CE484222325, 0x100000001B3, (1 << 64) - 1
+
+
+def fnv1a64(data):
+    h = _FNV_OFFSET
+    for b in data:
+        h = ((h ^ b) * _FNV_PRIME) & _M64
+    return h
+
+
+def sieve_hash(primes):
+    """FNV-1a 64 over the sieve list as little-endian u32 (v16:4080-4083)."""
+    return fnv1a64(b"".join(int(q).to_bytes(4, "little") for q in primes))
+
+
+def pool_hash(dv):
+    """FNV-1a 64 over "D_dec," for every variant (v16:4087-4097)."""
+    return fnv1a64(b"".join(str(int(d)).encode() + b"," for d in dv))
+
+
+class QCampaign:
+    """A q-iteration campaign: per-variant Q walkers over a bit band, the
+    reference's round-robin variant choice, sequential cursors or random
+    starts (--q-order), per-variant choice by window width
+    (--q-band-mode exhaustive, --exhaustive-max-q-bits), its checkpoint file
+    (v16:4108-4400: identity keys, FNV-1a hashes of the sieve list and the
+    pool, sparse drained cursors) and its HIT log.
+
+    The sieve list hashed is the reference's GPU list (primes 7..sieve_max
+    outside the immune set); the engine may sieve more (509..1009), which
+    the reference does on its CPU."""
+
+    def __init__(self, qiter, bits_min=90, bits_max=127, q_order="random", q_band_mode="fixed",
+                 exhaustive_max_q_bits=40, q_chunk=1 << 24, seed=1, immune=(2, 3, 5), sieve_max=503,
+                 chunks_per_step=256, min_report_len=8, dedup_p0=True, checkpoint_path=None, resume=False,
+                 out_path=None):
+        if q_order not in ("random", "sequential") or q_band_mode not in ("fixed", "exhaustive"):
+            raise ValueError("q_order: random | sequential; q_band_mode: fixed | exhaustive")
+        self.qi = qiter
+        self.bits_min, self.bits_max = bits_min, bits_max
+        self.q_order, self.q_band_mode = q_order, q_band_mode
+        self.xbits = exhaustive_max_q_bits
+        self.q_chunk, self.seed = int(q_chunk), seed
+        self.immune = tuple(immune)
+        self.D = 1
+        for q in self.immune:
+            self.D *= q
+        self.sieve_max = sieve_max
+        self.gpu_list = qiter_sieve_primes(self.immune, sieve_max, ext=False)
+        self.chunks_per_step = chunks_per_step
+        self.min_report_len = min_report_len
+        self.seen = set() if dedup_p0 else None
+        self.ck_path, self.out_path = checkpoint_path, out_path
+        from .campaign import XorShift64
+        self.rng = XorShift64(seed)
+        self.win = qiter.windows(bits_min, bits_max)
+        n = len(self.win)
+        self.exhausted = [a > b for a, b in self.win]
+        self.cursor = [a for a, _ in self.win]
+        self.random = []
+        for a, b in self.win:
+            if q_band_mode == "exhaustive":
+                self.random.append(a <= b and (b - a + 1).bit_length() > self.xbits)
+            else:
+                self.random.append(q_order == "random")
+        self.cur_v = 0
+        self.totals = {"steps": 0, "q": 0, "survivors": 0, "chains": 0, "primes": 0}
+        self.lines = []
+        if resume and checkpoint_path:
+            import os
+            if os.path.exists(checkpoint_path):
+                self.load(checkpoint_path)
+        assert len(self.cursor) == n
+
+    # -- walkers (v16:5647-5700) -------------------------------------------
+    def _next_chunk(self):
+        n = len(self.win)
+        for step in range(n):
+            v = (self.cur_v + step) % n
+            if self.exhausted[v]:
+                continue
+            qmn, qmx = self.win[v]
+            if self.random[v]:
+                span = qmx - qmn + 1
+                this = min(self.q_chunk, span)
+                r = ((self.rng.next() << 64) | self.rng.next()) % (span - this + 1)
+                qb = qmn + r
+            else:
+                cur = self.cursor[v]
+                if cur > qmx:
+                    self.exhausted[v] = True
+                    continue
+                this = min(self.q_chunk, qmx - cur + 1)
+                qb = cur
+                self.cursor[v] = cur + this
+            self.cur_v = (v + 1) % n
+            return (qb, this, v)
+        return None
+
+    def next_step(self):
+        segs = []
+        while len(segs) < self.chunks_per_step:
+            c = self._next_chunk()
+            if c is None:
+                break
+            segs.append(c)
+        return segs or None
+
+    def run(self, max_steps=None):
+        done = 0
+        plan = []
+        while max_steps is None or done < max_steps:
+            segs = self.next_step()
+            if segs is None:
+                break
+            plan.append(segs)
+            done += 1
+        if plan:
+            tot, lines = self.qi.run(plan, self.min_report_len, dedup_p0=False)
+            for k in tot:
+                self.totals[k] += tot[k]
+            if self.seen is not None:
+                kept = []
+                for ln in lines:                              # dedup across steps and runs
+                    p0 = int(ln.rsplit("p_0=0x", 1)[1], 16)
+                    if p0 in self.seen:
+                        A = ln.split(" A=", 1)[1].split(" ", 1)[0]
+                        L = ln.split(" len=", 1)[1].split(" ", 1)[0]
+                        ln = f"HIT-DUP seed={self.qi.seed_name} len={L} A={A} p_0=0x{p0:x}"
+                    else:
+                        self.seen.add(p0)
+                    kept.append(ln)
+                lines = kept
+            self.lines.extend(lines)
+            if self.out_path and lines:
+                with open(self.out_path, "a") as f:
+                    f.write("".join(ln + "\n" for ln in lines))
+        if self.ck_path:
+            self.save(self.ck_path)
+        return dict(self.totals)
+
+    # -- checkpoint (v16:4108-4218, 4242-4390) --------------------------------
+    def _identity(self):
+        return {"version": QITER_CHECKPOINT_VERSION, "mode": "q-iter", "target_len": str(self.qi.target),
+                "sieve_depth": str(self.qi.depth), "bits_min": str(self.bits_min),
+                "bits_max": str(self.bits_max), "seed_name": self.qi.seed_name, "D_dec": str(self.D),
+                "exp_start": str(self.qi.exp_start), "sieve_prime_max": str(self.sieve_max),
+                "sieve_fnv1a64": f"0x{sieve_hash(self.gpu_list):016x}",
+                "pool_seeds_count": str(len(self.qi.dv)),
+                "pool_seeds_fnv1a64": f"0x{pool_hash(self.qi.dv):016x}", "q_order": self.q_order,
+                "q_band_mode": self.q_band_mode}
+
+    def save(self, path):
+        import os
+        idn = self._identity()
+        out = [f"version={idn['version']}", "mode=q-iter", f"target_len={idn['target_len']}",
+               f"sieve_depth={idn['sieve_depth']}", "target_bits=0", f"bits_min={self.bits_min}",
+               f"bits_max={self.bits_max}", f"seed_name={self.qi.seed_name}", f"D_dec={self.D}",
+               "D_primes=" + ",".join(str(q) for q in self.immune), f"exp_start={self.qi.exp_start}",
+               f"sieve_prime_max={self.sieve_max}",
+               "sieve_primes=" + ",".join(str(q) for q in self.gpu_list if q > 53),
+               f"sieve_fnv1a64={idn['sieve_fnv1a64']}", f"pool_seeds_count={idn['pool_seeds_count']}",
+               f"pool_seeds_fnv1a64={idn['pool_seeds_fnv1a64']}", f"q_order={self.q_order}"]
+        if self.q_order == "random":
+            out.append(f"q_seed={self.seed}")
+        out.append(f"q_chunk={self.q_chunk}")
+        out.append(f"q_band_mode={self.q_band_mode}")
+        if self.q_band_mode == "exhaustive":
+            out.append(f"exhaustive_max_q_bits={self.xbits}")
+        for v, (cur, (qmn, _)) in enumerate(zip(self.cursor, self.win)):
+            if cur > qmn:
+                out.append(f"v_cursor_drained[{v}]={cur}")
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            f.write("\n".join(out) + "\n")
+        os.replace(tmp, path)
+
+    def load(self, path):
+        kv, cursors = {}, {}
+        with open(path) as f:
+            for ln in f:
+                if "=" not in ln:
+                    continue
+                k, val = ln.rstrip("\n").split("=", 1)
+                if k.startswith("v_cursor_drained["):
+                    cursors[int(k[17:].split("]", 1)[0])] = int(val)
+                else:
+                    kv[k] = val
+        if kv.get("mode") != "q-iter":
+            raise ValueError("checkpoint is not a q-iter checkpoint")
+        idn = self._identity()
+        for k in ("version", "seed_name", "D_dec", "target_len", "sieve_depth", "exp_start", "bits_min",
+                  "bits_max", "sieve_prime_max", "pool_seeds_count", "q_order"):
+            if kv.get(k) != idn[k]:
+                raise ValueError(f"checkpoint {k}={kv.get(k)} does not match current {idn[k]}")
+        for k in ("sieve_fnv1a64", "pool_seeds_fnv1a64"):
+            if int(kv.get(k, "0"), 0) != int(idn[k], 0):
+                raise ValueError(f"checkpoint {k} does not match")
+        if kv.get("q_band_mode", self.q_band_mode) != self.q_band_mode:
+            raise ValueError("checkpoint q_band_mode does not match")
+        if self.q_band_mode == "exhaustive" and int(kv.get("exhaustive_max_q_bits", self.xbits)) != self.xbits:
+            raise ValueError("checkpoint exhaustive_max_q_bits does not match")
+        for v, cur in cursors.items():
+            if 0 <= v < len(self.cursor):
+                self.cursor[v] = cur
+                if cur > self.win[v][1]:
+                    self.exhausted[v] = True

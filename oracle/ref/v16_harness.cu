@@ -175,4 +175,83 @@ float ref16_qiter_time(const unsigned* primes, int n_qp, unsigned long long d_lo
     return ms;
 }
 
+/* The reference's q-iter checkpoint writer and reader on a configuration
+ * given field by field (v16:4108-4390).  The sieve list hashed is q_primes;
+ * its "sieve_primes=" line lists the q_primes above the default wheel bound
+ * 53 (select_wheel_sieve with --wheel-max 53, v16:1408-1451).  pool_csv:
+ * D_V in decimal, comma-separated. */
+static void ref16_cfg(v16_cfg* c, int target, int depth, int bits_min, int bits_max, const char* seed_name,
+                      const unsigned* immune, int n_immune, int E, unsigned sieve_max, const unsigned* q_primes,
+                      int n_qp, int q_random, unsigned long long q_seed, unsigned q_chunk, int exhaustive,
+                      int xbits) {
+    memset(c, 0, sizeof(*c));
+    c->target_len = target;
+    c->sieve_depth = depth;
+    c->bits_min = bits_min;
+    c->bits_max = bits_max;
+    strncpy(c->seed_name, seed_name, sizeof(c->seed_name) - 1);
+    c->D = 1;
+    for (int i = 0; i < n_immune; i++) { c->D_primes[i] = immune[i]; c->D *= immune[i]; }
+    c->n_D_primes = n_immune;
+    u128_to_dec(c->D, c->D_dec, sizeof(c->D_dec));
+    c->exp_start = E;
+    c->sieve_prime_max = sieve_max;
+    c->wheel_prime_max = 53;
+    for (int i = 0; i < n_qp; i++)
+        if (q_primes[i] > 53) c->sieve_primes[c->n_sieve_primes++] = q_primes[i];
+    c->q_iter = 1;
+    c->q_order_random = q_random;
+    c->q_seed = q_seed;
+    c->q_chunk = q_chunk;
+    c->q_band_mode_exhaustive = exhaustive;
+    c->exhaustive_max_q_bits = xbits;
+}
+
+static v16_pool_seed* ref16_pool(const char* pool_csv, int n_v) {
+    v16_pool_seed* ps = (v16_pool_seed*)calloc((size_t)n_v, sizeof(v16_pool_seed));
+    const char* p = pool_csv;
+    for (int v = 0; v < n_v; v++) {
+        int k = 0;
+        while (*p && *p != ',' && k < 79) ps[v].D_dec[k++] = *p++;
+        if (*p == ',') p++;
+    }
+    return ps;
+}
+
+int ref16_ckpt_save(const char* path, int target, int depth, int bits_min, int bits_max, const char* seed_name,
+                    const unsigned* immune, int n_immune, int E, unsigned sieve_max, const unsigned* q_primes,
+                    int n_qp, int q_random, unsigned long long q_seed, unsigned q_chunk, int exhaustive,
+                    int xbits, const char* pool_csv, int n_v, const unsigned long long* cur_lo,
+                    const unsigned long long* cur_hi, const unsigned long long* qmin_lo,
+                    const unsigned long long* qmin_hi) {
+    static v16_cfg c;
+    ref16_cfg(&c, target, depth, bits_min, bits_max, seed_name, immune, n_immune, E, sieve_max, q_primes,
+              n_qp, q_random, q_seed, q_chunk, exhaustive, xbits);
+    strncpy(c.checkpoint_file, path, sizeof(c.checkpoint_file) - 1);
+    v16_pool_seed* ps = ref16_pool(pool_csv, n_v);
+    int r = save_q_iter_checkpoint(&c, (const u64*)cur_lo, (const u64*)cur_hi, (const u64*)qmin_lo,
+                                   (const u64*)qmin_hi, n_v, q_iter_sieve_fnv1a64(q_primes, n_qp),
+                                   q_iter_pool_fnv1a64(ps, n_v));
+    free(ps);
+    return r;
+}
+
+/* 0 and the cursors found (others left as given), or -1 when the reference
+ * refuses the file */
+int ref16_ckpt_load(const char* path, int target, int depth, int bits_min, int bits_max, const char* seed_name,
+                    const unsigned* immune, int n_immune, int E, unsigned sieve_max, const unsigned* q_primes,
+                    int n_qp, int q_random, unsigned long long q_seed, unsigned q_chunk, int exhaustive,
+                    int xbits, const char* pool_csv, int n_v, unsigned long long* cur_lo,
+                    unsigned long long* cur_hi) {
+    static v16_cfg c;
+    ref16_cfg(&c, target, depth, bits_min, bits_max, seed_name, immune, n_immune, E, sieve_max, q_primes,
+              n_qp, q_random, q_seed, q_chunk, exhaustive, xbits);
+    strncpy(c.resume_file, path, sizeof(c.resume_file) - 1);
+    v16_pool_seed* ps = ref16_pool(pool_csv, n_v);
+    int r = load_q_iter_checkpoint(&c, (u64*)cur_lo, (u64*)cur_hi, n_v, q_iter_sieve_fnv1a64(q_primes, n_qp),
+                                   q_iter_pool_fnv1a64(ps, n_v));
+    free(ps);
+    return r;
+}
+
 }  // extern "C"

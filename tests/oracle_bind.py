@@ -350,6 +350,11 @@ def ref16():
     lib.ref16_qiter_filter.restype = C.c_uint
     lib.ref16_qiter_filter.argtypes = [_u32p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_int,
                                        C.c_ulonglong, C.c_ulonglong, C.c_uint, _u32p, C.c_uint]
+    ck = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, _u32p, C.c_int, C.c_int, C.c_uint,
+          _u32p, C.c_int, C.c_int, C.c_ulonglong, C.c_uint, C.c_int, C.c_int, C.c_char_p, C.c_int]
+    _u64p_ = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+    lib.ref16_ckpt_save.argtypes = ck + [_u64p_, _u64p_, _u64p_, _u64p_]
+    lib.ref16_ckpt_load.argtypes = ck + [_u64p_, _u64p_]
     lib.ref16_qiter_time.restype = C.c_float
     lib.ref16_qiter_time.argtypes = [_u32p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_int,
                                      C.c_ulonglong, C.c_ulonglong, C.c_uint, C.c_int, C.POINTER(C.c_uint)]
