@@ -176,7 +176,7 @@ qiter_sweep_kernel(QSweepArgs a) {
                 const uint32_t sh = ph & 31;
                 klo |= __funnelshift_r(x0, x1, sh);
                 khi |= __funnelshift_r(x1, x2, sh);
-                if ((i & 3) == 3 && __all_sync(0xFFFFFFFFu, (klo & khi) == 0xFFFFFFFFu)) break;
+                if (__all_sync(0xFFFFFFFFu, (klo & khi) == 0xFFFFFFFFu)) break;   // after every window
             }
             const uint32_t llo = ~klo, lhi = ~khi;
             const uint32_t cnt = __popc(llo) + __popc(lhi);
