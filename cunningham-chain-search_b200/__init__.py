@@ -154,6 +154,12 @@ class _QIterParams(C.Structure):
                 ("flags", C.c_uint32)]
 
 
+class _RangePlan(C.Structure):
+    _fields_ = [("extended", C.c_uint32), ("q0", C.c_uint32), ("n_lines", C.c_uint64),
+                ("n_words", C.c_uint32), ("unit_words", C.c_uint32), ("units", C.c_uint64),
+                ("grid", C.c_uint32), ("block_threads", C.c_uint32)]
+
+
 class _QSeg(C.Structure):
     _fields_ = [("q_base", C.c_uint32 * 4), ("n_q", C.c_uint32), ("variant", C.c_uint32)]
 
@@ -168,6 +174,7 @@ _SIGS = {
     "ccs_abi_version": (C.c_int, []),
     "ccs_filter_range": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
     "ccs_filter_range_noalloc": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
+    "ccs_plan_range": (C.c_int, [_vp, _u64, _u64, _u64, C.POINTER(_RangePlan)]),
     "ccs_prove": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64),
                             C.POINTER(_u64), _vp]),
     "ccs_set_bits": (C.c_int, [_vp, C.c_uint32]),
@@ -443,12 +450,21 @@ class Engine:
         _check(st, "ccs_filter_range")
         return out[: n.value]
 
+    def plan_range(self, tile_start, n_tiles):
+        """How filter_range would sweep the range with the current tuning
+        (ccs_plan_range): lattice, words, work units, launch shape."""
+        lo, hi = _split128(tile_start)
+        p = _RangePlan()
+        _check(load_library().ccs_plan_range(self.h, lo, hi, int(n_tiles), C.byref(p)), "ccs_plan_range")
+        return {f: getattr(p, f) for f, _ in _RangePlan._fields_}
+
     def filter_range_noalloc(self, tile_start, n_tiles, out, stream=None):
         """filter_range through the entry point that allocates no device
         memory (ccs_filter_range_noalloc); out is a caller-owned int32 CUDA
-        tensor [cap, 4].  For callers that cannot allocate at call time
-        (inside stream capture, fixed-footprint embedders); calls that overlap
-        on one GPU race on its shared working array."""
+        tensor [cap, 4].  For callers that may not allocate device memory
+        once running (a GPU footprint fixed at start-up, allocators that do
+        not grow, memory quotas); synchronous; calls that overlap on one GPU
+        race on its shared working array."""
         lo, hi = _split128(tile_start)
         n = _u64(0)
         s = stream.cuda_stream if stream is not None else None

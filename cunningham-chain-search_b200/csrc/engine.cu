@@ -1011,6 +1011,29 @@ int engine_slot(const ccs_engine* E) { return E->slot; }
 
 extern "C" {
 
+ccs_status ccs_plan_range(const ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint64_t n_tiles,
+                          ccs_range_plan* out) {
+    if (!E || !out) return fail(CCS_ERR_INVALID, "null argument");
+    if (n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
+    memset(out, 0, sizeof(*out));
+    RangeDev R;
+    memset(&R, 0, sizeof(R));
+    const FilterSet& f = place_range(E, mk128(ts_lo, ts_hi), n_tiles, R);
+    out->extended = &f == &E->fs[1] ? 1u : 0u;
+    out->q0 = f.hp.q0;
+    out->n_lines = f.hp.lines.size();
+    out->n_words = R.n_words;
+    out->unit_words = R.unit_words;
+    out->units = n_tiles ? units_of(f, R.n_words, R.unit_words) : 0;
+    uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
+    const uint32_t wpb = E->tune.block_threads / 32;
+    const uint64_t need = (out->units + wpb - 1) / wpb;
+    if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
+    out->grid = grid;
+    out->block_threads = E->tune.block_threads;
+    return CCS_OK;
+}
+
 ccs_status ccs_walk_modmuls(ccs_engine* E, uint64_t* count, int reset) {
     if (!E || !count) return fail(CCS_ERR_INVALID, "null argument");
     CU(cudaSetDevice(E->device));
@@ -1028,12 +1051,13 @@ ccs_status ccs_walk_word_products(ccs_engine* E, uint64_t* modmuls, uint64_t* wo
 // ---------------------------------------------------------------------------
 // filter without allocation
 //
-// For callers that cannot allocate device memory at the point of the call:
-// code running inside a CUDA stream capture or a host callback (where
-// cudaMalloc is not allowed), allocators that forbid growth after start-up,
-// and embedders that pre-size their GPU footprint.  The engine's tables were
-// allocated by ccs_create; this entry point uses only a fixed scratch area
-// that lives in the library image itself.
+// For callers that may not allocate device memory once they are running:
+// services whose GPU footprint is fixed and accounted for at start-up,
+// allocators that refuse to grow after initialisation, and hosts that share
+// the device with other tenants under a memory quota.  The engine's tables
+// were allocated by ccs_create; this entry point uses only a fixed scratch
+// area that lives in the library image itself.  It is synchronous: it waits
+// for its stream before returning the survivor count.
 // ---------------------------------------------------------------------------
 
 // Scratch layout (bytes):
@@ -1042,18 +1066,22 @@ ccs_status ccs_walk_word_products(ccs_engine* E, uint64_t* modmuls, uint64_t* wo
 constexpr uint32_t kNoAllocMaxPrimes = 16384;
 constexpr size_t kNoAllocJmodOff = 1024;
 constexpr size_t kNoAllocBytes = kNoAllocJmodOff + 4ull * kNoAllocMaxPrimes;   // 66,560 B
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(sizeof(RangeDev) <= 256, "range descriptor must fit its 256-byte scratch slot");
+static_assert(sizeof(SweepHeader) <= 256, "sweep header must fit its 256-byte scratch slot");
 
 // One copy per device that loads the library, held until process exit.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 namespace {
 std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_ptr[64] = {nullptr};
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
 
 // Device address of the scratch array on `device` (which must be current).
 // Resolved once per device; the host-side name of the array is not a device
 // address and is never passed to a kernel.
 ccs_status noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(CCS_ERR_INVALID, "bad device ordinal");
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_ptr[device]) {
         void* p = nullptr;
@@ -1072,14 +1100,14 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
     if (!E || !n_out) return fail(CCS_ERR_INVALID, "null argument");
     if (cap && !out_dev) return fail(CCS_ERR_INVALID, "out_dev is null");
     if (n_tiles >= (1ull << 32)) return fail(CCS_ERR_INVALID, "n_tiles must be < 2^32");
-    const FilterSet& f = E->fs[0];
-    const HostProfile& hp = f.hp;
-    const uint32_t np = (uint32_t)hp.range_primes.size();
-    if (np > kNoAllocMaxPrimes)
-        return fail(CCS_ERR_INVALID, "ccs_filter_range_noalloc supports at most " +
-                                         std::to_string(kNoAllocMaxPrimes - kNumA) +
-                                         " filter primes per engine (this engine has " +
-                                         std::to_string(np - kNumA) + ")");
+    for (int v = 0; v < E->n_fs; v++) {
+        const uint32_t np = (uint32_t)E->fs[v].hp.range_primes.size();
+        if (np > kNoAllocMaxPrimes)
+            return fail(CCS_ERR_INVALID, "ccs_filter_range_noalloc supports at most " +
+                                             std::to_string(kNoAllocMaxPrimes - kNumA) +
+                                             " filter primes per engine (this engine has " +
+                                             std::to_string(np - kNumA) + ")");
+    }
     unsigned __int128 ts = mk128(ts_lo, ts_hi);
     if (ts + n_tiles < ts) return fail(CCS_ERR_INVALID, "tile range wraps 2^128");
     CU(cudaSetDevice(E->device));
@@ -1096,45 +1124,46 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
     uint32_t* d_jmod = (uint32_t*)(base + kNoAllocJmodOff);
     // the array keeps the previous call's contents: zero the counter
     CU(cudaMemsetAsync(d_cnt, 0, 4, st));
+    // descriptors are staged through the engine's pinned buffer (the same
+    // slots the plain path uses; the call waits for its copies below)
+    RangeDev* hr = (RangeDev*)E->h_stage;
+    uint64_t* hpre = (uint64_t*)((char*)E->h_stage + 1024);
+    SweepHeader* hh = (SweepHeader*)((char*)E->h_stage + 2048);
     if (n_tiles) {
-        const uint64_t nt = n_tiles, off = 0;
-        const unsigned __int128 cts = ts;
-        RangeDev hr;
-        memset(&hr, 0, sizeof(hr));
-        fill_J0(hr.J0, cts / 6);
-        hr.e0 = (uint32_t)(cts % 6);
-        hr.n_tiles = (uint32_t)nt;
-        hr.n_words = words_for(hr.e0, nt);
-        hr.unit_words = choose_unit_words(E, f, hr.n_words, true);
-        hr.profile = (uint32_t)f.slot;
-        hr.n_range_primes = np;
-        hr.surv_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
-        hr.surv_count = d_cnt;
-        hr.surv = (uint32_t*)out_dev;
-        hr.tile_bias = (uint32_t)off;
-        const uint64_t units = units_of(f, hr.n_words, hr.unit_words);
-        uint64_t hpre[2] = {0, units};
-        SweepHeader hh;
-        memset(&hh, 0, sizeof(hh));
-        hh.n_ranges = 1;
-        hh.total_units = units;
-        CU(cudaMemcpyAsync(d_range, &hr, sizeof(hr), cudaMemcpyHostToDevice, st));
-        CU(cudaMemcpyAsync(d_prefix, hpre, sizeof(hpre), cudaMemcpyHostToDevice, st));
-        CU(cudaMemcpyAsync(d_hdr, &hh, sizeof(hh), cudaMemcpyHostToDevice, st));
+        memset(hr, 0, sizeof(RangeDev));
+        // the same placement as ccs_filter_range (plain or extended lattice)
+        const FilterSet& f = place_range(E, ts, n_tiles, *hr);
+        const uint32_t np = (uint32_t)f.hp.range_primes.size();
+        hr->prime_base = 0;
+        hr->surv_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
+        hr->surv_count = d_cnt;
+        hr->surv = (uint32_t*)out_dev;
+        hr->range_count = nullptr;
+        hr->range_id = 0;
+        hr->tile_bias = 0;
+        const uint64_t units = units_of(f, hr->n_words, hr->unit_words);
+        hpre[0] = 0;
+        hpre[1] = units;
+        memset(hh, 0, sizeof(SweepHeader));
+        hh->n_ranges = 1;
+        hh->total_units = units;
+        CU(cudaMemcpyAsync(d_range, hr, sizeof(RangeDev), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_prefix, hpre, 16, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_hdr, hh, sizeof(SweepHeader), cudaMemcpyHostToDevice, st));
         CU(launch_range_setup(d_range, d_hdr, 1, f.range_primes.p, np, d_jmod, np, st));
         uint32_t grid = (uint32_t)E->sms * E->tune.blocks_per_sm;
         const uint32_t wpb = E->tune.block_threads / 32;
         const uint64_t need = (units + wpb - 1) / wpb;
         if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
-        CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, b_stride_of((uint32_t)hp.primesB.size()),
+        CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, b_stride_of((uint32_t)f.hp.primesB.size()),
                         grid, E->tune.block_threads, st));
         E->launches += 2;
     }
-    uint32_t cnt = 0;
-    CU(cudaMemcpyAsync(&cnt, d_cnt, 4, cudaMemcpyDeviceToHost, st));
+    uint32_t* hcnt = (uint32_t*)((char*)E->h_stage + 3072);
+    CU(cudaMemcpyAsync(hcnt, d_cnt, 4, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    *n_out = cnt;
-    if (cnt > cap) return fail(CCS_OVERFLOW, "survivor capacity exceeded");
+    *n_out = *hcnt;
+    if (*hcnt > cap) return fail(CCS_OVERFLOW, "survivor capacity exceeded");
     return CCS_OK;
 }
 

@@ -172,18 +172,19 @@ ccs_status ccs_filter_range(ccs_engine* eng, uint64_t tile_start_lo, uint64_t ti
                             uint64_t* n_out, void* stream);
 
 /* ccs_filter_range without any device allocation.  No counterpart in the
- * reference.  For callers that cannot allocate device memory when they
- * filter: code inside a CUDA stream capture or a host callback, where
- * cudaMalloc is not allowed, and embedders that must fix their GPU footprint
- * at start-up.  The working memory is a 66,560-byte array compiled into
- * the library; every GPU that loads the library holds one copy until the
- * process exits.  Limit: engines with at most 16362 filter primes (larger
- * ones return CCS_ERR_INVALID); any n_tiles < 2^32.  The first call on a
- * device looks up the array's device address, so make that first call
- * before any stream capture.  Every call on a device shares the one array:
- * calls that overlap on the GPU (other streams, other threads, other
- * engines on the same device) race and must be serialised by the caller.
- * Results equal ccs_filter_range's. */
+ * reference.  For callers that may not allocate device memory once they are
+ * running: services whose GPU footprint is fixed and accounted for at
+ * start-up, allocators that refuse to grow after initialisation, and hosts
+ * that share the GPU with other tenants under a memory quota.  The working
+ * memory is a 66,560-byte array compiled into the library; every GPU that
+ * loads the library holds one copy until the process exits.  Limit: engines
+ * with at most 16362 filter primes (larger ones return CCS_ERR_INVALID); any
+ * n_tiles < 2^32.  The call is synchronous: it waits for its stream and
+ * returns the exact survivor count.  The first call on a device looks up the
+ * array's device address.  Every call on a device shares the one array:
+ * calls that overlap on the GPU (other streams, other threads, other engines
+ * on the same device) race and must be serialised by the caller.  Results
+ * equal ccs_filter_range's. */
 ccs_status ccs_filter_range_noalloc(ccs_engine* eng, uint64_t tile_start_lo, uint64_t tile_start_hi,
                                     uint64_t n_tiles, ccs_survivor* out_dev, uint64_t cap,
                                     uint64_t* n_out, void* stream);
@@ -374,6 +375,24 @@ ccs_status ccs_batch_autotune(ccs_batch* b, const ccs_range* ranges, uint32_t n_
                               ccs_batch_tuning* chosen);
 
 /* ---- diagnostics ----------------------------------------------------------- */
+
+/* How ccs_filter_range would sweep a range on this engine with its current
+ * tuning (host-only; no GPU work): the lattice chosen, the work units and
+ * the launch shape.  A work unit is 32 lines x unit_words 64-position words;
+ * the line table and line phase rows are read once per unit. */
+typedef struct {
+    uint32_t extended;        /* 1: the extended lattice (q0 absorbed into the modulus) */
+    uint32_t q0;              /* absorbed prime (1: plain lattice) */
+    uint64_t n_lines;         /* lines (residue classes) of the lattice used */
+    uint32_t n_words;         /* 64-position words each line spans */
+    uint32_t unit_words;      /* words per work unit */
+    uint64_t units;           /* work units of the launch */
+    uint32_t grid;            /* sweep blocks launched */
+    uint32_t block_threads;
+} ccs_range_plan;
+
+ccs_status ccs_plan_range(const ccs_engine* eng, uint64_t tile_start_lo, uint64_t tile_start_hi,
+                          uint64_t n_tiles, ccs_range_plan* out);
 
 /* Measured INT32 ALU issue rate of the device (tera ops/s): eight independent
  * IADD3/LOP3 chains per thread, all SMs.  The roofline denominator of the

@@ -1,8 +1,9 @@
 """The no-allocation filter entry point (ccs_filter_range_noalloc) gives the
-same survivors as ccs_filter_range.  It exists for callers that cannot
-allocate device memory at call time -- code inside a CUDA stream capture or
-a host callback, or embedders whose GPU footprint is fixed at start-up -- and
-works from a fixed array compiled into the library.  This file is collected
+same survivors as ccs_filter_range.  It exists for callers that may not
+allocate device memory once they are running -- services whose GPU footprint
+is fixed and accounted for at start-up, allocators that refuse to grow, hosts
+under a per-tenant memory quota -- and works from a fixed array compiled into
+the library.  This file is collected
 last on purpose and runs the entry point twice in a row, so it also checks
 that the array's leftover contents from the previous call do not leak into
 the next one."""
