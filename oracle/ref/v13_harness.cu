@@ -119,6 +119,73 @@ float ref13_time_filter(unsigned long long ts_lo, unsigned long long ts_hi, unsi
     return ms / reps;
 }
 
+/* d_target_bits alone (the --bits of a later batch, v13:3092) */
+int ref13_set_bits(int bits) {
+    CUDA_CHECK(cudaMemcpyToSymbol(d_target_bits, &bits, sizeof(int)));
+    return 0;
+}
+
+/* Times n_batches consecutive batches of batch_tiles tiles from ts with the
+ * reference main loop's launch sequence (v13:3764-3815): prepare_batch on the
+ * host and the residue uploads (untimed), then K1 and, with with_k2, K2 on
+ * one stream, each bracketed by CUDA events.  k1_ms / k2_ms receive the
+ * summed device times; counts = {survivors, chain records, K2 primes}. */
+int ref13_time_batches(unsigned long long ts_lo, unsigned long long ts_hi, unsigned batch_tiles,
+                       int n_batches, int blocks_per_sm, int with_k2, float* k1_ms, float* k2_ms,
+                       unsigned long long* counts) {
+    u128 ts = ((u128)ts_hi << 64) | ts_lo;
+    static u16 hl2[MAX_BASES * FILTER_PRIMES_COUNT];
+    static u16 hext[MAX_BASES * EXT_FILTER_PRIMES_COUNT];
+    static u16 hline[MAX_BASES * LINE_SIEVE_COUNT];
+    cudaDeviceProp prop;
+    CUDA_CHECK(cudaGetDeviceProperties(&prop, 0));
+    const int num_blocks = prop.multiProcessorCount * blocks_per_sm;
+    const int prove_blocks = (MAX_SURVIVORS_PER_BATCH + 255) / 256;
+    cudaEvent_t e[3];
+    for (int i = 0; i < 3; i++) cudaEventCreate(&e[i]);
+    *k1_ms = 0; *k2_ms = 0;
+    counts[0] = counts[1] = counts[2] = 0;
+    for (int bi = 0; bi < n_batches; bi++) {
+        u128 cur = ts + (u128)bi * batch_tiles;
+        prepare_batch(cur, hl2, hext, hline);
+        CUDA_CHECK(cudaMemcpy(d_batch_l2[0], hl2, h_num_bases * FILTER_PRIMES_COUNT * sizeof(u16), cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemcpy(d_batch_ext[0], hext, h_num_bases * EXT_FILTER_PRIMES_COUNT * sizeof(u16), cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemcpy(d_batch_line[0], hline, h_num_bases * LINE_SIEVE_COUNT * sizeof(u16), cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemset(d_survivor_count[0], 0, sizeof(u32)));
+        CUDA_CHECK(cudaMemset(d_chain_result_count[0], 0, sizeof(u32)));
+        CUDA_CHECK(cudaMemset(d_gpu_primes_count[0], 0, sizeof(u32)));
+        CUDA_CHECK(cudaDeviceSynchronize());
+        cudaEventRecord(e[0]);
+        cc18_filter_kernel<<<num_blocks, THREADS_PER_BLOCK>>>(
+            batch_tiles, (u32)(cur % 6),
+            d_kmod_filter, d_kmod_ext_filter, d_kM_mod_line,
+            d_ext_filter_first, d_line_kill_first,
+            d_batch_l2[0], d_batch_ext[0], d_batch_line[0],
+            d_wheel_offsets, d_wheel_start_m6, d_wheel_count_m6,
+            d_survivors[0], d_survivor_count[0]);
+        cudaEventRecord(e[1]);
+        if (with_k2)
+            cc18_prove_kernel<<<prove_blocks, 256>>>(d_survivors[0], d_survivor_count[0],
+                                                     (u64)cur, (u64)(cur >> 64), d_chain_results[0],
+                                                     d_chain_result_count[0], d_gpu_primes_count[0]);
+        cudaEventRecord(e[2]);
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaEventSynchronize(e[2]));
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, e[0], e[1]);
+        cudaEventElapsedTime(&b, e[1], e[2]);
+        *k1_ms += a;
+        *k2_ms += b;
+        u32 ns = 0, nc = 0, np = 0;
+        CUDA_CHECK(cudaMemcpy(&ns, d_survivor_count[0], sizeof(u32), cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(&nc, d_chain_result_count[0], sizeof(u32), cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(&np, d_gpu_primes_count[0], sizeof(u32), cudaMemcpyDeviceToHost));
+        counts[0] += ns; counts[1] += nc; counts[2] += np;
+    }
+    for (int i = 0; i < 3; i++) cudaEventDestroy(e[i]);
+    return 0;
+}
+
 /* K2 over survivors already placed by ref13_filter in d_survivors[0]
  * (v13:3797-3815).  Writes ChainResult records; returns their count. */
 unsigned ref13_prove_gpu(unsigned long long ts_lo, unsigned long long ts_hi,

@@ -22,9 +22,17 @@ reference itself (run in the container that holds the reference tree):
   * second_kind.json   -- the same for second-kind chains (v13b): self-test
                           vectors with GMP 2p - 1 walks and the v13b CPU
                           prover's output lines
+  * cc16_windows.json  -- the oracle's survivor sets on 64+ seeded windows of
+                          the depth-16 / primes-to-2^17 profile (W = 31#,
+                          88-bit roots) holding at least 300 survivors in
+                          total; no reference engine takes stage primes up to
+                          2^17, so these pin the GPU filter to the oracle,
+                          whose per-candidate test is itself pinned to the
+                          reference's counters and kernels at 37..863
 
-Usage: python tests/golden/make_golden.py [--second-kind]   (needs oracle/_ref
-built by `make -C oracle`).
+Usage: python tests/golden/make_golden.py [--second-kind | --cc16-windows]
+(the reference fixtures need oracle/_ref built by `make -C oracle` and the
+reference tree in $CCS_REFERENCE_DIR).
 """
 import json
 import os
@@ -40,7 +48,17 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 import oracle_bind as ob  # noqa: E402
 
-REF = "/root/reference"
+
+
+def reference_dir():
+    """The reference tree: $CCS_REFERENCE_DIR, else a directory named
+    `reference` beside this repository."""
+    d = os.environ.get("CCS_REFERENCE_DIR") or os.path.join(
+        os.path.dirname(os.path.dirname(HERE)), "..", "reference")
+    d = os.path.abspath(d)
+    if not os.path.isdir(os.path.join(d, "src")):
+        sys.exit(f"reference tree not found at {d}: set CCS_REFERENCE_DIR")
+    return d
 
 
 def dump(name, obj):
@@ -74,7 +92,7 @@ def main():
 
     # ---- data sample -----------------------------------------------------
     rows = []
-    with open(os.path.join(REF, "data/sample/cc10plus_roots_sample_1000.txt")) as f:
+    with open(os.path.join(reference_dir(), "data/sample/cc10plus_roots_sample_1000.txt")) as f:
         for line in f:
             parts = line.split()
             if len(parts) >= 2 and parts[1].startswith("0x"):
@@ -193,7 +211,7 @@ def second_kind():
     r33 = ob.ref33()
     r13b = ob.ref13b()
     assert r33 is not None and r13b is not None, "build oracle/_ref first (make -C oracle)"
-    src = open(os.path.join(REF, "src/cuda/cc18_filter_cuda_CpC_v13b.cu")).read()
+    src = open(os.path.join(reference_dir(), "src/cuda/cc18_filter_cuda_CpC_v13b.cu")).read()
     table = src[src.index("Known second-kind Cunningham chain test vectors"):]
     table = table[:table.index("};")]
     vecs = re.findall(r'\{\s*"(\d+)",\s*(\d+),', table)
@@ -223,13 +241,60 @@ def second_kind():
                               "chains": known, "prover": prover})
 
 
+CC16_WINDOW_TILES = 16384
+
+
+def _cc16_window(args):
+    """Oracle survivors of one window (runs in a spawned worker)."""
+    ts, n = args
+    lat = ob.Lattice(lattice_len=16, depth=16, stages=cc16_stages())
+    surv = lat.filter_range(ts, n)
+    return sorted(map(tuple, surv[:, :3].astype(np.int64).tolist()))
+
+
+def cc16_stages():
+    """Stage primes 37..2^10 / 2^10..2^14 / 2^14..2^17 at chain positions 0..15."""
+    return [(ob.primes_between(37, 1 << 10), 0), (ob.primes_between(1 << 10, 1 << 14), 0),
+            (ob.primes_between(1 << 14, 1 << 17), 0)]
+
+
+def cc16_windows(min_windows=64, min_survivors=300):
+    """cc16_windows.json: seeded 2^14-tile windows spread over the 88-bit tile
+    range of the depth-16 profile, filtered by the oracle on every core, until
+    at least min_windows windows and min_survivors survivors are collected."""
+    import multiprocessing as mp
+    lat = ob.Lattice(lattice_len=16, depth=16, stages=cc16_stages())
+    M, WP = lat.M, lat.WP
+    bases = lat.bases()
+    t_lo = -(-((1 << 87) - max(bases)) // (M * WP))
+    t_hi = ((1 << 88) - 1) // (M * WP) - CC16_WINDOW_TILES
+    rw = random.Random(16172026)
+    windows, total = [], 0
+    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        while len(windows) < min_windows or total < min_survivors:
+            batch = [(rw.randint(t_lo, t_hi), CC16_WINDOW_TILES) for _ in range(16)]
+            for (ts, n), surv in zip(batch, pool.map(_cc16_window, batch)):
+                windows.append({"tile_start": str(ts), "n_tiles": n, "survivors": surv})
+                total += len(surv)
+            print(f"{len(windows)} windows, {total} survivors", flush=True)
+    dump("cc16_windows.json", {
+        "source": "oracle orc_filter_range (per-candidate restatement of v13:1551-1714 / "
+                  "v33:1795-1960) on the depth-16 profile",
+        "profile": {"target": 16, "depth": 16, "bits": 88, "crt": ob.CRT_PRIMES,
+                    "wheel": ob.WHEEL_PRIMES,
+                    "stages": "primes 37..2^10 / 2^10..2^14 / 2^14..2^17, positions 0..15"},
+        "candidates_per_tile": 73008, "total_survivors": total, "windows": windows})
+
+
 def C_buf():
     import ctypes as C
     return C.create_string_buffer(256)
 
 
 if __name__ == "__main__":
-    if "--second-kind" in sys.argv:
+    if "--cc16-windows" in sys.argv:
+        cc16_windows()
+    elif "--second-kind" in sys.argv:
         second_kind()
     else:
         main()
