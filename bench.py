@@ -98,6 +98,16 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def cpu_model():
+    """lscpu model name of this host (the CPU baselines' hardware)."""
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        m = re.search(r"Model name:\s*(.+)", out)
+        return m.group(1).strip() if m else None
+    except (OSError, subprocess.SubprocessError):
+        return None
+
+
 def v33_sample(bits, target, seconds_goal=15.0):
     """Runs the reference CPU engine (sieve only) on a sequential prefix range
     sized for about seconds_goal on this host.  Returns the parsed figures."""
@@ -205,9 +215,10 @@ def _gmp_walk_worker(hexes):
 
 def gmp_walk_baseline(roots, seconds_goal=10.0):
     """Proofs/s of the reference GMP prover walk on all host cores over a
-    bounded sample of the prove-batch roots."""
+    bounded sample (the first n) of the prove-batch roots.  Returns the
+    baseline dict and the GMP chain lengths of the sample, in order."""
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref33.so")):
-        return None
+        return None, None
     import multiprocessing as mp
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
@@ -217,18 +228,18 @@ def gmp_walk_baseline(roots, seconds_goal=10.0):
     _gmp_walk_worker(hexes[:200])
     per = (time.time() - t0) / 200
     n = int(min(len(hexes), max(cores * 200, seconds_goal * cores / max(per, 1e-7))))
-    if n > len(hexes):
-        n = len(hexes)
-    chunks = [hexes[i::cores] for i in range(cores)]
-    chunks = [c[: n // cores + 1] for c in chunks]
+    step = -(-n // cores)
+    chunks = [hexes[i:min(n, i + step)] for i in range(0, n, step)]
     with ctx.Pool(cores) as pool:
         t0 = time.time()
         res = pool.map(_gmp_walk_worker, chunks)
         dt = time.time() - t0
-    done = sum(len(c) for c in chunks)
-    return {"value": done / dt, "unit": "roots/s", "cores": cores, "kind": "reference",
-            "sample": f"{done} prove-batch roots walked with GMP mpz_probab_prime_p(.,1) "
-                      f"(the reference CPU prover's walk, v13:1870-1881) in {dt:.1f} s"}
+    lengths = [x for part in res for x in part]
+    return ({"value": n / dt, "unit": "roots/s", "cores": cores, "kind": "reference",
+             "cpu_model": cpu_model(),
+             "sample": f"{n} prove-batch roots walked with GMP mpz_probab_prime_p(.,1) "
+                       f"(the reference CPU prover's walk, v13:1870-1881) in {dt:.1f} s"},
+            lengths)
 
 
 def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
@@ -280,7 +291,11 @@ def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
     # IMAD ops: one lo/hi pair per 32x32-bit word product, counted on the device
     ops_per_mm = 2.0 * words / max(mm, 1)
     achieved = 2.0 * words / (ms * 1e-3) / 1e12
-    cpu = gmp_walk_baseline(roots[:20000])
+    cpu, gmp_len = gmp_walk_baseline(roots[:20000])
+    walk_mm = None
+    if gmp_len is not None:
+        walk_mm = {"compared": len(gmp_len),
+                   "mismatches": int(sum(int(a) != int(b) for a, b in zip(L[:len(gmp_len)], gmp_len)))}
     return {"workload": f"{total} roots (= {copies} x {n_unique} distinct), 80..110-bit, pre-filtered "
                         "by all primes < 2^17 at positions 0..15, BPSW walk",
             "roots_per_s": total / (ms * 1e-3), "primality_tests_per_s": tests / (ms * 1e-3),
@@ -292,7 +307,7 @@ def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
                          "work": f"{ops_per_mm:.1f} IMAD ops per Montgomery product (2 per word product, "
                                  "2NL^2+NL word products per CIOS product)",
                          "peak_source": "measured: ccs_measure_imad_peak"},
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu, "walk_vs_gmp": walk_mm}
 
 
 def autotune_engines(ccs, engines, seed):
@@ -311,17 +326,70 @@ def autotune_engines(ccs, engines, seed):
     return {"seconds": time.time() - t0, "engines": out}
 
 
+def _ref_gpu_lib(name):
+    """The reference's own engine harness (built from its sources into
+    oracle/_ref by oracle/Makefile) with its batch timer bound, or None."""
+    import ctypes as C
+    path = os.path.join(ROOT, "oracle", "_ref", f"lib{name}.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    fn = getattr(lib, f"{name}_time_batches")
+    fn.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_uint, C.c_int, C.c_int, C.c_int,
+                   C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_ulonglong)]
+    return lib
+
+
+def reference_gpu_batches(name, target, depth, plan, tiles, batch_tiles, blocks_per_sm, prove_forward):
+    """The reference's cc18_filter_kernel (K1) and cc18_prove_kernel (K2) on
+    the same tiles, launched as its main loop launches them: batches of
+    batch_tiles (its --batch), SMs x blocks_per_sm blocks of 256 (its
+    --blocks-per-sm), K2 over the fixed 2^20-survivor grid; device time of
+    each kernel from CUDA events."""
+    import ctypes as C
+    lib = _ref_gpu_lib(name)
+    if lib is None:
+        return None
+    getattr(lib, f"{name}_setup")(target, depth)
+    if name == "ref15":
+        lib.ref15_upload(depth, plan[0][0], target, prove_forward)
+    else:
+        lib.ref13_upload(depth, plan[0][0])
+    set_bits = getattr(lib, f"{name}_set_bits")
+    timer = getattr(lib, f"{name}_time_batches")
+    k1 = k2 = 0.0
+    tot = [0, 0, 0]
+    nb = tiles // batch_tiles
+    for i, (bits, ts) in enumerate(plan):
+        set_bits(bits)
+        a, b = C.c_float(0), C.c_float(0)
+        cnt = (C.c_ulonglong * 3)()
+        timer(ts & (2**64 - 1), ts >> 64, batch_tiles, 1 if i == 0 else nb, blocks_per_sm, 1,
+              C.byref(a), C.byref(b), cnt)
+        if i == 0:
+            continue                                   # warm-up batch
+        k1 += a.value
+        k2 += b.value
+        for j in range(3):
+            tot[j] += cnt[j]
+    return {"k1_ms": k1, "k2_ms": k2, "survivors": tot[0], "chains": tot[1], "primes": tot[2],
+            "batch_tiles": batch_tiles, "blocks_per_sm": blocks_per_sm}
+
+
 def section_reference_runs(ccs, torch, dev, local, tiles=1 << 22, steps=4):
-    """The reference's own GPU run configurations on this engine: v13
-    defaults (target = depth = 18, 89-bit roots, K2 roots-only prove with the
-    v13 witnesses) and the v15 CC19 configuration (target = depth = 19, 88-107
-    bit shells, reverse prove order), filter + prove per 2^22-tile batch,
-    device-timed on the engine stream."""
+    """The reference's own GPU run configurations, on this engine and on the
+    reference's own kernels over the same tiles: v13 defaults (target =
+    depth = 18, 89-bit roots, K2 roots-only prove with the v13 witnesses,
+    12 blocks/SM) and the v15 CC19 configuration (target = depth = 19, 88-107
+    bit shells, reverse prove order, --batch 524288, 16 blocks/SM); filter +
+    prove per 2^22 tiles, device-timed.  Survivor, chain and prime counts of
+    the two engines are compared tile for tile."""
     import random
     out = {}
-    for name, kw, bits_list in [
-            ("v13_defaults_cc18", dict(target=18, bits=89), [89]),
-            ("v15_cc19_reverse", dict(target=19, depth=19, reverse_prove=True), list(range(88, 108)))]:
+    for name, ref, kw, bits_list, ref_bps in [
+            ("v13_defaults_cc18", "ref13", dict(target=18, bits=89), [89], 12),
+            ("v15_cc19_reverse", "ref15", dict(target=19, depth=19, reverse_prove=True),
+             list(range(88, 108)), 16)]:
         eng = ccs.Engine(device=local, primality=ccs.PRIME_MR, prove_mode=ccs.PROVE_ROOTS, **kw)
         info = eng.info
         bases = eng.bases()
@@ -334,28 +402,46 @@ def section_reference_runs(ccs, torch, dev, local, tiles=1 << 22, steps=4):
             bits = bits_list[i % len(bits_list)]
             lo, hi = ccs.bit_tile_range(bits, bases, info["lattice_m"], info["wheel_period"])
             plan.append((bits, r.randint(lo, hi - tiles - 1)))
-        ms = 0.0
+        ms = f_ms = 0.0
         n_s = n_c = n_p = 0
         for i, (bits, ts) in enumerate(plan):
             eng.set_bits(bits)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             torch.cuda.synchronize()
             e0.record(stream)
             s_ = eng.filter_range(ts, tiles, out=surv, stream=stream)
-            c_, p_ = eng.prove(s_, ts, out=chains, stream=stream)
             e1.record(stream)
+            c_, p_ = eng.prove(s_, ts, out=chains, stream=stream)
+            e2.record(stream)
             torch.cuda.synchronize()
             if i == 0:
                 continue                                   # warm-up batch
-            ms += e0.elapsed_time(e1)
+            ms += e0.elapsed_time(e2)
+            f_ms += e0.elapsed_time(e1)
             n_s += s_.shape[0]
             n_c += c_.shape[0]
             n_p += p_
-        cand = steps * tiles * info["candidates_per_tile"]
-        out[name] = {"candidates_per_s": cand / (ms * 1e-3), "survivors": n_s, "chains": n_c,
-                     "primes": n_p, "ms": ms, "tiles_per_batch": tiles, "batches": steps,
-                     "candidates_per_tile": info["candidates_per_tile"]}
         eng.close()
+        cand = steps * tiles * info["candidates_per_tile"]
+        res = {"candidates_per_s": cand / (ms * 1e-3), "filter_candidates_per_s": cand / (f_ms * 1e-3),
+               "survivors": n_s, "chains": n_c, "primes": n_p, "ms": ms, "filter_ms": f_ms,
+               "tiles_per_batch": tiles, "batches": steps,
+               "candidates_per_tile": info["candidates_per_tile"]}
+        try:
+            rg = reference_gpu_batches(ref, kw["target"], kw.get("depth", kw["target"]), plan, tiles,
+                                       524288, ref_bps, 0 if kw.get("reverse_prove") else 1)
+        except Exception as ex:
+            rg = {"error": repr(ex)}
+        if rg and "k1_ms" in rg:
+            rg["k1_candidates_per_s"] = cand / (rg["k1_ms"] * 1e-3)
+            rg["k1k2_candidates_per_s"] = cand / ((rg["k1_ms"] + rg["k2_ms"]) * 1e-3)
+            rg["ours_over_ref_k1"] = res["filter_candidates_per_s"] / rg["k1_candidates_per_s"]
+            rg["ours_over_ref_k1k2"] = res["candidates_per_s"] / rg["k1k2_candidates_per_s"]
+            rg["count_mismatches"] = {"survivors": abs(rg["survivors"] - n_s),
+                                      "chains": abs(rg["chains"] - n_c),
+                                      "primes": abs(rg["primes"] - n_p)}
+        res["reference_kernels"] = rg
+        out[name] = res
     return out
 
 
@@ -415,6 +501,45 @@ def section_qiter(ccs, torch, dev, local, steps=8, segs_per_step=256):
             "qv_per_s_e2e": qv / e2e_s, "filter_ms": f_ms, "prove_ms": p_ms, "survivors": n_s,
             "chains": n_c, "primes": n_p, "hit_lines_len10": len(hits),
             "unit": "(Q, variant) pairs/s, the reference's G(Q,V)/s x 1e9"}
+
+
+def record_set(rec, words):
+    """Sorted tuples of the first `words` 32-bit words of survivor (16-byte)
+    or chain (48-byte) records: a numpy structured array, an int32 tensor or
+    an ndarray.  Survivors compare on 3 words (base, k, tile), chains on 11
+    (ChainResult words, root limbs, flags; not the survivor index)."""
+    import numpy as np
+    if hasattr(rec, "cpu"):
+        rec = rec.cpu().numpy()
+    a = np.ascontiguousarray(rec)
+    if len(a) == 0:
+        return []
+    a = a.view(np.uint32).reshape(len(a), -1)[:, :words].astype(np.int64)
+    return sorted(map(tuple, a.tolist()))
+
+
+def batched_rerun(ccs, eng, starts, sets, tiles, bits):
+    """Re-runs ranges already filtered and proved by the plain path through
+    one ccs_batch_run and counts the ranges whose survivor set, chain set or
+    prime count differ."""
+    import numpy as np
+    batch = ccs.Batch([eng], len(starts), surv_cap=1 << 21, chain_cap=1 << 18)
+    try:
+        res, bs, bc = batch.run([(t, tiles, 0, bits) for t in starts])
+    finally:
+        batch.close()
+    rid = bs["_pad"].astype(np.int64)
+    crid = rid[bc["survivor"].astype(np.int64)] if len(bc) else np.zeros(0, dtype=np.int64)
+    bad = 0
+    for i, (sv, ch, p) in enumerate(sets):
+        same = (record_set(bs[rid == i], 3) == record_set(sv, 3)
+                and record_set(bc[crid == i], 11) == record_set(ch, 11)
+                and res[i]["n_primes"] == p)
+        bad += not same
+    return {"ranges": len(starts), "tiles_per_range": tiles,
+            "survivors": int(sum(r["n_survivors"] for r in res)),
+            "chains": int(sum(r["n_chains"] for r in res)),
+            "ranges_differing": int(bad)}
 
 
 def section_batched(ccs, engines, n_ranges=4096):
@@ -486,9 +611,11 @@ def section_served(ccs, engines, n_req=2048, lam=2000.0, batch_tuning=None):
     th.join()
     lat = []
     first, last = 1e30, 0
+    served_sets = []
     for rid in ids:
         srv.wait(rid)
-        st, res, _, _ = srv.poll(rid, surv_cap=1 << 16, chain_cap=1 << 12)
+        st, res, sv, ch = srv.poll(rid, surv_cap=1 << 16, chain_cap=1 << 14)
+        served_sets.append((record_set(sv, 3), record_set(ch, 11)))
         lat.append(res["done_s"] - res["submit_s"])
         first = min(first, res["submit_s"])
         last = max(last, res["done_s"])
@@ -501,6 +628,7 @@ def section_served(ccs, engines, n_req=2048, lam=2000.0, batch_tuning=None):
 
     # plain: one request at a time in arrival order
     lat_p = []
+    plain_sets = []
     base = time.monotonic() + 0.05
     t_first = base + arr[0]
     for i, (ts, nt, p, bits) in enumerate(ranges):
@@ -510,14 +638,76 @@ def section_served(ccs, engines, n_req=2048, lam=2000.0, batch_tuning=None):
         e = engines[p]
         e.set_bits(bits)
         s = e.filter_range(ts, nt, cap=1 << 20)
-        e.prove(s, ts)
+        c, _ = e.prove(s, ts, cap=1 << 14)
         lat_p.append(time.monotonic() - (base + arr[i]))
+        plain_sets.append((s.cpu(), c.cpu()))
     t_last = time.monotonic()
+    mism = sum(served_sets[i] != (record_set(a, 3), record_set(b, 11))
+               for i, (a, b) in enumerate(plain_sets))
     plain = {"p50_s": float(np.percentile(lat_p, 50)), "p99_s": float(np.percentile(lat_p, 99)),
              "candidates_per_s": cand_total / (t_last - t_first), "makespan_s": t_last - t_first}
     return {"workload": f"{n_req} requests, Poisson arrivals {lam:.0f}/s, log-uniform 2^20..2^34 "
                         "candidates, depth 14..19, width 64..110 bits, admission cap 120 GB",
-            "offered_candidates_per_s": cand_total / arr[-1], "served": served, "plain": plain}
+            "offered_candidates_per_s": cand_total / arr[-1], "served": served, "plain": plain,
+            "requests_differing_from_plain": int(mism)}
+
+
+SWEEP_PROFILE = os.path.join(ROOT, "profiles", "sweep_kernel_cc16_4M_tiles.md")
+
+
+def profile_figures(path):
+    """Per-unit figures of an ncu summary under profiles/: the line starting
+    with `bench-figures:` holds a JSON object."""
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("bench-figures:"):
+                    return json.loads(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def sweep_roofline(ccs, device, plan, candidates, ms, clk, int_peak, ref_ops_per_candidate):
+    """Roofline of the dominant kernel (sweep_kernel) for one headline launch.
+
+    The kernel is bound by instruction issue: every SM sub-partition issues
+    at most one warp instruction per cycle, so the peak is SMs x 4 x the SM
+    clock sampled during the timed region.  Achieved = warp instructions of
+    the launch / its CUDA-event duration, with warp instructions per
+    candidate from the ncu summary of the same kernel and profile
+    (smsp__inst_executed.sum on a smaller launch of the current code).
+    traffic = that summary's DRAM bytes per work unit x the launch's units.
+    The reference's per-candidate test costs 4 x E[tests] INT32 operations;
+    candidates/s x that over the measured INT32 peak is reported separately
+    as the algorithmic gain over the reference's test, not as a roofline."""
+    import torch
+    fig = profile_figures(SWEEP_PROFILE) or {}
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+    out = {"bound": "issue", "unit": "warp instructions/s",
+           "kernel": "sweep_kernel", "launch_ms": ms, "candidates_per_launch": candidates,
+           "plan": plan, "peak_source": f"{sms} SMs x 4 issue slots x median sampled SM clock "
+                                        f"({mhz} MHz)",
+           "figures_source": os.path.relpath(SWEEP_PROFILE, ROOT)}
+    ipc = fig.get("warp_inst_per_candidate")
+    if mhz and ipc:
+        peak = sms * 4 * mhz * 1e6
+        ach = ipc * candidates / (ms * 1e-3)
+        out.update({"achieved": ach, "peak": peak, "frac": ach / peak,
+                    "warp_inst_per_candidate": ipc})
+    else:
+        out.update({"achieved": None, "peak": None, "frac": None})
+    bpu = fig.get("dram_bytes_per_unit")
+    out["traffic"] = bpu * plan["units"] if bpu else None
+    out["algorithmic_gain_vs_reference_test"] = {
+        "ops_per_candidate": ref_ops_per_candidate,
+        "tops_equivalent": candidates * ref_ops_per_candidate / (ms * 1e-3) / 1e12,
+        "int32_peak_tops": int_peak,
+        "ratio": candidates * ref_ops_per_candidate / (ms * 1e-3) / 1e12 / int_peak,
+        "note": "4 x E[tests] INT32 ops per candidate is the reference's per-candidate test; "
+                "the bit-sliced sweep does far fewer operations per candidate"}
+    return out
 
 
 def run_ours(args):
@@ -585,6 +775,7 @@ def run_ours(args):
     n_surv = n_chain = n_prime = 0
     torch.cuda.synchronize()
     t_wall = time.time()
+    step_starts, step_sets = [], []
     for i in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()                      # L2 flush between timed steps (not timed)
@@ -594,6 +785,9 @@ def run_ours(args):
         n_surv += s
         n_chain += c
         n_prime += p
+        # this step's records, kept for the batched re-run (after the events)
+        step_starts.append(ts)
+        step_sets.append((surv_buf[:s].cpu(), chain_buf[:c].cpu(), p))
         ts += TILES
     torch.cuda.synchronize()
     t_wall = time.time() - t_wall
@@ -618,20 +812,8 @@ def run_ours(args):
     filt_ms = ev0.elapsed_time(ev1)
     int_peak = ccs.measure_int32_peak(local)
     E = info["expected_tests"]
-    # DRAM traffic per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum
-    # of a 2^22-tile launch of this profile on the extended lattice (158.1 MB
-    # for 287,469 work units = one per 32-line group), scaled by the work units
-    # of this launch (the line table is read once per unit)
-    tune_now = eng.tuning()
-    span = (TILES + 5) // 6 + 1
-    n_words = ((span + 36) // 37 + 63) // 64
-    traffic, traffic_note = None, None
-    if n_words >= tune_now["ext_min_words"]:
-        chunks = -(-n_words // max(1, min(tune_now["unit_words"], n_words)))
-        traffic = 158.1e6 * chunks
-        traffic_note = (f"ncu DRAM bytes of a 2^22-tile launch (158.1 MB, one unit per line group) "
-                        f"x {chunks} units per group at {TILES} tiles")
-    achieved = cand_step * 4.0 * E / (filt_ms * 1e-3) / 1e12
+    plan = eng.plan_range(ts, TILES)
+    roofline = sweep_roofline(ccs, local, plan, cand_step, filt_ms, clk, int_peak, 4.0 * E)
 
     # end to end through the host-buffer C-ABI call (copies inside)
     e2e_steps = max(1, min(args.steps, 3))
@@ -646,6 +828,15 @@ def run_ours(args):
         ts += TILES
     e2e_s = time.time() - t0
     e2e_value = ws * e2e_steps * cand_step / e2e_s
+
+    # the timed tiles again through the batched executor (one persistent
+    # launch over all steps' ranges): survivor and chain sets must be equal
+    headline_mm = None
+    if not args.headline_only:
+        try:
+            headline_mm = batched_rerun(ccs, eng, step_starts, step_sets, TILES, BITS)
+        except Exception as ex:
+            headline_mm = {"error": repr(ex)}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -699,13 +890,7 @@ def run_ours(args):
                        "parallelism": f"lanes{ws}", "tuning": eng.tuning(), "autotune": tune_report},
             "survivors": n_surv, "chains": n_chain, "primes": n_prime,
             "survivor_rate": n_surv / (args.steps * cand_step),
-            "roofline": {"bound": "int32", "achieved": achieved, "peak": int_peak, "unit": "TOPS",
-                         "frac": achieved / int_peak, "traffic": traffic,
-                         "traffic_source": traffic_note,
-                         "kernel": "sweep_kernel (+ range setup, deferred stage)",
-                         "work_per_candidate": f"4 x E[tests] = {4 * E:.3f} int32 ops",
-                         "filter_ms_per_launch_group": filt_ms,
-                         "peak_source": "measured: ccs_measure_int32_peak (IADD3/LOP3 chains)"},
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "candidates/s", "h2d_bytes_per_step": h2d // e2e_steps,
@@ -714,6 +899,15 @@ def run_ours(args):
             "wall_s_timed": t_wall,
         }
         line.update(extra)
+        mm = {"headline_batched": headline_mm}
+        pv = extra.get("prove", {})
+        mm["walk_vs_gmp"] = pv.get("walk_vs_gmp") if isinstance(pv, dict) else None
+        sv = extra.get("served", {})
+        mm["served_vs_plain"] = sv.get("requests_differing_from_plain") if isinstance(sv, dict) else None
+        rr = extra.get("reference_runs", {})
+        mm["reference_kernels"] = {k: (v.get("reference_kernels") or {}).get("count_mismatches")
+                                   for k, v in rr.items() if isinstance(v, dict)} if isinstance(rr, dict) else None
+        line["mismatches"] = mm
         print(json.dumps(line))
     if pg:
         pg.barrier()
