@@ -31,9 +31,9 @@ constexpr uint32_t kTLimit = 211;
 constexpr int kPatTMax = 224;          // pattern-table words of the table-window primes
 constexpr double kTAdmit = 0.18;       // table-window admission (level-A survivors per 64 positions)
 
-// Pattern words of a table-window prime: a 64-bit window at any phase < q
-// lies inside them.
-constexpr uint32_t t_words(uint32_t q) { return (q - 1) / 32 + 3; }
+// Pattern words of a table-window prime: a 128-bit window (two 64-position
+// words, the sweep's step) at any phase < q lies inside them.
+constexpr uint32_t t_words(uint32_t q) { return (q - 1) / 32 + 5; }
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
 constexpr int kLevelBRound = 4;        // level-B primes tested per lane per round

@@ -109,9 +109,13 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
                                const uint32_t* primes, uint32_t max_primes, uint32_t* jmod,
                                uint32_t stride, cudaStream_t st);
 size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride);
+// lowreg: the register-capped variant (needed for more than the default
+// variant's resident blocks; sweep_needs_lowreg tells)
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
-                         uint32_t b_stride, uint32_t grid, uint32_t block_threads, cudaStream_t st);
+                         uint32_t b_stride, uint32_t grid, uint32_t block_threads, bool lowreg,
+                         cudaStream_t st);
+bool sweep_needs_lowreg(uint32_t b_stride, uint32_t block_threads, uint32_t blocks_per_sm);
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
 // breadth-first chain walk (prove.cu)
 struct WalkItem {

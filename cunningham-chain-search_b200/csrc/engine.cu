@@ -629,9 +629,10 @@ static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_t
     const uint32_t wpb = E->tune.block_threads / 32;
     uint64_t need = (units + wpb - 1) / wpb;
     if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
+    const uint32_t bs = b_stride_of((uint32_t)hp.primesB.size());
     CU(launch_sweep(E->d_range.p, E->d_prefix.p, E->d_hdr.p, E->d_jmod.p,
-                    (uint32_t)hp.range_primes.size(), b_stride_of((uint32_t)hp.primesB.size()),
-                    grid, E->tune.block_threads, st));
+                    (uint32_t)hp.range_primes.size(), bs, grid, E->tune.block_threads,
+                    sweep_needs_lowreg(bs, E->tune.block_threads, E->tune.blocks_per_sm), st));
     return CCS_OK;
 }
 
@@ -1155,8 +1156,9 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
         const uint32_t wpb = E->tune.block_threads / 32;
         const uint64_t need = (units + wpb - 1) / wpb;
         if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
-        CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, b_stride_of((uint32_t)f.hp.primesB.size()),
-                        grid, E->tune.block_threads, st));
+        const uint32_t bs = b_stride_of((uint32_t)f.hp.primesB.size());
+        CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, bs, grid, E->tune.block_threads,
+                        sweep_needs_lowreg(bs, E->tune.block_threads, E->tune.blocks_per_sm), st));
         E->launches += 2;
     }
     uint32_t* hcnt = (uint32_t*)((char*)E->h_stage + 3072);
@@ -1431,6 +1433,7 @@ static ccs_status batch_capture(ccs_batch* b) {
     b->blocks_per_sm = (b->req_blocks_per_sm == 0 || b->req_blocks_per_sm > (uint32_t)mx)
                            ? (uint32_t)mx : b->req_blocks_per_sm;
     b->grid = (uint32_t)b->prof[0]->sms * b->blocks_per_sm;
+    const bool lowreg = sweep_needs_lowreg(b->b_stride, bt, b->blocks_per_sm);
     const uint32_t max_ranges = b->max_ranges;
     const size_t nc = b->nc;
     cudaStream_t st = b->stream;
@@ -1443,7 +1446,7 @@ static ccs_status batch_capture(ccs_batch* b) {
     launch_range_setup(b->d_ranges.p, b->d_hdr.p, max_ranges, b->d_primes.p, b->max_range_primes,
                        b->d_jmod.p, b->jstride, st);
     launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, b->b_stride,
-                 b->grid, bt, st);
+                 b->grid, bt, lowreg, st);
     ProveArgs pa;
     pa.ranges = b->d_pranges.p;
     pa.surv = b->d_surv.p;
@@ -1624,8 +1627,10 @@ ccs_status ccs_batch_autotune(ccs_batch* b, const ccs_range* ranges, uint32_t n_
         if (s != CCS_OK) return s;
     }
     const uint32_t uw_best = best.unit_words;
-    const uint32_t shapes[5][2] = {{256, 1}, {256, 2}, {128, 2}, {128, 3}, {128, 4}};
+    // 3 x 256 and 5-6 x 128 run the register-capped sweep variant
+    const uint32_t shapes[8][2] = {{256, 1}, {256, 2}, {256, 3}, {128, 2}, {128, 3}, {128, 4}, {128, 5}, {128, 6}};
     for (const auto& sh : shapes) {
+        if (sh[1] > (uint32_t)sweep_blocks_per_sm(b->b_stride, sh[0])) continue;
         ccs_status s = measure(ccs_batch_tuning{sh[0], sh[1], uw_best, 0u});
         if (s != CCS_OK) return s;
     }

@@ -387,7 +387,8 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         B.pi = 0;
         __syncwarp();
 
-        uint64_t mrem = 0;          // positions of word wbm not yet queued
+        // positions of words wbm / wbm + 64 (relative to jbase) not yet queued
+        uint64_t ma = 0, mb = 0;
         uint32_t wbm = 0;
         uint32_t w = w0;            // next word to sweep
         for (;;) {
@@ -414,29 +415,36 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                 }
             }
             for (;;) {
-                if (!__any_sync(kFull, mrem != 0)) {
+                if (!__any_sync(kFull, (ma | mb) != 0)) {
                     if (w >= w1) break;
-                    uint64_t kill = 0;
+                    // two words per step: kill words ka (word w) and kb (w + 1)
+                    uint64_t ka = 0, kb = 0;
 #pragma unroll
                     for (int i = 0; i < kNumA1; i++) {
                         if (STD && i >= kStdA1[STD]) continue;       // dummy slots of the standard sets
                         const uint32_t q = STD ? kStdQ[STD][i] : P.A[i].q;
-                        const uint32_t s = STD ? (64u % q) : P.A[i].s;
-                        const uint32_t t = STD ? (q - 64u % q) : P.A[i].t;
+                        const uint32_t s1 = STD ? (64u % q) : P.A[i].s;
+                        const uint32_t t1 = STD ? (q - 64u % q) : P.A[i].t;
+                        // 128 mod q < q < 64: the same shift rule over two words
+                        const uint32_t s2 = STD ? (128u % q) : (s1 + s1 >= q ? s1 + s1 - q : s1 + s1);
+                        const uint32_t t2 = q - s2;
                         const uint64_t W = A1w[i];
-                        kill |= W;
-                        A1w[i] = (W >> s) | (W << t);
+                        ka |= W;
+                        kb |= (W >> s1) | (W << t1);
+                        A1w[i] = (W >> s2) | (W << t2);
                     }
 #pragma unroll
                     for (int i = 0; i < kNumA2; i++) {
                         const uint32_t t = STD ? (kStdQ[STD][kNumA1 + i] - 64u) : P.A[kNumA1 + i].t;
-                        const uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
-                        kill |= ((uint64_t)o1 << 32) | o0;
-                        A2w[i][0] = o2 | (o0 << t);
-                        A2w[i][1] = __funnelshift_l(o0, o1, t);
-                        A2w[i][2] = __funnelshift_l(o1, o2, t);
+                        uint32_t o0 = A2w[i][0], o1 = A2w[i][1], o2 = A2w[i][2];
+                        ka |= ((uint64_t)o1 << 32) | o0;
+                        uint32_t p0 = o2 | (o0 << t), p1 = __funnelshift_l(o0, o1, t), p2 = __funnelshift_l(o1, o2, t);
+                        kb |= ((uint64_t)p1 << 32) | p0;
+                        A2w[i][0] = p2 | (p0 << t);
+                        A2w[i][1] = __funnelshift_l(p0, p1, t);
+                        A2w[i][2] = __funnelshift_l(p1, p2, t);
                     }
-                    // table windows: 64 pattern bits from the phase, phase += 64 mod q
+                    // table windows: 128 pattern bits from the phase, phase += 128 mod q
 #pragma unroll
                     for (int i = 0; i < kNumT; i++) {
                         if (STD && i >= kStdNT[STD]) continue;
@@ -445,26 +453,41 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                         const uint32_t ph = Tph[i];
                         const uint32_t* pt = PT + toff + (ph >> 5);
                         const uint32_t b = ph & 31;
-                        const uint32_t x0 = pt[0], x1 = pt[1], x2 = pt[2];
-                        kill |= ((uint64_t)__funnelshift_r(x1, x2, b) << 32) | __funnelshift_r(x0, x1, b);
-                        uint32_t nx = min(ph + 64u, ph + 64u - q);
+                        const uint32_t x0 = pt[0], x1 = pt[1], x2 = pt[2], x3 = pt[3], x4 = pt[4];
+                        ka |= ((uint64_t)__funnelshift_r(x1, x2, b) << 32) | __funnelshift_r(x0, x1, b);
+                        kb |= ((uint64_t)__funnelshift_r(x3, x4, b) << 32) | __funnelshift_r(x2, x3, b);
+                        // ph + 128 < 3q for the table primes (q > 96); one
+                        // subtraction suffices from q = 128 on
+                        uint32_t nx = min(ph + 128u, ph + 128u - q);
+                        if (!STD || q < 128u) nx = min(nx, nx - q);
                         if (!STD) nx = q > 1 ? nx : 0u;
                         Tph[i] = nx;
                     }
-                    // positions of this word inside [jlo, jhi)
+                    // positions of words w, w + 1 inside [jlo, jhi) and this unit
                     const uint32_t wb = w * 64;
-                    uint64_t valid = 0;
-                    if (jhi > wb && jlo < wb + 64) {
-                        const uint32_t lo = jlo > wb ? jlo - wb : 0;
-                        const uint32_t hi = jhi - wb < 64 ? jhi - wb : 64;
-                        valid = (hi >= 64 ? ~0ull : ((1ull << hi) - 1)) & ~((1ull << lo) - 1);
+                    uint64_t va = ~0ull, vb = ~0ull;
+                    if (jlo > wb || jhi < wb + 128 || w + 2 > w1) {
+                        va = 0;
+                        vb = 0;
+                        if (jhi > wb && jlo < wb + 64) {
+                            const uint32_t lo = jlo > wb ? jlo - wb : 0;
+                            const uint32_t hi = jhi - wb < 64 ? jhi - wb : 64;
+                            va = (hi >= 64 ? ~0ull : ((1ull << hi) - 1)) & ~((1ull << lo) - 1);
+                        }
+                        const uint32_t wb2 = wb + 64;
+                        if (w + 1 < w1 && jhi > wb2 && jlo < wb2 + 64) {
+                            const uint32_t lo = jlo > wb2 ? jlo - wb2 : 0;
+                            const uint32_t hi = jhi - wb2 < 64 ? jhi - wb2 : 64;
+                            vb = (hi >= 64 ? ~0ull : ((1ull << hi) - 1)) & ~((1ull << lo) - 1);
+                        }
                     }
-                    mrem = ~kill & valid;
+                    ma = ~ka & va;
+                    mb = ~kb & vb;
                     wbm = wb - jbase;
-                    w++;
+                    w += 2;
                 }
                 // queue this lane's survivors: warp prefix sum of the counts
-                const uint32_t cnt = __popcll(mrem);
+                const uint32_t cnt = __popcll(ma) + __popcll(mb);
                 uint32_t incl = cnt;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
@@ -473,29 +496,25 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                 }
                 const uint32_t total = __shfl_sync(kFull, incl, 31);
                 const uint32_t room = (uint32_t)kQCap - (B.tail - B.head);
-                if (total <= room) {
-                    uint32_t pos = B.tail + incl - cnt;
-                    while (mrem) {
-                        const uint32_t bit = __ffsll((long long)mrem) - 1;
-                        mrem &= mrem - 1;
-                        B.Q[pos++ & (kQCap - 1)] = ((wbm + bit) << 5) | lane;
-                    }
-                    B.tail += total;
-                } else {
-                    // fill the remaining room in warp order, keep the rest
-                    uint32_t pos = incl - cnt;
-                    while (mrem && pos < room) {
-                        const uint32_t bit = __ffsll((long long)mrem) - 1;
-                        mrem &= mrem - 1;
-                        B.Q[(B.tail + pos) & (kQCap - 1)] = ((wbm + bit) << 5) | lane;
-                        pos++;
-                    }
-                    B.tail += room;
-                    break;
+                // fill in warp order up to the room left; what does not fit
+                // stays in ma / mb for the next segment
+                const uint32_t lim = total <= room ? total : room;
+                uint32_t pos = incl - cnt;
+                while (ma && pos < lim) {
+                    const uint32_t bit = __ffsll((long long)ma) - 1;
+                    ma &= ma - 1;
+                    B.Q[(B.tail + pos++) & (kQCap - 1)] = ((wbm + bit) << 5) | lane;
                 }
+                while (mb && pos < lim) {
+                    const uint32_t bit = __ffsll((long long)mb) - 1;
+                    mb &= mb - 1;
+                    B.Q[(B.tail + pos++) & (kQCap - 1)] = ((wbm + 64 + bit) << 5) | lane;
+                }
+                B.tail += lim;
+                if (total > room) break;
             }
             __syncwarp();
-            if (w >= w1 && !__any_sync(kFull, mrem != 0)) break;
+            if (w >= w1 && !__any_sync(kFull, (ma | mb) != 0)) break;
             // ---- level B until the queue has room again ----
             while (B.tail - B.head > kQLow) b_round(B, a, R, P, cur_range, g, jbase, lane_lt);
         }
@@ -506,7 +525,13 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         __syncwarp();
 }
 
-__global__ void __launch_bounds__(kSweepThreads)
+// MINB = 2: at most 128 registers per thread (2 blocks of
+// 256 per SM); MINB = 3: at most 80 registers (3 blocks of 256, or 6 of 128,
+// when shared memory allows), a few spills in exchange for 50 % more
+// resident warps.  The engine picks by the resident-block count it is tuned
+// for.
+template <int MINB>
+__global__ void __launch_bounds__(kSweepThreads, MINB)
 sweep_kernel(SweepArgs a) {
     extern __shared__ uint32_t s_mem[];
     const uint32_t lane = threadIdx.x & 31;
@@ -584,22 +609,36 @@ static bool g_sweep_attr_set = false;
 static cudaError_t ensure_sweep_attr() {
     if (g_sweep_attr_set) return cudaSuccess;
     const int lim = (int)sweep_smem_bytes(kSweepThreads, kMaxLevelB);
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     if (e == cudaSuccess) g_sweep_attr_set = true;
     return e;
 }
 
-int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads) {
+// resident blocks per SM of one register variant
+static int sweep_occupancy(bool lowreg, uint32_t b_stride, uint32_t block_threads) {
     int nb = 0;
     if (ensure_sweep_attr() != cudaSuccess) return 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_kernel, (int)block_threads,
-                                                  sweep_smem_bytes(block_threads, b_stride));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lowreg ? sweep_kernel<3> : sweep_kernel<2>,
+                                                  (int)block_threads, sweep_smem_bytes(block_threads, b_stride));
     return nb;
+}
+
+int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads) {
+    const int a = sweep_occupancy(false, b_stride, block_threads);
+    const int b = sweep_occupancy(true, b_stride, block_threads);
+    return a > b ? a : b;
+}
+
+bool sweep_needs_lowreg(uint32_t b_stride, uint32_t block_threads, uint32_t blocks_per_sm) {
+    return (int)blocks_per_sm > sweep_occupancy(false, b_stride, block_threads);
 }
 
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
-                         uint32_t b_stride, uint32_t grid, uint32_t block_threads, cudaStream_t st) {
+                         uint32_t b_stride, uint32_t grid, uint32_t block_threads, bool lowreg,
+                         cudaStream_t st) {
     if (block_threads != 128 && block_threads != 256) return cudaErrorInvalidValue;
     size_t smem = sweep_smem_bytes(block_threads, b_stride);
     cudaError_t e = ensure_sweep_attr();
@@ -611,7 +650,8 @@ cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
     a.jmod = jmod;
     a.jmod_stride = stride;
     a.b_stride = b_stride;
-    sweep_kernel<<<grid, block_threads, smem, st>>>(a);
+    if (lowreg) sweep_kernel<3><<<grid, block_threads, smem, st>>>(a);
+    else sweep_kernel<2><<<grid, block_threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -262,7 +262,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
         if (q < 64 && nA1 < kNumA1) slot = nA1++;
         else if (q > 64 && q < 96 && nA2 < kNumA2) slot = kNumA1 + nA2++;
         else if (q > 96 && q < kTLimit && nT < nT_max &&
-                 hp.patT.size() + t_words(q) + 3 <= (size_t)kPatTMax)
+                 hp.patT.size() + t_words(q) + 5 <= (size_t)kPatTMax)
             slot = kNumAR + nT++;
         if (slot >= 0) {
             LevelA& a = hp.A[slot];
@@ -276,7 +276,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
                 for (uint32_t x = 0; x < 256; x++)
                     if (std::binary_search(g.begin(), g.end(), x % q)) a.ext[x >> 5] |= 1u << (x & 31);
             } else {
-                // replicated pattern: a 64-bit window at any phase < q lies in tnw words
+                // replicated pattern: a 128-bit window at any phase < q lies in tnw words
                 a.toff = (uint32_t)hp.patT.size();
                 a.tnw = t_words(q);
                 for (uint32_t wd = 0; wd < a.tnw; wd++) {
@@ -320,8 +320,8 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
     // dummy table-window slots read an all-zero block (phase stays 0)
     {
         const uint32_t zoff = (uint32_t)hp.patT.size();
-        for (int i = 0; i < 3; i++) hp.patT.push_back(0);
-        for (int i = nT; i < kNumT; i++) { hp.A[kNumAR + i].toff = zoff; hp.A[kNumAR + i].tnw = 3; }
+        for (int i = 0; i < 5; i++) hp.patT.push_back(0);
+        for (int i = nT; i < kNumT; i++) { hp.A[kNumAR + i].toff = zoff; hp.A[kNumAR + i].tnw = 5; }
     }
     // pad the level-B records to a multiple of the per-round test count with
     // entries that never kill (q = 2, all-zero bitmap word)

@@ -366,9 +366,10 @@ ccs_status ccs_autotune(ccs_engine* eng, uint64_t ts_lo, uint64_t ts_hi, uint64_
                         ccs_tuning* chosen);
 
 /* Batch autotuner: runs the batch on the given ranges (results discarded)
- * for each block shape (256 and 128 threads, as many blocks as fit) and unit
- * length (each engine's own, 1024, 2048, 4096, 8192 words), keeps the one
- * with the shortest device time and leaves it set on the batch.  Points
+ * for each unit length (each engine's own, 1024, 2048, 4096, 8192 words) and
+ * block shape (1-3 blocks of 256 or 2-6 blocks of 128 threads, those that
+ * fit), keeps the one with the shortest device time and leaves it set on
+ * the batch.  Points
  * carry block_threads, blocks_per_sm and unit_words in their tuning. */
 ccs_status ccs_batch_autotune(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
                               ccs_tune_point* points, uint32_t cap, uint32_t* n_points,
