@@ -24,7 +24,7 @@ OK, ERR_INVALID, ERR_CUDA, OVERFLOW, ERR_NOMEM, ERR_TIMEOUT, ERR_BUSY, ERR_NOT_F
 STATUS_NAMES = ["OK", "ERR_INVALID", "ERR_CUDA", "OVERFLOW", "ERR_NOMEM", "ERR_TIMEOUT",
                 "ERR_BUSY", "ERR_NOT_FOUND", "ERR_CANCELLED", "PENDING"]
 
-PRIME_MR, PRIME_BPSW = 0, 1
+PRIME_MR, PRIME_BPSW, PRIME_V33 = 0, 1, 2
 PROVE_ROOTS, PROVE_FULL = 0, 1
 CHAIN_IS_ROOT, CHAIN_TARGET = 1, 2
 
@@ -203,6 +203,9 @@ _SIGS = {
     "ccs_autotune": (C.c_int, [_vp, _u64, _u64, _u64, C.c_uint32, C.POINTER(_TunePoint), C.c_uint32,
                                C.POINTER(C.c_uint32), C.POINTER(_Tuning)]),
     "ccs_batch_get_tuning": (C.c_int, [_vp, C.POINTER(_BatchTuning)]),
+    "ccs_batch_launch": (C.c_int, [_vp, _vp, C.c_uint32]),
+    "ccs_batch_wait": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ccs_server_memory": (C.c_int, [_vp, C.POINTER(_u64), C.POINTER(_u64)]),
     "ccs_server_set_batch_tuning": (C.c_int, [_vp, C.POINTER(_BatchTuning)]),
     "ccs_batch_set_tuning": (C.c_int, [_vp, C.POINTER(_BatchTuning)]),
     "ccs_batch_autotune": (C.c_int, [_vp, _vp, C.c_uint32, C.POINTER(_TunePoint), C.c_uint32,
@@ -335,6 +338,13 @@ def describe(**kw):
     _check(lib.ccs_describe(C.byref(p), C.byref(inf), bases, cap), "ccs_describe")
     info = {f: getattr(inf, f) for f, _ in _Info._fields_}
     return info, [int(bases[i]) for i in range(info["n_bases"])]
+
+
+def reference_cpu_stages():
+    """The reference CPU engine's filter stages on its own lattice: L2 primes
+    37..61 and ext-L2 primes 67..97 at positions 0..depth-1, the line sieve
+    101..863 at positions 1..depth-1 (v33 with --line-depth = target - 1)."""
+    return [(primes_in(37, 62), 0), (primes_in(67, 98), 0), (primes_in(101, 864), 1)]
 
 
 # configurations named by the workloads they describe
@@ -599,6 +609,27 @@ class Batch:
         nc = sum(o["n_chains"] for o in out)
         return out, surv[:ns], ch[:nc]
 
+    def launch(self, ranges):
+        """The first half of run(): stage the ranges and replay the graph
+        without waiting (ccs_batch_launch); wait() collects."""
+        self._pending = len(ranges)
+        _check(load_library().ccs_batch_launch(self.h, self._ranges(ranges), len(ranges)), "ccs_batch_launch")
+
+    def wait(self, want_records=True):
+        """Waits for the launch in flight (ccs_batch_wait); returns what run()
+        returns."""
+        n = getattr(self, "_pending", 0)
+        res = (_RangeResult * max(n, 1))()
+        surv = np.zeros(self.surv_cap if want_records else 0, dtype=SURVIVOR_DTYPE)
+        ch = np.zeros(self.chain_cap if want_records else 0, dtype=CHAIN_DTYPE)
+        st = load_library().ccs_batch_wait(self.h, res, surv.ctypes.data if want_records else None,
+                                           ch.ctypes.data if want_records else None)
+        _check(st, "ccs_batch_wait")
+        out = [{f: getattr(res[i], f) for f, _ in _RangeResult._fields_} for i in range(n)]
+        ns = sum(o["n_survivors"] for o in out)
+        nc = sum(o["n_chains"] for o in out)
+        return out, surv[:ns], ch[:nc]
+
     def last_ms(self):
         ms = C.c_float(0)
         _check(load_library().ccs_batch_last_ms(self.h, C.byref(ms)))
@@ -768,6 +799,12 @@ class Server:
         applied before its next tick."""
         t = _BatchTuning(block_threads, blocks_per_sm, unit_words, 0)
         _check(load_library().ccs_server_set_batch_tuning(self.h, C.byref(t)), "ccs_server_set_batch_tuning")
+
+    def memory(self):
+        """Device bytes reserved by admitted requests: (now, peak)."""
+        a, b = _u64(0), _u64(0)
+        _check(load_library().ccs_server_memory(self.h, C.byref(a), C.byref(b)), "ccs_server_memory")
+        return a.value, b.value
 
     def stats(self):
         out = (_u64 * 6)()

@@ -38,6 +38,8 @@ ccs_status fail(ccs_status st, const std::string& msg) {
 
 // survivor counts from which ccs_prove runs the staged (breadth-first) prove
 constexpr uint64_t kStagedProveMin = 256;
+// largest extended lattice built (lines of 16 bytes)
+constexpr uint64_t kExtLinesMax = 1ull << 26;
 
 // constant-memory profile slots, per device
 std::mutex g_slot_mu;
@@ -154,6 +156,8 @@ struct ccs_batch {
     // unit length of every range (0: each engine's own)
     uint32_t block_threads = 0, blocks_per_sm = 0, unit_words = 0;
     uint32_t req_blocks_per_sm = 0;      // requested (0: as many as fit)
+    bool in_flight = false;              // launched, not yet waited for
+    std::vector<ccs_range> cur_ranges;   // ranges of the launch in flight
 };
 
 // ---------------------------------------------------------------------------
@@ -307,7 +311,14 @@ ccs_status build_filters(ccs_engine* E, uint32_t split, uint32_t t_count) {
     if (!err.empty()) return fail(CCS_ERR_INVALID, err);
     if (nh[0].primesB.size() > (size_t)kMaxLevelB) return fail(CCS_ERR_INVALID, "too many level-B primes");
     int n_new = 1;
+    // the extended lattice multiplies the lines by q0 - |F_q0|; it is built
+    // while its line table stays within kExtLinesMax lines (1 GiB)
+    uint64_t ext_lines = 0;
     if (nh[0].A[0].q > 1 && nh[0].A[0].q < 64) {
+        for (const auto& fp : nh[0].fprimes)
+            if (fp.q == nh[0].A[0].q) ext_lines = (uint64_t)nh[0].lines.size() * (fp.q - fp.forb.size());
+    }
+    if (ext_lines && ext_lines <= kExtLinesMax) {
         params_of(nh[1]);
         if (build_profile(nh[1], split, nh[0].A[0].q).empty() && nh[1].primesB.size() <= (size_t)kMaxLevelB)
             n_new = 2;
@@ -441,7 +452,10 @@ static ccs_status params_to_profile(const ccs_params* params, HostProfile& hp) {
     }
     hp.primality = p.primality;
     hp.prove_mode = p.prove_mode;
-    if (hp.primality > 1 || hp.prove_mode > 1) return fail(CCS_ERR_INVALID, "bad primality / prove_mode");
+    if (hp.primality > CCS_PRIME_V33 || hp.prove_mode > 1) return fail(CCS_ERR_INVALID, "bad primality / prove_mode");
+    if (hp.primality == CCS_PRIME_V33 && (hp.prove_mode != CCS_PROVE_FULL || hp.kind != 1))
+        return fail(CCS_ERR_INVALID, "CCS_PRIME_V33 is the reference CPU engine's first-kind full prove "
+                                     "(CCS_PROVE_FULL, first kind)");
     if (p.flags & ~CCS_FLAG_REVERSE_PROVE) return fail(CCS_ERR_INVALID, "unknown flags");
     hp.reverse_prove = (p.flags & CCS_FLAG_REVERSE_PROVE) ? 1u : 0u;
     if (hp.reverse_prove && hp.prove_mode != CCS_PROVE_ROOTS)
@@ -661,7 +675,7 @@ ccs_status ccs_filter_range(ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, uint6
 }
 
 static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
-                               const ProveRange* pr_dev, const QiterProve* q, ccs_chain* out_dev,
+                               const ProveRange* pr_dev, uint32_t bits, const QiterProve* q, ccs_chain* out_dev,
                                uint64_t cap, uint64_t* n_out, uint64_t* primes_out, cudaStream_t st);
 
 ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv, uint64_t ts_lo,
@@ -683,7 +697,8 @@ ccs_status ccs_prove(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_sur
     pr->prime_count = E->d_counters.p + 3;
     CU(cudaMemcpyAsync(E->d_prange.p, pr, sizeof(ProveRange), cudaMemcpyHostToDevice, st));
     if (n_surv >= kStagedProveMin)
-        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, nullptr, out_dev, cap, n_out, primes_out, st);
+        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, E->hp.bits, nullptr, out_dev, cap, n_out,
+                            primes_out, st);
     CU(cudaMemsetAsync(E->d_counters.p + 2, 0, 8, st));
     ProveArgs a;
     a.ranges = E->d_prange.p;
@@ -770,9 +785,40 @@ static ccs_status walk_reserve(ccs_engine* E, uint64_t n) {
 // Breadth-first walk rounds over the n items already in E->w_act: every walk
 // ends at its first composite member or at max_len; lengths[idx] receives
 // the count (the items' len included).
-static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint32_t max_len, cudaStream_t st) {
+// The tests a walk applies: pred to members that start a walk (or are tested
+// alone), link_pred to forward links; with screen, links are screened by the
+// 132 primes 67..863 and capped at cap bits first.
+struct WalkPreds {
+    uint32_t pred, link_pred;
+    bool screen;
+    uint32_t cap;
+};
+
+// the profile's tests for stage members (root_role: n itself) and for the
+// forward links of a range of bit width `bits`
+static WalkPreds walk_preds(const HostProfile& hp, bool root_role, uint32_t bits) {
+    WalkPreds w;
+    if (hp.primality == CCS_PRIME_V33) {
+        const bool wide = bits + hp.target > 127;                 // v33:3095-3101
+        w.pred = (root_role && !wide) ? kPredMR235 : kPredBPSW;
+        w.link_pred = wide ? kPredBPSW : kPredFermat2;
+        w.screen = true;
+        w.cap = wide ? bits + 2 * hp.target : 127u;               // v33:1694-1703
+    } else {
+        w.pred = w.link_pred = hp.primality;
+        w.screen = false;
+        w.cap = 0;
+    }
+    return w;
+}
+
+static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint32_t max_len,
+                              const WalkPreds& wp, cudaStream_t st) {
     WalkState* hs = (WalkState*)((char*)E->h_stage + 12288);
-    const bool two_stage = E->hp.primality == CCS_PRIME_BPSW || E->hp.witnesses.size() > 1;
+    auto needs_second = [&](uint32_t p) {
+        return p == kPredBPSW || p == kPredMR235 || (p == kPredMR && E->hp.witnesses.size() > 1);
+    };
+    const bool two_stage = needs_second(wp.pred) || (wp.screen && needs_second(wp.link_pred));
     WalkItem* act = E->w_act.p;
     WalkItem* nxt = E->w_next.p;
     uint32_t n_act = n;
@@ -782,6 +828,10 @@ static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint
         CU(cudaMemcpyAsync(E->w_state.p, hs, sizeof(WalkState), cudaMemcpyHostToDevice, st));
         WalkArgs a;
         a.max_len = max_len;
+        a.pred = wp.pred;
+        a.link_pred = wp.link_pred;
+        a.screen = wp.screen ? 1u : 0u;
+        a.cap_bits = wp.cap;
         a.st = E->w_state.p;
         a.act = act;
         a.sorted = E->w_sorted.p;
@@ -819,7 +869,9 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
         const uint32_t cn = (uint32_t)std::min<uint64_t>(chunk, n - first);
         CU(launch_walk_load(numbers_dev, first, cn, limbs, E->w_act.p, st));
         E->launches += 1;
-        ccs_status s = walk_rounds(E, cn, lengths_dev, kMaxChain, st);
+        // the walk of a given number tests it as a walk start (v33
+        // follow_chain_first: is_prime_fast, v33:1535-1540), then its links
+        ccs_status s = walk_rounds(E, cn, lengths_dev, kMaxChain, walk_preds(E->hp, false, E->hp.bits), st);
         if (s != CCS_OK) return s;
     }
     CU(cudaStreamSynchronize(st));
@@ -830,7 +882,7 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
 // breadth-first stages; see prove.cu).  pr_dev: the range's ProveRange on
 // the device; counters: chains at hc[0], primes at hc[1].
 static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint64_t n_surv,
-                               const ProveRange* pr_dev, const QiterProve* q, ccs_chain* out_dev,
+                               const ProveRange* pr_dev, uint32_t bits, const QiterProve* q, ccs_chain* out_dev,
                                uint64_t cap, uint64_t* n_out, uint64_t* primes_out, cudaStream_t st) {
     if (n_surv == 0) {
         *n_out = 0;
@@ -886,7 +938,11 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
         while (n) {
             CU(cudaMemcpyAsync(E->w_act.p, lists[cur], sizeof(WalkItem) * n, cudaMemcpyDeviceToDevice, st));
             {
-                ccs_status s = walk_rounds(E, n, p.lengths, 1, st);
+                // stage 1 tests n itself (the root test), the others the top
+                // member and predecessors
+                WalkPreds wp = walk_preds(E->hp, stage == 1, bits);
+                wp.screen = false;
+                ccs_status s = walk_rounds(E, n, p.lengths, 1, wp, st);
                 if (s != CCS_OK) return s;
             }
             CU(cudaMemsetAsync(ctr, 0, 4, st));
@@ -901,7 +957,7 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
         const uint32_t nr = read_ctr(1);
         if (nr) {
             CU(cudaMemcpyAsync(E->w_act.p, E->p_fwd.p, sizeof(WalkItem) * nr, cudaMemcpyDeviceToDevice, st));
-            ccs_status s = walk_rounds(E, nr, p.lengths, kMaxChain, st);
+            ccs_status s = walk_rounds(E, nr, p.lengths, kMaxChain, walk_preds(E->hp, false, bits), st);
             if (s != CCS_OK) return s;
             CU(launch_prove_stage(3, p, E->p_fwd.p, nr, st));
             E->launches += 1;
@@ -979,7 +1035,7 @@ ccs_status engine_prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
     h->prime_count = E->d_counters.p + 3;
     CU(cudaMemcpyAsync(E->d_prange.p, h, sizeof(ProveRange), cudaMemcpyHostToDevice, st));
     if (n_surv >= kStagedProveMin)
-        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, q, out_dev, cap, n_out, primes_out, st);
+        return prove_staged(E, surv_dev, n_surv, E->d_prange.p, pr.bits, q, out_dev, cap, n_out, primes_out, st);
     // few survivors: one thread each, one launch
     CU(cudaMemsetAsync(E->d_counters.p + 2, 0, 8, st));
     ProveArgs a;
@@ -1480,6 +1536,7 @@ ccs_status ccs_batch_set_tuning(ccs_batch* b, const ccs_batch_tuning* t) {
     if (t->block_threads && t->block_threads != 128 && t->block_threads != 256)
         return fail(CCS_ERR_INVALID, "block_threads must be 128 or 256");
     if (t->unit_words > (1u << 20)) return fail(CCS_ERR_INVALID, "unit_words too large");
+    if (b->in_flight) return fail(CCS_ERR_BUSY, "the batch's previous launch has not been waited for");
     CU(cudaSetDevice(b->device));
     b->unit_words = t->unit_words;
     const uint32_t bt = t->block_threads ? t->block_threads : b->block_threads;
@@ -1492,13 +1549,11 @@ ccs_status ccs_batch_set_tuning(ccs_batch* b, const ccs_batch_tuning* t) {
     return CCS_OK;
 }
 
-ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
-                         ccs_range_result* results, ccs_survivor* surv_host, ccs_chain* chains_host,
-                         void* stream) {
+ccs_status ccs_batch_launch(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges) {
     if (!b || (n_ranges && !ranges)) return fail(CCS_ERR_INVALID, "null argument");
     if (n_ranges > b->max_ranges) return fail(CCS_ERR_INVALID, "too many ranges for this batch");
+    if (b->in_flight) return fail(CCS_ERR_BUSY, "the batch's previous launch has not been waited for");
     CU(cudaSetDevice(b->device));
-    (void)stream;
     uint64_t total = 0;
     uint32_t* cnt = b->d_counts.p;
     for (uint32_t i = 0; i < n_ranges; i++) {
@@ -1514,6 +1569,7 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
         if (ranges[x].profile != ranges[y].profile) return ranges[x].profile < ranges[y].profile;
         return ranges[x].n_tiles > ranges[y].n_tiles;
     });
+    b->cur_ranges.assign(ranges, ranges + n_ranges);
     for (uint32_t k = 0; k < n_ranges; k++) {
         const uint32_t i = order[k];
         const ccs_range& rg = ranges[i];
@@ -1548,28 +1604,36 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
     CU(cudaEventRecord(b->ev0, b->stream));
     CU(cudaGraphLaunch(b->gexec, b->stream));
     CU(cudaEventRecord(b->ev1, b->stream));
-    CU(cudaStreamSynchronize(b->stream));
+    b->in_flight = true;
+    return CCS_OK;
+}
+
+ccs_status ccs_batch_wait(ccs_batch* b, ccs_range_result* results, ccs_survivor* surv_host,
+                          ccs_chain* chains_host) {
+    if (!b) return fail(CCS_ERR_INVALID, "null argument");
+    if (!b->in_flight) return fail(CCS_ERR_INVALID, "no batch launch to wait for");
+    const uint32_t n_ranges = (uint32_t)b->cur_ranges.size();
+    if (n_ranges && !results) return fail(CCS_ERR_INVALID, "results is null");
+    CU(cudaSetDevice(b->device));
+    b->in_flight = false;
+    CU(cudaEventSynchronize(b->ev1));
     CU(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
     const uint32_t* hc = b->h_counts;
     ccs_status st = CCS_OK;
     uint64_t ns = hc[0], nch = hc[2];
-    // per-range offsets follow the order records were written; results report
-    // counts, and offsets are recovered from the flat arrays on the host
-    std::vector<uint64_t> soff(n_ranges + 1, 0), coff(n_ranges + 1, 0);
     for (uint32_t i = 0; i < n_ranges; i++) {
+        const ccs_range& rg = b->cur_ranges[i];
         ccs_range_result& r = results[i];
         memset(&r, 0, sizeof(r));
         r.n_survivors = hc[4 + 3 * i];
         r.n_chains = hc[4 + 3 * i + 1];
         r.n_primes = hc[4 + 3 * i + 2];
-        ccs_engine* E = b->prof[ranges[i].profile];
-        uint64_t cpt = 0;
-        for (uint32_t w : E->hp.wheel_total) cpt += w;
+        ccs_engine* E = b->prof[rg.profile];
         // exact candidate count: lines of each tile class times their blocks
-        uint32_t e0 = (uint32_t)(mk128(ranges[i].tile_start_lo, ranges[i].tile_start_hi) % 6);
+        uint32_t e0 = (uint32_t)(mk128(rg.tile_start_lo, rg.tile_start_hi) % 6);
         uint64_t cand = 0;
         for (uint32_t c6 = 0; c6 < 6; c6++) {
-            uint64_t endc = (uint64_t)e0 + ranges[i].n_tiles;
+            uint64_t endc = (uint64_t)e0 + rg.n_tiles;
             uint64_t jhi = endc > c6 ? (endc - c6 + 5) / 6 : 0;
             uint64_t jlo = c6 < e0 ? 1 : 0;
             if (jhi > jlo) cand += (jhi - jlo) * E->hp.lines_per_class[c6];
@@ -1577,12 +1641,26 @@ ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_range
         r.candidates = cand;
         r.status = (ns > b->surv_cap || nch > b->chain_cap) ? CCS_OVERFLOW : CCS_OK;
     }
+    // records are copied on the batch stream: a launch of another batch may
+    // already be running on the GPU
     uint64_t ncopy = std::min<uint64_t>(ns, b->surv_cap);
     uint64_t ccopy = std::min<uint64_t>(nch, b->chain_cap);
-    if (surv_host && ncopy) CU(cudaMemcpy(surv_host, b->d_surv.p, 16 * ncopy, cudaMemcpyDeviceToHost));
-    if (chains_host && ccopy) CU(cudaMemcpy(chains_host, b->d_chains.p, 48 * ccopy, cudaMemcpyDeviceToHost));
+    if (surv_host && ncopy)
+        CU(cudaMemcpyAsync(surv_host, b->d_surv.p, 16 * ncopy, cudaMemcpyDeviceToHost, b->stream));
+    if (chains_host && ccopy)
+        CU(cudaMemcpyAsync(chains_host, b->d_chains.p, 48 * ccopy, cudaMemcpyDeviceToHost, b->stream));
+    if ((surv_host && ncopy) || (chains_host && ccopy)) CU(cudaStreamSynchronize(b->stream));
     if (ns > b->surv_cap || nch > b->chain_cap) st = fail(CCS_OVERFLOW, "batch capacity exceeded");
     return st;
+}
+
+ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
+                         ccs_range_result* results, ccs_survivor* surv_host, ccs_chain* chains_host,
+                         void* stream) {
+    (void)stream;
+    ccs_status st = ccs_batch_launch(b, ranges, n_ranges);
+    if (st != CCS_OK) return st;
+    return ccs_batch_wait(b, results, surv_host, chains_host);
 }
 
 ccs_status ccs_batch_autotune(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,

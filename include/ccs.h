@@ -63,7 +63,18 @@ enum { CCS_KIND_FIRST = 1, CCS_KIND_SECOND = 2 };
 /* Primality predicate used by the prover. */
 enum {
     CCS_PRIME_MR = 0,      /* strong-PRP for every witness (v13 gpu_is_prime, v13:1428-1452) */
-    CCS_PRIME_BPSW = 1     /* Baillie-PSW: GMP 6.3 mpz_probab_prime_p(n, 1) (v13:1841) */
+    CCS_PRIME_BPSW = 1,    /* Baillie-PSW: GMP 6.3 mpz_probab_prime_p(n, 1) (v13:1841) */
+    CCS_PRIME_V33 = 2      /* the reference CPU engine's own tests (first kind, CCS_PROVE_FULL):
+                              n after trial division by 101..409 -> strong PRP to bases
+                              2, 3, 5 (v33:1326-1339, 2112-2130); predecessors and backward
+                              steps -> Baillie-PSW (is_prime_fast, v33:1345-1362, 1489-1495);
+                              forward links -> zero residue mod any of the 132 screen primes
+                              67..863 is composite (a link equal to a screen prime included),
+                              then Fermat base 2 (v33:1512-1577, 1290-1302), walk stopped at
+                              2^127.  Ranges with bits + target > 127 take the reference's
+                              wide path instead: Baillie-PSW for n and the links, walk
+                              stopped at 2^(bits + 2 target) (v33:1594-1656, 1694-1703,
+                              1982-1997). */
 };
 
 /* Prove semantics. */
@@ -252,6 +263,15 @@ ccs_status ccs_batch_destroy(ccs_batch* b);
 ccs_status ccs_batch_run(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges,
                          ccs_range_result* results, ccs_survivor* surv_host, ccs_chain* chains_host,
                          void* stream);
+/* The same as ccs_batch_run in two halves, so that a caller can prepare
+ * (and another batch can run) while the GPU works: ccs_batch_launch stages
+ * the ranges and replays the graph without waiting; ccs_batch_wait waits for
+ * that launch and fills results and the host records.  A batch holds one
+ * launch at a time (CCS_ERR_BUSY otherwise); two batches over the same
+ * engines may be in flight together. */
+ccs_status ccs_batch_launch(ccs_batch* b, const ccs_range* ranges, uint32_t n_ranges);
+ccs_status ccs_batch_wait(ccs_batch* b, ccs_range_result* results, ccs_survivor* surv_host,
+                          ccs_chain* chains_host);
 /* device-side timing of the last ccs_batch_run: filter+prove milliseconds */
 ccs_status ccs_batch_last_ms(const ccs_batch* b, float* ms);
 
@@ -271,10 +291,12 @@ ccs_status ccs_batch_set_tuning(ccs_batch* b, const ccs_batch_tuning* t);
 /* ---- served path ------------------------------------------------------------ */
 
 /* A request server with continuous batching: requests (lattice ranges) are
- * admitted as slots and memory free up; every scheduling tick runs one chunk
- * of every admitted request together in one batched graph replay, so new
- * arrivals overlap with long-running requests on the device.  Results are
- * identical to a plain ccs_filter_range + ccs_prove of the whole range. */
+ * admitted as slots and device memory free up; every scheduling tick runs
+ * one chunk of every admitted request together in one batched graph replay,
+ * so new arrivals overlap with long-running requests on the device.  Ticks
+ * alternate between two batch executors: tick k is on the GPU while the host
+ * collects and routes tick k - 1.  Results are identical to a plain
+ * ccs_filter_range + ccs_prove of the whole range. */
 typedef struct ccs_server ccs_server;
 
 typedef struct {
@@ -308,6 +330,10 @@ ccs_status ccs_cancel(ccs_server* s, uint64_t id);
 /* batch tuning of the server's executor (ccs_batch_set_tuning), applied
  * before its next tick */
 ccs_status ccs_server_set_batch_tuning(ccs_server* s, const ccs_batch_tuning* t);
+/* device bytes reserved by admitted requests (residue rows and survivor /
+ * chain slots of two ticks in flight), now and at the peak, against
+ * mem_cap_bytes */
+ccs_status ccs_server_memory(ccs_server* s, uint64_t* reserved_now, uint64_t* reserved_peak);
 /* counters: [0] submitted [1] admitted [2] completed [3] cancelled [4] ticks [5] pending now */
 ccs_status ccs_server_stats(ccs_server* s, uint64_t* out6);
 

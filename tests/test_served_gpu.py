@@ -1,5 +1,6 @@
 """Served path: requests that arrive while others run share ticks on the
-GPU, and each request's survivors and chains equal a plain run of the same
+GPU (two ticks in flight, on alternating batch executors), and each
+request's survivors and chains equal a plain filter + prove of the same
 range alone."""
 import time
 
@@ -16,6 +17,11 @@ def surv_set(a):
 def chain_set(a):
     return sorted((int(r["base_idx"]), int(r["k_offset"]), int(r["tile_idx"]), int(r["chain_len"]),
                    tuple(int(x) for x in r["root"])) for r in a)
+
+
+def chain_rows(t):
+    a = t.cpu().numpy().astype(np.int64) & 0xFFFFFFFF
+    return sorted((int(r[0]), int(r[1]), int(r[2]), int(r[3]), tuple(int(x) for x in r[4:10])) for r in a)
 
 
 def test_served_results_equal_alone_and_in_the_mix(ccs):
@@ -53,6 +59,14 @@ def test_served_results_equal_alone_and_in_the_mix(ccs):
         want = sorted(map(tuple, (plain.cpu().numpy()[:, :3].astype(np.int64) & 0xFFFFFFFF).tolist()))
         assert mixed[rid][1] == want
         assert res2["n_survivors"] == len(want)
+        # chains equal a plain prove of the plain survivors
+        eng.set_bits(bits)
+        pch, pprimes = eng.prove(plain, ts)
+        assert mixed[rid][2] == chain_rows(pch)
+        assert mixed[rid][0]["n_primes"] == pprimes
+    # device-byte admission: reserved while running, released at the end
+    now, peak = srv.memory()
+    assert now == 0 and peak > 0
     srv.close()
     for e in engines:
         e.close()
