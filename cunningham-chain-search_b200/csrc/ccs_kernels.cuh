@@ -131,8 +131,23 @@ struct WalkState {
     uint32_t fill[kMaxLimbs + 1];
     uint32_t n_lucas[kMaxLimbs + 1];     // base-2 probable primes per limb count
 };
+// Primality tests a walk round can apply (CCS_PRIME_MR / CCS_PRIME_BPSW,
+// plus the two native tests of the reference CPU engine v33)
+enum : uint32_t {
+    kPredMR = 0,                         // strong PRP for every witness of the profile
+    kPredBPSW = 1,                       // Baillie-PSW (GMP mpz_probab_prime_p(n, 1))
+    kPredMR235 = 3,                      // strong PRP to bases 2, 3, 5 (v33 is_prime_root_native)
+    kPredFermat2 = 4                     // 2^(n-1) == 1 (mod n) (v33 is_prime_pocklington_native)
+};
+
 struct WalkArgs {
     uint32_t max_len;                    // walks end at this length (chain lengths cap)
+    uint32_t pred;                       // test of members that start a walk (len 0) or are
+                                         // tested alone (stage tests)
+    uint32_t link_pred;                  // test of forward links (len >= 1) when screen is set
+    uint32_t screen;                     // 1: links are first screened by the 132 primes
+                                         // 67..863 (a zero residue is composite) and capped
+    uint32_t cap_bits;                   // with screen: a link of more bits ends the walk (0: none)
     WalkState* st;
     const WalkItem* act;
     WalkItem* sorted;                    // act, grouped by limb count

@@ -11,7 +11,10 @@
 // Primality: CCS_PRIME_MR = strong-PRP for each witness after trial division
 // by {3..71} (v13 gpu_is_prime, v13:1428-1452); CCS_PRIME_BPSW = Baillie-PSW
 // (strong PRP base 2 + strong Lucas, Selfridge method A), the semantics of
-// GMP 6.3 mpz_probab_prime_p(n, 1) used by the reference CPU prover.
+// GMP 6.3 mpz_probab_prime_p(n, 1) used by the reference CPU prover;
+// CCS_PRIME_V33 = the reference CPU engine's own per-role tests (strong PRP
+// to 2, 3, 5 for n; Baillie-PSW for predecessors; screened Fermat base 2 for
+// forward links, v33:1290-1339, 1512-1577).
 #include "ccs_kernels.cuh"
 #include "../../include/ccs.h"
 
@@ -500,15 +503,44 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
     return false;
 }
 
+// Fermat test to base 2: 2^(n-1) == 1 (mod n), n odd > 2 (the link test of
+// the reference CPU engine, is_prime_pocklington_native, v33:1290-1302)
 template <int NL>
-__device__ bool prp_suite(const Big& nb, int nbits, uint32_t primality, const ProveConst& pc,
+__device__ bool fermat2(Mont<NL>& M, const Big& nb) {
+    Big e = nb;
+    e.w[0] -= 1;                              // n odd: no borrow
+    uint32_t x[NL];
+#pragma unroll
+    for (int i = 0; i < NL; i++) x[i] = M.one[i];
+    dblmod<NL>(x, x, M.n);                    // 2 R mod n: the top bit of n - 1
+    const int top = big_bits(e) - 1;
+#pragma unroll
+    for (int wi = kMaxLimbs - 1; wi >= 0; wi--) {
+        if (32 * wi > top - 1) continue;
+        const uint32_t word = e.w[wi];
+        const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
+        for (int b = hb; b >= 0; b--) {
+            montmul<NL>(x, x, x, M.n, M.ninv);
+            M.count++;
+            if ((word >> b) & 1u) dblmod<NL>(x, x, M.n);
+        }
+    }
+    return eq<NL>(x, M.one);
+}
+
+template <int NL>
+__device__ bool prp_suite(const Big& nb, int nbits, uint32_t pred, const ProveConst& pc,
                           uint32_t& mm) {
     Mont<NL> M;
     mont_setup<NL>(M, nb, nbits);
     M.count = 0;
     bool r = true;
-    if (primality == CCS_PRIME_BPSW) {
+    if (pred == kPredBPSW) {
         r = strong_prp<NL>(M, nb, 2) && strong_lucas<NL>(M, nb);
+    } else if (pred == kPredMR235) {
+        r = strong_prp<NL>(M, nb, 2) && strong_prp<NL>(M, nb, 3) && strong_prp<NL>(M, nb, 5);
+    } else if (pred == kPredFermat2) {
+        r = fermat2<NL>(M, nb);
     } else {
         for (uint32_t i = 0; i < pc.n_wit && r; i++) r = strong_prp<NL>(M, nb, pc.wit[i]);
     }
@@ -535,12 +567,20 @@ __constant__ uint32_t c_small_magic[27] = {
 // v13:1428-1452, and of the BPSW screen): returns 0 = composite, 1 = prime
 // without a probable-prime test, or the Montgomery limb count (2..6) of the
 // test that decides.
-__device__ int prime_screen(const Big& nb, const ProveConst& pc, int& nbits_out) {
+__device__ int prime_screen(const Big& nb, uint32_t pred, int& nbits_out) {
     const int nbits = big_bits(nb);
     nbits_out = nbits;
     if (nbits <= 1) return 0;
     const uint32_t lo = nb.w[0];
-    const bool mr = pc.primality == CCS_PRIME_MR;
+    if (pred == kPredMR235 || pred == kPredFermat2) {
+        // the reference's native tests: 2, 3, 5 directly, even numbers out,
+        // no trial division (its callers divide before, v33:1290-1339)
+        if (nbits <= 3) return (lo == 2 || lo == 3 || lo == 5) ? 1 : (lo == 7 ? 2 : 0);
+        if ((lo & 1u) == 0) return 0;
+        const int nl = (nbits + 31) >> 5;
+        return nl <= 2 ? 2 : nl;
+    }
+    const bool mr = pred == kPredMR;
     const int ntrial = mr ? 19 : 27;
     if (mr) {
         if (nbits <= 64 && nb.w[1] == 0) {
@@ -580,30 +620,50 @@ __device__ int prime_screen(const Big& nb, const ProveConst& pc, int& nbits_out)
     return nl <= 2 ? 2 : nl;
 }
 
-// primality predicate of the profile for any n < 2^192; mm counts the
-// Montgomery products spent
-__device__ bool is_prime_dev(const Big& nb, const ProveConst& pc, uint32_t& mm) {
+// one primality test for any n < 2^192; mm counts the Montgomery products
+// spent
+__device__ bool is_prime_pred(const Big& nb, uint32_t pred, const ProveConst& pc, uint32_t& mm) {
     int nbits;
-    const int v = prime_screen(nb, pc, nbits);
+    const int v = prime_screen(nb, pred, nbits);
     if (v < 2) return v == 1;
     switch (v) {
-        case 2: return prp_suite<2>(nb, nbits, pc.primality, pc, mm);
-        case 3: return prp_suite<3>(nb, nbits, pc.primality, pc, mm);
-        case 4: return prp_suite<4>(nb, nbits, pc.primality, pc, mm);
-        case 5: return prp_suite<5>(nb, nbits, pc.primality, pc, mm);
-        default: return prp_suite<6>(nb, nbits, pc.primality, pc, mm);
+        case 2: return prp_suite<2>(nb, nbits, pred, pc, mm);
+        case 3: return prp_suite<3>(nb, nbits, pred, pc, mm);
+        case 4: return prp_suite<4>(nb, nbits, pred, pc, mm);
+        case 5: return prp_suite<5>(nb, nbits, pred, pc, mm);
+        default: return prp_suite<6>(nb, nbits, pred, pc, mm);
     }
 }
 
+// the profile's test for a number that is neither n's root test nor a
+// forward link (the reference CPU engine tests those with is_prime_fast:
+// Baillie-PSW)
+__device__ __forceinline__ uint32_t other_pred(const ProveConst& pc) {
+    return pc.primality == CCS_PRIME_V33 ? (uint32_t)kPredBPSW : pc.primality;
+}
+
+__device__ bool is_prime_dev(const Big& nb, const ProveConst& pc, uint32_t& mm) {
+    return is_prime_pred(nb, other_pred(pc), pc, mm);
+}
+
+__device__ bool screen_composite(const Big& nb);
+
 // forward walk p -> 2p + 1 (second kind 2p - 1) while prime, counting p
-// (v13:1519-1528, 1873-1881; v13b:1527-1535, 1878-1886)
-__device__ int walk_forward(Big cur, const ProveConst& pc, uint32_t& mm) {
+// (v13:1519-1528, 1873-1881; v13b:1527-1535, 1878-1886).  With screen, a
+// link first ends the walk when it has more than cap_bits bits or a zero
+// residue mod a screen prime (v33:1540-1562).
+__device__ int walk_forward(Big cur, const ProveConst& pc, uint32_t link_pred, bool screen,
+                            uint32_t cap_bits, uint32_t& mm) {
     int len = 1;
     while (len < kMaxChain) {
         if (big_bits(cur) >= 32 * kMaxLimbs) break;   // next member would exceed 192 bits
         Big nx = cur;
         big_next(nx, pc.kind);
-        if (!is_prime_dev(nx, pc, mm)) break;
+        if (screen) {
+            if (cap_bits && big_bits(nx) > (int)cap_bits) break;
+            if (screen_composite(nx)) break;
+        }
+        if (!is_prime_pred(nx, link_pred, pc, mm)) break;
         len++;
         cur = nx;
     }
@@ -619,6 +679,45 @@ __constant__ uint32_t c_screen[132] = {
     571, 577, 587, 593, 599, 601, 607, 613, 617, 619, 631, 641, 643, 647, 653, 659, 661,
     673, 677, 683, 691, 701, 709, 719, 727, 733, 739, 743, 751, 757, 761, 769, 773, 787,
     797, 809, 811, 821, 823, 827, 829, 839, 853, 857, 859, 863};
+
+// a zero residue mod any of the 132 screen primes 67..863 (the reference CPU
+// engine's link screen counts a link equal to a screen prime as composite
+// too, v33:1551-1562)
+__device__ bool screen_composite(const Big& nb) {
+    for (int t = 0; t < 132; t++)
+        if (big_mod_small(nb, c_screen[t]) == 0) return true;
+    return false;
+}
+
+// The tests of one range under the profile's predicate: the root test of n,
+// and the forward-link rules (v33: native path up to bits + target = 127,
+// wide path above, v33:3095-3101)
+struct RangePreds {
+    uint32_t root, link, cap;
+    bool screen;
+};
+__device__ __forceinline__ RangePreds range_preds(const ProveConst& pc, uint32_t bits, uint32_t target) {
+    RangePreds r;
+    if (pc.primality == CCS_PRIME_V33) {
+        const bool wide = bits + target > 127;
+        r.root = wide ? (uint32_t)kPredBPSW : (uint32_t)kPredMR235;
+        r.link = wide ? (uint32_t)kPredBPSW : (uint32_t)kPredFermat2;
+        r.cap = wide ? bits + 2 * target : 127u;
+        r.screen = true;
+    } else {
+        r.root = r.link = pc.primality;
+        r.cap = 0;
+        r.screen = false;
+    }
+    return r;
+}
+
+// trial division of n before its root test: v13 K2's 132 primes (roots
+// mode), its CPU prover's 62 (full mode), or v33's 101..409 (v33:2112-2128)
+__device__ __forceinline__ void trial_list(const ProveConst& pc, uint32_t& t0, uint32_t& t1) {
+    if (pc.primality == CCS_PRIME_V33) { t0 = 7; t1 = 62; }
+    else { t0 = 0; t1 = pc.prove_mode == CCS_PROVE_ROOTS ? 132u : 62u; }   // v13:1499 / 1832
+}
 
 // ---------------------------------------------------------------------------
 // prove kernel: one thread per survivor
@@ -745,10 +844,12 @@ prove_kernel(ProveArgs a) {
         // trial division only rejects composites that the primality test
         // rejects too (n > 863); q-iteration survivors passed the sieve at
         // position 0 already, so for them it is skipped
-        const int ntd = a.q.seg ? 0 : (pc.prove_mode == CCS_PROVE_ROOTS) ? 132 : 62;  // v13:1499 / 1832
+        uint32_t t0 = 0, t1 = 0;
+        if (!a.q.seg) trial_list(pc, t0, t1);
         bool comp = false;
-        for (int t = 0; t < ntd && !comp; t++) comp = big_mod_small(nb, c_screen[t]) == 0;
+        for (uint32_t t = t0; t < t1 && !comp; t++) comp = big_mod_small(nb, c_screen[t]) == 0;
         if (comp) continue;
+        const RangePreds rp = range_preds(pc, R.bits, R.target);
         uint32_t mm = 0;
         if (pc.reverse) {
             // chain position target - 1 first (the largest member, the
@@ -761,7 +862,7 @@ prove_kernel(ProveArgs a) {
                 if (!is_prime_dev(top, pc, mm)) continue;
             }
         }
-        if (!is_prime_dev(nb, pc, mm)) continue;
+        if (!is_prime_pred(nb, rp.root, pc, mm)) continue;
         if (R.prime_count) atomicAdd(R.prime_count, 1u);
         Big root = nb;
         bool is_root = true;
@@ -779,7 +880,7 @@ prove_kernel(ProveArgs a) {
                 root = p2;
             }
         }
-        const int len = walk_forward(root, pc, mm);
+        const int len = walk_forward(root, pc, rp.link, rp.screen, rp.cap, mm);
         if (R.chain_count) atomicAdd(R.chain_count, 1u);
         const uint32_t slot = atomicAdd(a.chain_count, 1u);
         if (slot < a.chain_cap) {
@@ -877,7 +978,13 @@ walk_screen_kernel(WalkArgs a) {
             Big b;
 #pragma unroll
             for (int w = 0; w < kMaxLimbs; w++) b.w[w] = it.x[w];
-            v = prime_screen(b, pc, nbits);
+            const bool link = a.screen && it.len >= 1;
+            if (link && ((a.cap_bits && big_bits(b) > (int)a.cap_bits) || screen_composite(b))) {
+                nbits = big_bits(b);
+                v = 0;                                   // the walk ends here (v33:1546-1562)
+            } else {
+                v = prime_screen(b, link ? a.link_pred : a.pred, nbits);
+            }
             a.code[i] = (uint8_t)v;
             if (v == 0) a.lengths[it.idx] = it.len;
         }
@@ -936,18 +1043,23 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
             Mont<NL> M;
             mont_setup<NL>(M, b, nbits);
             M.count = 0;
+            const uint32_t pred = (a.screen && it.len >= 1) ? a.link_pred : a.pred;
             if (stage == 0) {
                 // the first test for every member; the rest only for its
                 // probable primes, in a second launch of uniform warps
-                if (pc.primality == CCS_PRIME_BPSW) {
+                if (pred == kPredBPSW || pred == kPredMR235) {
                     to_lucas = strong_prp<NL>(M, b, 2);
+                } else if (pred == kPredFermat2) {
+                    prime = fermat2<NL>(M, b);
                 } else if (pc.n_wit <= 1) {
                     prime = pc.n_wit == 0 || strong_prp<NL>(M, b, pc.wit[0]);
                 } else {
                     to_lucas = strong_prp<NL>(M, b, pc.wit[0]);
                 }
-            } else if (pc.primality == CCS_PRIME_BPSW) {
+            } else if (pred == kPredBPSW) {
                 prime = strong_lucas<NL>(M, b);
+            } else if (pred == kPredMR235) {
+                prime = strong_prp<NL>(M, b, 3) && strong_prp<NL>(M, b, 5);
             } else {
                 prime = true;
                 for (uint32_t k = 1; k < pc.n_wit && prime; k++) prime = strong_prp<NL>(M, b, pc.wit[k]);
@@ -1031,7 +1143,8 @@ __global__ void __launch_bounds__(256)
 prove_seed_kernel(StagedProve p) {
     const ProveConst& pc = c_prove[p.range->profile];
     const ProveRange& R = *p.range;
-    const uint32_t ntd = p.q.seg ? 0u : (pc.prove_mode == CCS_PROVE_ROOTS) ? 132u : 62u;  // v13:1499 / 1832
+    uint32_t t0 = 0, t1 = 0;
+    if (!p.q.seg) trial_list(pc, t0, t1);
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < p.n_surv; i0 += gridDim.x * blockDim.x) {
         const uint32_t i = i0 + threadIdx.x;
         bool keep = false;
@@ -1045,7 +1158,7 @@ prove_seed_kernel(StagedProve p) {
                 nb = survivor_number(sv, R, pc);
                 keep = big_bits(nb) == (int)R.bits;                              // v13:1495, 1828
             }
-            for (uint32_t t = 0; t < ntd && keep; t++) keep = big_mod_small(nb, c_screen[t]) != 0;
+            for (uint32_t t = t0; t < t1 && keep; t++) keep = big_mod_small(nb, c_screen[t]) != 0;
             x = nb;
             if (keep) {
                 big_store(p.nval + (size_t)i * kMaxLimbs, nb);

@@ -704,6 +704,98 @@ int orc_prove_n(const u64* n_words, int nw, int bits, int mode, int primality,
     return len;
 }
 
+/* ---- the reference CPU engine's own tests (v33), first kind ------------ */
+
+/* is_prime_root_native (v33:1326-1339): 2, 3, 5 prime, even composite, then
+ * strong PRP to bases 2, 3 and 5 */
+static int v33_root_test(const big* n) {
+    if (big_bits(n) <= 3) {
+        u64 v = n->w[0];
+        if (v == 2 || v == 3 || v == 5) return 1;
+        if (v != 7) return 0;
+    }
+    if (!(n->w[0] & 1)) return 0;
+    return strong_prp(n, 2) && strong_prp(n, 3) && strong_prp(n, 5);
+}
+
+/* is_prime_pocklington_native (v33:1290-1302): n <= 5 -> n in {2, 3, 5};
+ * else 2^(n-1) == 1 (mod n) */
+static int v33_fermat2(const big* n) {
+    if (big_bits(n) <= 3 && n->w[0] <= 5) return n->w[0] == 2 || n->w[0] == 3 || n->w[0] == 5;
+    big e, two, r, one;
+    big_sub_u64(&e, n, 1);
+    big_set_u64(&two, 2);
+    big_set_u64(&one, 1);
+    powmod(&r, &two, &e, n);
+    return big_cmp(&r, &one) == 0;
+}
+
+/* follow_chain_first_screened / its wide twin from a known-prime root
+ * (v33:1512-1577, 1594-1656): a link of more than cap bits ends the walk,
+ * then a zero residue mod any chain-screen prime, then the link test
+ * (Fermat base 2 on the native path, Baillie-PSW on the wide one) */
+static int v33_walk(const big* root, int wide, int cap_bits) {
+    int len = 1;
+    big cur = *root, nx;
+    while (len < ORC_MAX_CHAIN) {
+        nx = cur;
+        big_shl1(&nx);
+        big_add_u64(&nx, &nx, 1);
+        if (big_bits(&nx) > cap_bits) break;
+        int comp = 0;
+        for (int i = 0; i < 132 && !comp; i++) comp = big_mod_u32(&nx, CHAIN_SCREEN[i]) == 0;
+        if (comp) break;
+        if (!(wide ? is_prime_bpsw(&nx) : v33_fermat2(&nx))) break;
+        len++;
+        cur = nx;
+    }
+    return len;
+}
+
+/* One survivor through the reference CPU engine's proving path
+ * (worker_sequential, v33:2112-2215; wide path v33:1982-2098): trial division
+ * by 101..409, root test (native: v33_root_test; wide, bits + target > 127:
+ * Baillie-PSW), backward walk with Baillie-PSW from n, at most MAX_CHAIN
+ * steps (is_chain_root_first / follow_chain_backward_first, v33:1489-1495,
+ * 1665-1676), forward walk from the root (v33_walk; cap 2^127 native,
+ * 2^(bits + 2 target) wide).  Returns -1 when the survivor yields no
+ * record, else the chain length. */
+int orc_prove_v33(const u64* n_words, int nw, int bits, int target, u64* root_out, int* flags,
+                  int* is_prime_out) {
+    big n; big_from_words(&n, n_words, nw);
+    *flags = 0;
+    *is_prime_out = 0;
+    if (big_bits(&n) != bits) return -1;
+    for (int i = 7; i < 62; i++)
+        if (big_mod_u32(&n, CHAIN_SCREEN[i]) == 0) return -1;
+    const int wide = bits + target > 127;
+    const int cap = wide ? bits + 2 * target : 127;
+    if (!(wide ? is_prime_bpsw(&n) : v33_root_test(&n))) return -1;
+    *is_prime_out = 1;
+    big pred, root = n, two;
+    big_set_u64(&two, 2);
+    for (int steps = 0; steps < ORC_MAX_CHAIN; steps++) {
+        big_sub_u64(&pred, &root, 1);
+        big_shr1(&pred);
+        if (big_cmp(&pred, &two) < 0) break;
+        if (!is_prime_bpsw(&pred)) break;
+        root = pred;
+    }
+    const int is_root = big_cmp(&root, &n) == 0;
+    int len = v33_walk(&root, wide, cap);
+    memcpy(root_out, root.w, sizeof(u64) * ORC_LIMBS);
+    *flags = is_root ? 1 : 0;
+    return len;
+}
+
+/* The walk of a given number under those rules (follow_chain_first: the
+ * number itself by Baillie-PSW, v33:1535-1540): 0 when it is not prime */
+int orc_chain_from_v33(const u64* n_words, int nw, int wide, int cap_bits) {
+    big n; big_from_words(&n, n_words, nw);
+    if (!is_prime_bpsw(&n)) return 0;
+    return v33_walk(&n, wide, cap_bits);
+}
+
 /* n = ((tile_start + tile_idx) * WP + k) * M + base as ORC_LIMBS words */
 void orc_reconstruct(const orc_lattice* L, u64 ts_lo, u64 ts_hi, u32 base_idx, u32 k,
                      u32 tile_idx, u64* out) {

@@ -148,3 +148,77 @@ int ref_gmp_forward_chain2(const char* hex) {
     mpz_clear(cur); mpz_clear(t);
     return len;
 }
+
+/* ---- the native (u128) prove path of worker_sequential, per candidate ---- */
+
+/* follow_chain_first_screened on the native path (v33:1512-1577) from n, cap
+ * 2^127, no prefilter residues; root_known_prime as given (0: n is tested
+ * with is_prime_fast first) */
+int ref33_follow_native(unsigned long long lo, unsigned long long hi, int root_known_prime) {
+    mpz_t n, maxv, cur, t, t2, pp;
+    mpz_init(n); mpz_init(maxv); mpz_init(cur); mpz_init(t); mpz_init(t2); mpz_init(pp);
+    u128_to_mpz(n, ((u128)hi << 64) | lo);
+    mpz_ui_pow_ui(maxv, 2, 127);
+    int len = follow_chain_first_screened(n, maxv, cur, t, t2, pp, NULL, root_known_prime, NULL, NULL);
+    mpz_clear(n); mpz_clear(maxv); mpz_clear(cur); mpz_clear(t); mpz_clear(t2); mpz_clear(pp);
+    return len;
+}
+
+int ref33_root_native(unsigned long long lo, unsigned long long hi) {
+    return is_prime_root_native(((u128)hi << 64) | lo);
+}
+
+int ref33_fermat2_native(unsigned long long lo, unsigned long long hi) {
+    u128 n = ((u128)hi << 64) | lo;
+    MontCtx ctx;
+    if (n > 5) mont_ctx_init(&ctx, n);
+    return is_prime_pocklington_native(n, &ctx);
+}
+
+/* One candidate n (< 2^127) through the native proving path of
+ * worker_sequential (v33:2112-2215) with the given log threshold: trial
+ * division by 101..409, root test, root check, then the forward walk from n
+ * (root) or the full chain from its true root (non-root).  Returns -1 when
+ * trial division rejects n, 0 when the root test does, -2 when the
+ * prefilter skips a root (its predicted ceiling is below log_threshold),
+ * else the chain length; root_out receives the root's hex, *is_root the
+ * root check.  Call ref33_setup first (trial batches, prefilter tables). */
+int ref33_prove_native(unsigned long long lo, unsigned long long hi, int log_threshold, char* root_out,
+                       int* is_root_out) {
+    u128 n128 = ((u128)hi << 64) | lo;
+    *is_root_out = 0;
+    root_out[0] = 0;
+    for (int tb = 0; tb < g_num_batches_extl2; tb++) {
+        unsigned long r = (unsigned long)(n128 % g_trial_batches_extl2[tb].product);
+        for (int j = 0; j < g_trial_batches_extl2[tb].count; j++)
+            if (r % TRIAL_PRIMES[g_trial_batches_extl2[tb].start + j] == 0) return -1;
+    }
+    if (!is_prime_root_native(n128)) return 0;
+    mpz_t n, pred, temp, temp2, root, cur, maxv, pp;
+    mpz_init(n); mpz_init(pred); mpz_init(temp); mpz_init(temp2); mpz_init(root); mpz_init(cur);
+    mpz_init(maxv); mpz_init(pp);
+    mpz_ui_pow_ui(maxv, 2, 127);
+    u128_to_mpz(n, n128);
+    int saved = g_wide_mode;
+    g_wide_mode = 0;
+    int len;
+    int is_root = is_chain_root_first(n, pred, temp);
+    if (!is_root) {
+        len = get_full_chain_length(n, maxv, root, pred, cur, temp, temp2, pp);
+        mpz_get_str(root_out, 16, root);
+    } else {
+        u32 pf[PREFILTER_PRIMES_COUNT];
+        int ceiling = prefilter_predict_ceiling(n, log_threshold, pf);
+        if (ceiling < log_threshold) {
+            len = -2;
+        } else {
+            len = follow_chain_first_screened(n, maxv, cur, temp, temp2, pp, pf, 1, NULL, NULL);
+        }
+        mpz_get_str(root_out, 16, n);
+    }
+    g_wide_mode = saved;
+    *is_root_out = is_root;
+    mpz_clear(n); mpz_clear(pred); mpz_clear(temp); mpz_clear(temp2); mpz_clear(root); mpz_clear(cur);
+    mpz_clear(maxv); mpz_clear(pp);
+    return len;
+}

@@ -22,6 +22,10 @@ reference itself (run in the container that holds the reference tree):
   * second_kind.json   -- the same for second-kind chains (v13b): self-test
                           vectors with GMP 2p - 1 walks and the v13b CPU
                           prover's output lines
+  * v33_native.json    -- the reference CPU engine's own proving path (root
+                          test, root check, backward / screened forward walks)
+                          on every survivor of seeded ranges of its lattice,
+                          and its screened walk of seeded numbers
   * cc16_windows.json  -- the oracle's survivor sets on 64+ seeded windows of
                           the depth-16 / primes-to-2^17 profile (W = 31#,
                           88-bit roots) holding at least 300 survivors in
@@ -30,7 +34,7 @@ reference itself (run in the container that holds the reference tree):
                           whose per-candidate test is itself pinned to the
                           reference's counters and kernels at 37..863
 
-Usage: python tests/golden/make_golden.py [--second-kind | --cc16-windows]
+Usage: python tests/golden/make_golden.py [--second-kind | --cc16-windows | --v33-native]
 (the reference fixtures need oracle/_ref built by `make -C oracle` and the
 reference tree in $CCS_REFERENCE_DIR).
 """
@@ -59,6 +63,12 @@ def reference_dir():
     if not os.path.isdir(os.path.join(d, "src")):
         sys.exit(f"reference tree not found at {d}: set CCS_REFERENCE_DIR")
     return d
+
+
+def dump_compact(name, obj):
+    with open(os.path.join(HERE, name), "w") as f:
+        json.dump(obj, f, separators=(",", ":"))
+    print("wrote", name)
 
 
 def dump(name, obj):
@@ -241,6 +251,57 @@ def second_kind():
                               "chains": known, "prover": prover})
 
 
+def v33_native():
+    """v33_native.json: the reference CPU engine's native proving path
+    (worker_sequential, v33:2112-2215) on every survivor of seeded ranges of
+    its own lattice (W = 31#, stages 37..61 / 67..97 at positions 0..L-1,
+    101..863 at 1..line_depth), and its screened walk (follow_chain_first,
+    v33:1512-1577) of the self-test vectors, the data-sample roots, the
+    walk-batch roots and small numbers near the screen primes."""
+    r33 = ob.ref33()
+    assert r33 is not None, "build oracle/_ref first (make -C oracle)"
+    runs = []
+    # (about 2,500 / 670 / 150 / 0.1 survivors per tile at targets 10 / 11 / 12 / 18)
+    for (target, line_depth, bits, seed, n_tiles) in [(10, 9, 61, 1, 1), (11, 10, 64, 2, 2),
+                                                       (12, 11, 72, 3, 8), (18, 17, 89, 4, 4000)]:
+        r33.ref33_setup(target, line_depth)
+        lat = ob.Lattice(lattice_len=target, depth=target,
+                         stages=[(ob.L2_PRIMES, 0), (ob.EXT_PRIMES, 0), (ob.LINE_PRIMES, 1)])
+        M, WP = lat.M, lat.WP
+        bases = lat.bases()
+        rr = random.Random(seed)
+        lo = (1 << (bits - 1)) // (M * WP) + 1
+        hi = (1 << bits) // (M * WP) - n_tiles - 1
+        ts = rr.randint(lo, hi)
+        surv = lat.filter_range(ts, n_tiles)
+        out = []
+        for b, k, t, _ in surv:
+            n = ((ts + int(t)) * WP + int(k)) * M + bases[int(b)]
+            code, root, is_root = ob.ref33_prove_native(r33, n, 1)
+            out.append([int(b), int(k), int(t), code, format(root, "x"), int(is_root)])
+        runs.append({"target": target, "line_depth": line_depth, "bits": bits, "tile_start": str(ts),
+                     "n_tiles": n_tiles, "survivors": out})
+        print(f"target {target} bits {bits}: {len(out)} survivors, "
+              f"{sum(1 for x in out if x[3] > 0 or x[3] == -2)} primes", flush=True)
+    r33.ref33_setup(18, 17)
+    walks = []
+    known = json.load(open(os.path.join(HERE, "known_roots.json")))["chains"]
+    nums = [int(c["root"]) for c in known]
+    nums += [int(x["root"], 16) for x in json.load(open(os.path.join(HERE, "cc10_sample.json")))["roots"]][:300]
+    nums += [int(x["n"]) for x in json.load(open(os.path.join(HERE, "walk_roots.json")))["roots"]][:300]
+    nums += [89, 179, 359, 719, 1439, 2879, 5, 11, 23, 47, 67, 137, 863, 1727]
+    for n in nums:
+        if n >= 1 << 127:
+            continue
+        walks.append([str(n), r33.ref33_follow_native(n & (2**64 - 1), n >> 64, 0)])
+    dump_compact("v33_native.json", {
+        "source": "cc_gmp_v33 native proving path (v33:2112-2215) and follow_chain_first "
+                  "(v33:1512-1577) via oracle/_ref/libref33.so; codes: -1 trial division, "
+                  "0 root test failed, -2 skipped by the prefilter (log threshold 1), "
+                  "else the chain length of the root",
+        "runs": runs, "walks": walks})
+
+
 CC16_WINDOW_TILES = 16384
 
 
@@ -294,6 +355,8 @@ def C_buf():
 if __name__ == "__main__":
     if "--cc16-windows" in sys.argv:
         cc16_windows()
+    elif "--v33-native" in sys.argv:
+        v33_native()
     elif "--second-kind" in sys.argv:
         second_kind()
     else:

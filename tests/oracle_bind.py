@@ -65,6 +65,9 @@ def _load_oracle():
                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.orc_reconstruct.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32,
                                     C.c_uint32, _u64p]
+    lib.orc_prove_v33.argtypes = [_u64p, C.c_int, C.c_int, C.c_int, _u64p, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int)]
+    lib.orc_chain_from_v33.argtypes = [_u64p, C.c_int, C.c_int, C.c_int]
     lib.orc_qiter_forbidden.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, C.c_int, C.c_int, _u32p]
     lib.orc_qiter_filter_seg.restype = C.c_uint64
     lib.orc_qiter_filter_seg.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64,
@@ -152,6 +155,24 @@ def prove_n(n, bits, mode=1, primality=PRIME_BPSW, witnesses=V13_WITNESSES, kind
     if r < 0:
         return None, bool(isp.value)
     return (r, words_to_int(root), bool(flags.value & 1)), bool(isp.value)
+
+
+def prove_v33(n, bits, target):
+    """The reference CPU engine's proving semantics (CCS_PRIME_V33) for one
+    candidate n: None or (chain_len, root, is_root), plus whether n passed
+    its root test."""
+    root = np.zeros(4, dtype=np.uint64)
+    flags = C.c_int(0)
+    isp = C.c_int(0)
+    r = oracle().orc_prove_v33(int_to_words(n), 4, bits, target, root, C.byref(flags), C.byref(isp))
+    if r < 0:
+        return None, bool(isp.value)
+    return (r, words_to_int(root), bool(flags.value & 1)), bool(isp.value)
+
+
+def chain_from_v33(n, wide=False, cap_bits=127):
+    """v33's walk of a given number: Baillie-PSW for it, then screened links."""
+    return oracle().orc_chain_from_v33(int_to_words(n), 4, int(wide), cap_bits)
 
 
 class Lattice:
@@ -254,7 +275,22 @@ def ref33():
     lib.ref33_is_root.argtypes = [C.c_char_p]
     lib.ref_gmp_forward_chain.argtypes = [C.c_char_p]
     lib.ref_gmp_forward_chain2.argtypes = [C.c_char_p]
+    lib.ref33_follow_native.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_int]
+    lib.ref33_root_native.argtypes = [C.c_ulonglong, C.c_ulonglong]
+    lib.ref33_fermat2_native.argtypes = [C.c_ulonglong, C.c_ulonglong]
+    lib.ref33_prove_native.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_int, C.c_char_p,
+                                       C.POINTER(C.c_int)]
     return lib
+
+
+def ref33_prove_native(lib, n, log_threshold=1):
+    """The reference CPU engine's native proving path on one candidate (see
+    oracle/ref/v33_harness.c): (code or chain length, root, is_root)."""
+    buf = C.create_string_buffer(64)
+    isr = C.c_int(0)
+    r = lib.ref33_prove_native(n & (2**64 - 1), n >> 64, log_threshold, buf, C.byref(isr))
+    root = int(buf.value, 16) if buf.value else 0
+    return r, root, bool(isr.value)
 
 
 def ref15():
