@@ -310,16 +310,18 @@ def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
             "cpu_baseline": cpu, "walk_vs_gmp": walk_mm}
 
 
-def autotune_engines(ccs, engines, seed):
-    """Project autotuner on every depth profile: probe of ~2^30 candidates at
-    a seeded 88-bit start (before any batch holds the engines)."""
+def autotune_engines(ccs, engines, seed, probe_log2=34):
+    """Project autotuner on every depth profile (before any batch holds the
+    engines): a probe of 2^probe_log2 candidates, the longest range of the
+    mixed workloads, at a seeded 88-bit start; the lattice threshold is
+    searched on its prefixes down to 1/64 of it."""
     import random
     r = random.Random(seed)
     out = []
     t0 = time.time()
     for e in engines:
         info = e.info
-        nt = max(1024, (1 << 30) // info["candidates_per_tile"])
+        nt = max(1024, (1 << probe_log2) // info["candidates_per_tile"])
         lo, hi = ccs.bit_tile_range(88, e.bases(), info["lattice_m"], info["wheel_period"])
         chosen, pts = e.autotune(r.randint(lo, hi - nt - 1), nt)
         out.append({"depth": info["depth"], "chosen": chosen, "points": len(pts)})
@@ -452,6 +454,155 @@ def qiter_plan(ccs, qi, steps, segs_per_step):
     return [qi.random_segments(segs_per_step, QITER_CFG["chunk"], QITER_CFG["bits_min"],
                                QITER_CFG["bits_max"], seed=SEED + 71 + i, start_variant=i * segs_per_step)
             for i in range(steps)]
+
+
+def v33_prefix_range(bits, prefix_value, prefix_bits, bases, M, WP):
+    """The candidates cc_gmp_v33 --prefix P --sequential --bits B visits
+    (v33:2994-3061, 1783-1793, 2108-2114): k = tile WP + k_offset in
+    [k_min, k_max) and n in [n_min, n_max], over the tiles [t0, t1)."""
+    shift = bits - prefix_bits
+    n_min = max(prefix_value << shift, 1 << (bits - 1))
+    n_max = min(((prefix_value + 1) << shift) - 1, (1 << bits) - 1)
+    k_min = -(-(n_min - max(bases)) // M) if n_min > max(bases) else 0
+    k_max = (n_max - min(bases)) // M
+    return k_min // WP, -(-k_max // WP), k_min, k_max, n_min, n_max
+
+
+def v33_prove_run(bits, target, prefix_bits, seed, threads, log_threshold=6):
+    """cc_gmp_v33 (the reference CPU engine, filter + prove) on a sequential
+    prefix range; returns its figures and its chain lines as (len, root,
+    is_root)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "cc_gmp_v33")
+    if not os.path.exists(exe):
+        return None
+    pv = (1 << (prefix_bits - 1)) | (seed & ((1 << (prefix_bits - 1)) - 1))
+    prefix = "0b" + format(pv, "b")
+    r = subprocess.run([exe, "--prefix", prefix, "--sequential", "--bits", str(bits), "--target", str(target),
+                        "--line-depth", str(target - 1), "--log", str(log_threshold), "--threads", str(threads)],
+                       capture_output=True, text=True, timeout=900)
+    out = r.stdout
+    lines = [(int(m.group(1)), int(m.group(2), 16), True)
+             for m in re.finditer(r"\*\*\* CC(\d+)a FOUND! 0x([0-9a-fA-F]+)", out)]
+    lines += [(int(m.group(1)), int(m.group(2), 16), False)
+              for m in re.finditer(r"\[NON-ROOT\] CC(\d+)a elem, root: 0x([0-9a-fA-F]+)", out)]
+    return {"prefix": prefix, "prefix_value": pv, "prefix_bits": prefix_bits,
+            "candidates": int(re.search(r"Wheel candidates \(L1\):\s+(\d+)", out).group(1)),
+            "primes": int(re.search(r"Primes found:\s+(\d+)", out).group(1)),
+            "seconds": float(re.search(r"Time: ([\d.]+) seconds", out).group(1)),
+            "lines": sorted(lines)}
+
+
+def section_cpu_method(ccs, torch, dev, local, seconds_goal=8.0):
+    """BASELINE's CPU-method configuration and the reference CPU engine
+    beside it.
+
+    GPU: lattice W = 23#, depth 8, filter primes 29..1021 at positions 0..7,
+    a seed-drawn 60-bit block offset (88-bit n), 1e9 candidates; every
+    survivor proved with the reference CPU engine's own tests
+    (CCS_PRIME_V33, full prove: true roots and lengths), chains >= 6
+    counted.  CPU: cc_gmp_v33 --target 8 --line-depth 7 --log 6 on all host
+    cores over a sequential prefix range of 61-bit n, sized for about
+    seconds_goal, on its own lattice (W = 31#, stages 37..61 / 67..97 /
+    101..863); the engine then runs the same lattice, stages, tests and
+    range, and its prime count and chain lines (>= 6) are compared with the
+    reference's output."""
+    import random
+    import numpy as np
+    cores = os.cpu_count() or 1
+    r = random.Random(SEED + 81)
+    # ---- GPU, config 1 ----
+    cfg = ccs.config_cpu_method()
+    probe = ccs.Engine(device=local, **cfg)
+    info = probe.info
+    cpt = info["candidates_per_tile"]
+    probe.close()
+    j0 = r.getrandbits(59) | (1 << 59)                 # 60-bit block offset
+    ts = 6 * j0
+    tiles = -(-10**9 // cpt)
+    n0 = ts * info["wheel_period"] * info["lattice_m"]
+    bits = n0.bit_length()
+    cfg["bits"] = bits
+    eng = ccs.Engine(device=local, primality=ccs.PRIME_V33, prove_mode=ccs.PROVE_FULL, **cfg)
+    stream = torch.cuda.Stream(device=dev)
+    surv = torch.empty((1 << 23, 4), dtype=torch.int32, device=dev)
+    chains = torch.empty((1 << 22, 12), dtype=torch.int32, device=dev)
+    best = None
+    for rep in range(3):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s_ = eng.filter_range(ts, tiles, out=surv, stream=stream)
+        e1.record(stream)
+        c_, p_ = eng.prove(s_, ts, out=chains, stream=stream)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        t = (e0.elapsed_time(e2), e0.elapsed_time(e1), s_.shape[0], c_.shape[0], p_)
+        if rep > 0 and (best is None or t[0] < best[0]):
+            best = t
+    lens = chains[:best[3]].cpu().numpy()[:, 3] if best[3] else np.zeros(0)
+    eng.close()
+    cand = tiles * cpt
+    gpu = {"workload": f"W = 23#, depth 8, primes 29..1021 at positions 0..7, {bits}-bit n from a "
+                       f"seed-drawn 60-bit block offset, {cand} candidates",
+           "candidates_per_s": cand / (best[0] * 1e-3), "filter_candidates_per_s": cand / (best[1] * 1e-3),
+           "ms": best[0], "survivors": best[2], "primes": best[4],
+           "proofs_per_s": best[4] / (best[0] * 1e-3),
+           "chains_ge6": int((lens >= 6).sum()), "predicate": "CCS_PRIME_V33 (the reference CPU engine's)"}
+    # ---- reference CPU engine, and the engine on its range ----
+    out = {"gpu_config1": gpu}
+    ref_bits, target = 61, 8
+    e_ref = ccs.Engine(device=local, target=target, depth=target, bits=ref_bits,
+                       stages=ccs.reference_cpu_stages(), primality=ccs.PRIME_V33,
+                       prove_mode=ccs.PROVE_FULL)
+    rinfo = e_ref.info
+    bases = e_ref.bases()
+    M, WP = rinfo["lattice_m"], rinfo["wheel_period"]
+    # about 2.5e8 candidates per second on 16 cores at target 8: size the range
+    want = 2.5e8 / 16 * cores * seconds_goal
+    pbits = 2
+    while pbits < ref_bits - 1:
+        t0_, t1_ = v33_prefix_range(ref_bits, 1 << (pbits - 1), pbits, bases, M, WP)[:2]
+        if (t1_ - t0_) * rinfo["candidates_per_tile"] <= want:
+            break
+        pbits += 1
+    ref = v33_prove_run(ref_bits, target, pbits, SEED + 83, cores)
+    if ref is None:
+        out["reference_cpu"] = {"unavailable": "oracle/_ref/cc_gmp_v33 not built"}
+        e_ref.close()
+        return out
+    t0, t1, k_min, k_max, n_min, n_max = v33_prefix_range(ref_bits, ref["prefix_value"], ref["prefix_bits"],
+                                                         bases, M, WP)
+    n_t = t1 - t0
+    s_ = e_ref.filter_range(t0, n_t, cap=1 << 26)
+    c_, p_ = e_ref.prove(s_, t0, cap=1 << 24)
+    e_ref.close()
+    a = c_.cpu().numpy().astype(np.int64) & 0xFFFFFFFF
+    ours, primes_in = [], 0
+    for rec in a:
+        k = (t0 + int(rec[2])) * WP + int(rec[1])
+        n = k * M + bases[int(rec[0])]
+        if not (k_min <= k < k_max and n_min <= n <= n_max):
+            continue
+        primes_in += 1
+        if rec[3] >= 6:
+            root = sum(int(rec[4 + w]) << (32 * w) for w in range(6))
+            ours.append((int(rec[3]), root, bool(rec[10] & 1)))
+    ours.sort()
+    out["reference_cpu"] = {
+        "value": ref["candidates"] / ref["seconds"], "unit": "candidates/s", "cores": cores,
+        "cpu_model": cpu_model(), "kind": "reference",
+        "sample": (f"cc_gmp_v33 --prefix {ref['prefix']} --sequential --bits {ref_bits} --target {target} "
+                   f"--line-depth {target - 1} --log 6 --threads {cores}: {ref['candidates']} candidates, "
+                   f"{ref['primes']} primes, {len(ref['lines'])} chain lines in {ref['seconds']:.1f} s"),
+        "proofs_per_s": ref["primes"] / ref["seconds"]}
+    out["parity_vs_reference_cpu"] = {
+        "tiles": n_t, "engine_candidates": n_t * rinfo["candidates_per_tile"],
+        "reference_candidates": ref["candidates"], "engine_primes": primes_in,
+        "reference_primes": ref["primes"], "chain_lines_ge6": len(ref["lines"]),
+        "chain_lines_equal": ours == ref["lines"],
+        "lines_only_in_reference": len(set(ref["lines"]) - set(ours)),
+        "lines_only_in_engine": len(set(ours) - set(ref["lines"]))}
+    return out
 
 
 def section_qiter(ccs, torch, dev, local, steps=8, segs_per_step=256):
@@ -609,7 +760,13 @@ def section_served(ccs, engines, n_req=2048, lam=2000.0, batch_tuning=None):
     th = threading.Thread(target=submitter)
     th.start()
     th.join()
+    # backlog when the last request arrived: queued (not admitted) requests
+    # and admitted ones not yet done
+    st_last = srv.stats()
+    backlog = {"pending": st_last["pending"],
+               "admitted_not_done": st_last["admitted"] - st_last["completed"] - st_last["cancelled"]}
     lat = []
+    waits = []
     first, last = 1e30, 0
     served_sets = []
     for rid in ids:
@@ -617,14 +774,19 @@ def section_served(ccs, engines, n_req=2048, lam=2000.0, batch_tuning=None):
         st, res, sv, ch = srv.poll(rid, surv_cap=1 << 16, chain_cap=1 << 14)
         served_sets.append((record_set(sv, 3), record_set(ch, 11)))
         lat.append(res["done_s"] - res["submit_s"])
+        waits.append(res["admit_s"] - res["submit_s"])
         first = min(first, res["submit_s"])
         last = max(last, res["done_s"])
         cand_total += res["candidates"]
     stats = srv.stats()
+    mem_now, mem_peak = srv.memory()
     srv.close()
     served = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+              "admission_wait_p50_s": float(np.percentile(waits, 50)),
+              "admission_wait_p99_s": float(np.percentile(waits, 99)),
               "candidates_per_s": cand_total / (last - first), "makespan_s": last - first,
-              "ticks": stats["ticks"]}
+              "ticks": stats["ticks"], "backlog_at_last_arrival": backlog,
+              "device_bytes_reserved_peak": mem_peak}
 
     # plain: one request at a time in arrival order
     lat_p = []
@@ -729,12 +891,13 @@ def run_ours(args):
     info = eng.info
     tune_report = None
     if not args.no_autotune:
-        # project autotuner on a 2^22-tile probe away from the timed tiles
+        # project autotuner on a probe away from the timed tiles
         bases0 = eng.bases()
         lo0, hi0 = ccs.bit_tile_range(BITS, bases0, info["lattice_m"], info["wheel_period"])
         t_tune = time.time()
-        chosen, pts = eng.autotune(lo0 + 1000, 1 << 22)
-        tune_report = {"probe_tiles": 1 << 22, "points": len(pts), "seconds": time.time() - t_tune}
+        # a probe as long as one step, so the unit length is tuned for it
+        chosen, pts = eng.autotune(lo0 + 1000, TILES)
+        tune_report = {"probe_tiles": TILES, "points": len(pts), "seconds": time.time() - t_tune}
     if args.unit_words:
         eng.set_tuning(unit_words=args.unit_words)
     if args.ext_min_words:
@@ -861,6 +1024,10 @@ def run_ours(args):
             extra["qiter"] = section_qiter(ccs, torch, dev, local)
         except Exception as ex:
             extra["qiter"] = {"error": repr(ex)}
+        try:
+            extra["cpu_method"] = section_cpu_method(ccs, torch, dev, local)
+        except Exception as ex:
+            extra["cpu_method"] = {"error": repr(ex)}
         depth_engines = [ccs.Engine(device=local, **ccs.config_depth_profile(d)) for d in range(14, 20)]
         if not args.no_autotune:
             try:
@@ -907,6 +1074,12 @@ def run_ours(args):
         rr = extra.get("reference_runs", {})
         mm["reference_kernels"] = {k: (v.get("reference_kernels") or {}).get("count_mismatches")
                                    for k, v in rr.items() if isinstance(v, dict)} if isinstance(rr, dict) else None
+        cm = extra.get("cpu_method", {})
+        par = cm.get("parity_vs_reference_cpu") if isinstance(cm, dict) else None
+        mm["cpu_method_vs_reference_cpu"] = (
+            {"chain_lines": par["lines_only_in_reference"] + par["lines_only_in_engine"],
+             "primes": abs(par["engine_primes"] - par["reference_primes"]),
+             "candidates": abs(par["engine_candidates"] - par["reference_candidates"])} if par else None)
         line["mismatches"] = mm
         print(json.dumps(line))
     if pg:
