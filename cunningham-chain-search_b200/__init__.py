@@ -175,6 +175,7 @@ _SIGS = {
     "ccs_filter_range": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
     "ccs_filter_range_noalloc": (C.c_int, [_vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64), _vp]),
     "ccs_plan_range": (C.c_int, [_vp, _u64, _u64, _u64, C.POINTER(_RangePlan)]),
+    "ccs_prove_stats": (C.c_int, [_vp, C.POINTER(_u64), C.c_int]),
     "ccs_prove": (C.c_int, [_vp, _vp, _u64, _u64, _u64, _vp, _u64, C.POINTER(_u64),
                             C.POINTER(_u64), _vp]),
     "ccs_set_bits": (C.c_int, [_vp, C.c_uint32]),
@@ -519,6 +520,13 @@ class Engine:
         _check(load_library().ccs_walk_numbers(self.h, dev.data_ptr(), len(numbers), limbs,
                                                out.data_ptr(), None), "ccs_walk_numbers")
         return out.cpu().numpy().astype(np.int64)
+
+    def prove_stats(self, reset=True):
+        """Staged-prove counters (ccs_prove_stats): survivors, primes n,
+        predecessor tests, roots decided by a birth certificate."""
+        out = (_u64 * 4)()
+        _check(load_library().ccs_prove_stats(self.h, out, int(reset)), "ccs_prove_stats")
+        return dict(zip(["survivors", "primes", "predecessor_tests", "certified_roots"], [int(x) for x in out]))
 
     def walk_modmuls(self, reset=True):
         """Montgomery products spent by walk launches since the last reset."""

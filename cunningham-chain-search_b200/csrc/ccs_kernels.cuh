@@ -179,6 +179,7 @@ struct StagedProve {
     uint32_t* chains;
     uint32_t* chain_count;
     uint32_t chain_cap;
+    uint32_t* certified;                 // roots decided by a birth certificate (no predecessor test)
 };
 // which: -1 seed, 0 after the top member, 1 after n, 2 after a predecessor, 3 emit
 cudaError_t launch_prove_stage(int which, const StagedProve& p, const WalkItem* in, uint32_t n,

@@ -121,6 +121,9 @@ struct ccs_engine {
     void* h_stage = nullptr;
     size_t h_stage_bytes = 0;
     uint64_t launches = 0;           // kernels launched by this engine
+    // staged proves: survivors, primes n, predecessor tests, roots decided
+    // by a birth certificate
+    uint64_t stats[4] = {0, 0, 0, 0};
 };
 
 struct ccs_batch {
@@ -919,6 +922,8 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
     p.chains = (uint32_t*)out_dev;
     p.chain_count = ctr + 3;
     p.chain_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFull);
+    p.certified = ctr + 4;
+    uint64_t pred_tests = 0;
     auto read_ctr = [&](int i) -> uint32_t {
         cudaMemcpyAsync(hc, ctr + i, 4, cudaMemcpyDeviceToHost, st);
         cudaStreamSynchronize(st);
@@ -950,6 +955,7 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
             CU(launch_prove_stage(stage, p, lists[cur], n, st));
             E->launches += 1;
             n = read_ctr(0);
+            if (stage == 1) pred_tests += n;                    // predecessors of the primes n
             cur ^= 1;
             if (stage < 2) stage++;
         }
@@ -963,10 +969,14 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
             E->launches += 1;
         }
     }
-    CU(cudaMemcpyAsync(hc, ctr + 2, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(hc, ctr + 2, 12, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
     *n_out = hc[1];
     if (primes_out) *primes_out = hc[0];
+    E->stats[0] += n_surv;
+    E->stats[1] += hc[0];
+    E->stats[2] += pred_tests;
+    E->stats[3] += hc[2];
     if (hc[1] > cap) return fail(CCS_OVERFLOW, "chain capacity exceeded");
     return CCS_OK;
 }
@@ -1088,6 +1098,13 @@ ccs_status ccs_plan_range(const ccs_engine* E, uint64_t ts_lo, uint64_t ts_hi, u
     if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
     out->grid = grid;
     out->block_threads = E->tune.block_threads;
+    return CCS_OK;
+}
+
+ccs_status ccs_prove_stats(ccs_engine* E, uint64_t* out4, int reset) {
+    if (!E || !out4) return fail(CCS_ERR_INVALID, "null argument");
+    for (int i = 0; i < 4; i++) out4[i] = E->stats[i];
+    if (reset) for (int i = 0; i < 4; i++) E->stats[i] = 0;
     return CCS_OK;
 }
 

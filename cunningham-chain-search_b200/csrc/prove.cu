@@ -670,6 +670,10 @@ __device__ int walk_forward(Big cur, const ProveConst& pc, uint32_t link_pred, b
     return len;
 }
 
+// staged prove: per-survivor flag set by the seed kernel (cleared to the
+// record flags when n tests prime)
+constexpr uint32_t kFlagCertificate = 1u << 8;
+
 __constant__ uint32_t c_screen[132] = {
     67, 71, 73, 79, 83, 89, 97, 101, 103, 107, 109, 113, 127, 131, 137, 139, 149, 151,
     157, 163, 167, 173, 179, 181, 191, 193, 197, 199, 211, 223, 227, 229, 233, 239, 241,
@@ -717,6 +721,25 @@ __device__ __forceinline__ RangePreds range_preds(const ProveConst& pc, uint32_t
 __device__ __forceinline__ void trial_list(const ProveConst& pc, uint32_t& t0, uint32_t& t1) {
     if (pc.primality == CCS_PRIME_V33) { t0 = 7; t1 = 62; }
     else { t0 = 0; t1 = pc.prove_mode == CCS_PROVE_ROOTS ? 132u : 62u; }   // v13:1499 / 1832
+}
+
+// Trial division of n before its root test, together with the birth
+// certificate of v34 (v34:70-77, 2598-2612): when n == 1 (mod q) for a screen
+// prime q (second kind: n == -1), q divides the predecessor (n -/+ 1) / 2,
+// which is then composite (it is larger than q for every n above 1727), so n
+// is a root without a primality test of its predecessor.  Returns false when
+// trial division rejects n; *cert receives the certificate.
+__device__ __forceinline__ bool trial_and_certificate(const Big& nb, const ProveConst& pc, uint32_t t0,
+                                                      uint32_t t1, bool& cert) {
+    cert = false;
+    for (uint32_t t = 0; t < 132; t++) {
+        const uint32_t q = c_screen[t];
+        const uint32_t r = big_mod_small(nb, q);
+        if (r == 0 && t >= t0 && t < t1) return false;
+        cert |= r == (pc.kind == 2 ? q - 1 : 1u);
+    }
+    cert &= !big_lt_u32(nb, 1728);
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -846,9 +869,8 @@ prove_kernel(ProveArgs a) {
         // position 0 already, so for them it is skipped
         uint32_t t0 = 0, t1 = 0;
         if (!a.q.seg) trial_list(pc, t0, t1);
-        bool comp = false;
-        for (uint32_t t = t0; t < t1 && !comp; t++) comp = big_mod_small(nb, c_screen[t]) == 0;
-        if (comp) continue;
+        bool cert = false;
+        if (!trial_and_certificate(nb, pc, t0, t1, cert)) continue;
         const RangePreds rp = range_preds(pc, R.bits, R.target);
         uint32_t mm = 0;
         if (pc.reverse) {
@@ -868,7 +890,7 @@ prove_kernel(ProveArgs a) {
         bool is_root = true;
         Big pred = nb;
         big_prev(pred, pc.kind);
-        if (!big_lt_u32(pred, 2) && is_prime_dev(pred, pc, mm)) {
+        if (!cert && !big_lt_u32(pred, 2) && is_prime_dev(pred, pc, mm)) {
             is_root = false;
             if (pc.prove_mode == CCS_PROVE_ROOTS) continue;              // v13:1513-1516
             root = pred;
@@ -1158,10 +1180,12 @@ prove_seed_kernel(StagedProve p) {
                 nb = survivor_number(sv, R, pc);
                 keep = big_bits(nb) == (int)R.bits;                              // v13:1495, 1828
             }
-            for (uint32_t t = t0; t < t1 && keep; t++) keep = big_mod_small(nb, c_screen[t]) != 0;
+            bool cert = false;
+            if (keep) keep = trial_and_certificate(nb, pc, t0, t1, cert);
             x = nb;
             if (keep) {
                 big_store(p.nval + (size_t)i * kMaxLimbs, nb);
+                p.flags[i] = cert ? kFlagCertificate : 0u;
                 if (pc.reverse) {
                     // chain position target - 1 first (v15:1704-1708)
                     const int pos = R.target - 1 < 63 ? (int)R.target - 1 : 63;
@@ -1201,10 +1225,18 @@ prove_select_kernel(StagedProve p, const WalkItem* in, uint32_t n_in, int stage)
                     atomicAdd(p.primes, 1u);
                     const Big nb = big_load(p.nval + (size_t)idx * kMaxLimbs);
                     big_store(p.root + (size_t)idx * kMaxLimbs, nb);
+                    const bool cert = p.flags[idx] & kFlagCertificate;
                     p.flags[idx] = CCS_CHAIN_IS_ROOT;
                     x = nb;
                     big_prev(x, pc.kind);
-                    if (big_lt_u32(x, 2)) to_fwd = true; else emit = true;
+                    if (big_lt_u32(x, 2)) {
+                        to_fwd = true;
+                    } else if (cert) {
+                        to_fwd = true;                     // birth certificate: the predecessor is composite
+                        atomicAdd(p.certified, 1u);
+                    } else {
+                        emit = true;
+                    }
                 }
             } else {
                 if (prime) {

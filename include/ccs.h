@@ -430,6 +430,14 @@ ccs_status ccs_measure_int32_peak(int device, double* tops);
  * ops/s: the roofline denominator of the Montgomery prover. */
 ccs_status ccs_measure_imad_peak(int device, double* tops);
 
+/* Counters of the staged proves (ccs_prove from 256 survivors on) of this
+ * engine since the last reset: [0] survivors, [1] survivors whose n tested
+ * prime, [2] primality tests of those n's predecessors, [3] n found to be
+ * roots by a birth certificate instead (n == 1 mod a screen prime 67..863 --
+ * second kind: n == -1 -- makes the predecessor a multiple of it; v34:70-77,
+ * 2598-2612). */
+ccs_status ccs_prove_stats(ccs_engine* eng, uint64_t* out4, int reset);
+
 /* Montgomery products executed by ccs_walk_numbers launches on this device
  * since the last reset (reset != 0 clears after reading). */
 ccs_status ccs_walk_modmuls(ccs_engine* eng, uint64_t* count, int reset);

@@ -251,3 +251,28 @@ def test_staged_prove_equals_per_survivor_prove(ccs, cfg):
     assert p_whole == p_parts
     assert key(whole) == key(parts) and whole.shape[0] > 0
     eng.close()
+
+
+def test_birth_certificates_replace_predecessor_tests(ccs, ob):
+    """A prime n == 1 (mod q) for a screen prime q has a predecessor divisible
+    by q (v34:70-77): the staged prove marks it a root without testing the
+    predecessor.  Records still equal the oracle's full predecessor tests;
+    every prime n is either certified or has its predecessor tested."""
+    lat = ob.Lattice()
+    eng = ccs.Engine(bits=61)
+    ts = (1 << 60) // (20677 * 1616615) + 4321
+    surv = eng.filter_range(ts, 3000)
+    assert surv.shape[0] >= 256                       # staged path
+    eng.prove_stats(reset=True)
+    chains, primes = eng.prove(surv, ts)
+    st = eng.prove_stats(reset=True)
+    assert st["survivors"] == surv.shape[0] and st["primes"] == primes
+    assert st["predecessor_tests"] + st["certified_roots"] == primes
+    assert st["certified_roots"] > 0.2 * primes
+    want = []
+    for b, k, t, _ in np.asarray(surv.cpu().numpy()).astype(np.int64):
+        res, _ = ob.prove_n(lat.reconstruct(ts, b, k, t), 61, mode=1)
+        if res is not None:
+            want.append(ccs.format_chain_line(res[0], res[1], 18, res[2]))
+    assert _lines(ccs, chains, 18) == sorted(want)
+    eng.close()
