@@ -242,7 +242,7 @@ def gmp_walk_baseline(roots, seconds_goal=10.0):
             lengths)
 
 
-def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
+def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256, cpu=True):
     """Prove batch: 2^24 roots of 80..110 bits pre-filtered by every prime
     < 2^17 at chain positions 0..15 (survivors of the cc16 filter at seeded
     widths), walked p -> 2p+1 until the first composite (BPSW)."""
@@ -291,7 +291,7 @@ def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256):
     # IMAD ops: one lo/hi pair per 32x32-bit word product, counted on the device
     ops_per_mm = 2.0 * words / max(mm, 1)
     achieved = 2.0 * words / (ms * 1e-3) / 1e12
-    cpu, gmp_len = gmp_walk_baseline(roots[:20000])
+    cpu, gmp_len = gmp_walk_baseline(roots[:20000]) if cpu else (None, None)
     walk_mm = None
     if gmp_len is not None:
         walk_mm = {"compared": len(gmp_len),
@@ -1107,7 +1107,7 @@ def main():
                     help="skip the prove-batch, batched and served sections")
     ap.add_argument("--batch-ranges", type=int, default=4096)
     ap.add_argument("--served-requests", type=int, default=2048)
-    ap.add_argument("--only", choices=["qiter"], default=None,
+    ap.add_argument("--only", choices=["qiter", "prove"], default=None,
                     help="run one section alone and print its JSON (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -1121,6 +1121,14 @@ def main():
             print(json.dumps(reference_qiter()))
         else:
             print(json.dumps(section_qiter(ccs, torch, torch.device("cuda:0"), 0, steps=args.steps)))
+        return 0
+    if args.only == "prove":
+        import importlib
+        import torch
+        ccs = importlib.import_module("cunningham-chain-search_b200")
+        eng = ccs.Engine(device=0, **ccs.config_cc16_scale())
+        print(json.dumps(section_prove(ccs, torch, eng, torch.device("cuda:0"), 0, cpu=not args.no_cpu_baseline)))
+        eng.close()
         return 0
     if args.impl == "reference":
         return run_reference(args)

@@ -159,7 +159,10 @@ struct WalkArgs {
 };
 cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
                              WalkItem* out, cudaStream_t st);
-cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, cudaStream_t st);
+// round_pred: the test of this round's members (every member of a round is
+// either a walk start / stage member or a forward link)
+cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, uint32_t round_pred,
+                              cudaStream_t st);
 
 // staged prove of one range's survivors (prove.cu)
 struct StagedProve {

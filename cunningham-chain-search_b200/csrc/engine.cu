@@ -815,13 +815,12 @@ static WalkPreds walk_preds(const HostProfile& hp, bool root_role, uint32_t bits
     return w;
 }
 
+// first_len: the chain length the members of round 0 carry (0: walk starts,
+// 1: forward links from a root); members of round r carry first_len + r
 static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint32_t max_len,
-                              const WalkPreds& wp, cudaStream_t st) {
+                              const WalkPreds& wp, uint32_t first_len, cudaStream_t st) {
     WalkState* hs = (WalkState*)((char*)E->h_stage + 12288);
-    auto needs_second = [&](uint32_t p) {
-        return p == kPredBPSW || p == kPredMR235 || (p == kPredMR && E->hp.witnesses.size() > 1);
-    };
-    const bool two_stage = needs_second(wp.pred) || (wp.screen && needs_second(wp.link_pred));
+
     WalkItem* act = E->w_act.p;
     WalkItem* nxt = E->w_next.p;
     uint32_t n_act = n;
@@ -843,8 +842,11 @@ static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint
         a.code = E->w_code.p;
         a.lengths = lengths;
         a.profile = E->slot;
-        CU(launch_walk_round(a, n_act, two_stage, st));
-        E->launches += two_stage ? 5 : 4;
+        const uint32_t rp = (wp.screen && first_len + round >= 1) ? wp.link_pred : wp.pred;
+        const bool second = rp == kPredBPSW || rp == kPredMR235 ||
+                            (rp == kPredMR && E->hp.witnesses.size() > 1);
+        CU(launch_walk_round(a, n_act, second, rp, st));
+        E->launches += second ? 5 : 4;
         CU(cudaMemcpyAsync(hs, &E->w_state.p->n_next, 4, cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         n_act = hs->n_act;
@@ -874,7 +876,7 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
         E->launches += 1;
         // the walk of a given number tests it as a walk start (v33
         // follow_chain_first: is_prime_fast, v33:1535-1540), then its links
-        ccs_status s = walk_rounds(E, cn, lengths_dev, kMaxChain, walk_preds(E->hp, false, E->hp.bits), st);
+        ccs_status s = walk_rounds(E, cn, lengths_dev, kMaxChain, walk_preds(E->hp, false, E->hp.bits), 0, st);
         if (s != CCS_OK) return s;
     }
     CU(cudaStreamSynchronize(st));
@@ -947,7 +949,7 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
                 // member and predecessors
                 WalkPreds wp = walk_preds(E->hp, stage == 1, bits);
                 wp.screen = false;
-                ccs_status s = walk_rounds(E, n, p.lengths, 1, wp, st);
+                ccs_status s = walk_rounds(E, n, p.lengths, 1, wp, 0, st);
                 if (s != CCS_OK) return s;
             }
             CU(cudaMemsetAsync(ctr, 0, 4, st));
@@ -963,7 +965,7 @@ static ccs_status prove_staged(ccs_engine* E, const ccs_survivor* surv_dev, uint
         const uint32_t nr = read_ctr(1);
         if (nr) {
             CU(cudaMemcpyAsync(E->w_act.p, E->p_fwd.p, sizeof(WalkItem) * nr, cudaMemcpyDeviceToDevice, st));
-            ccs_status s = walk_rounds(E, nr, p.lengths, kMaxChain, walk_preds(E->hp, false, bits), st);
+            ccs_status s = walk_rounds(E, nr, p.lengths, kMaxChain, walk_preds(E->hp, false, bits), 1, st);
             if (s != CCS_OK) return s;
             CU(launch_prove_stage(3, p, E->p_fwd.p, nr, st));
             E->launches += 1;

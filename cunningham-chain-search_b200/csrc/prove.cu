@@ -236,7 +236,8 @@ __device__ __forceinline__ void halfmod(uint32_t (&x)[NL], const uint32_t (&n)[N
     }
 }
 
-// CIOS Montgomery product r = a b R^{-1} mod n (a, b < n)
+// CIOS Montgomery product r = a b R^{-1} mod n (a, b < n); the portable
+// definition, specialised below for every limb count the prover uses
 template <int NL>
 __device__ __forceinline__ void montmul(uint32_t (&r)[NL], const uint32_t (&a)[NL],
                                         const uint32_t (&b)[NL], const uint32_t (&n)[NL],
@@ -275,6 +276,228 @@ __device__ __forceinline__ void montmul(uint32_t (&r)[NL], const uint32_t (&a)[N
 #pragma unroll
     for (int i = 0; i < NL; i++) r[i] = res[i];
 }
+
+// The products actually used: CIOS with the carry chains written out in PTX
+// (mad.lo/hi.cc, madc), one row of a_i * b and one of m * n per limb: 4 NL + 5
+// instructions a row instead of the 64-bit sums above.  Generated for the
+// limb counts 2..6 from one pattern: t (NL + 2 words) += x * v for x a word
+// and v an NL-word vector, low halves then high halves, each a single carry
+// chain.
+template <>
+__device__ __forceinline__ void montmul<2>(uint32_t (&r)[2], const uint32_t (&a)[2],
+                                           const uint32_t (&b)[2], const uint32_t (&n)[2],
+                                           uint32_t ninv) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const uint32_t ai = a[i];
+        asm(
+            "mad.lo.cc.u32 %0, %4, %5, %0;\n\t"
+            "madc.lo.cc.u32 %1, %4, %6, %1;\n\t"
+            "addc.cc.u32 %2, %2, 0;\n\t"
+            "addc.u32 %3, %3, 0;\n\t"
+            "mad.hi.cc.u32 %1, %4, %5, %1;\n\t"
+            "madc.hi.cc.u32 %2, %4, %6, %2;\n\t"
+            "addc.u32 %3, %3, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3)
+            : "r"(ai), "r"(b[0]), "r"(b[1]));
+        const uint32_t m = t0 * ninv;
+        asm(
+            "mad.lo.cc.u32 %0, %4, %5, %0;\n\t"
+            "madc.lo.cc.u32 %1, %4, %6, %1;\n\t"
+            "addc.cc.u32 %2, %2, 0;\n\t"
+            "addc.u32 %3, %3, 0;\n\t"
+            "mad.hi.cc.u32 %1, %4, %5, %1;\n\t"
+            "madc.hi.cc.u32 %2, %4, %6, %2;\n\t"
+            "addc.u32 %3, %3, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3)
+            : "r"(m), "r"(n[0]), "r"(n[1]));
+        t0 = t1; t1 = t2; t2 = t3; t3 = 0;
+    }
+    r[0] = t0; r[1] = t1;
+    if (t2 || ge<2>(r, n)) sub_n<2>(r, r, n);
+}
+
+template <>
+__device__ __forceinline__ void montmul<3>(uint32_t (&r)[3], const uint32_t (&a)[3],
+                                           const uint32_t (&b)[3], const uint32_t (&n)[3],
+                                           uint32_t ninv) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const uint32_t ai = a[i];
+        asm(
+            "mad.lo.cc.u32 %0, %5, %6, %0;\n\t"
+            "madc.lo.cc.u32 %1, %5, %7, %1;\n\t"
+            "madc.lo.cc.u32 %2, %5, %8, %2;\n\t"
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.u32 %4, %4, 0;\n\t"
+            "mad.hi.cc.u32 %1, %5, %6, %1;\n\t"
+            "madc.hi.cc.u32 %2, %5, %7, %2;\n\t"
+            "madc.hi.cc.u32 %3, %5, %8, %3;\n\t"
+            "addc.u32 %4, %4, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4)
+            : "r"(ai), "r"(b[0]), "r"(b[1]), "r"(b[2]));
+        const uint32_t m = t0 * ninv;
+        asm(
+            "mad.lo.cc.u32 %0, %5, %6, %0;\n\t"
+            "madc.lo.cc.u32 %1, %5, %7, %1;\n\t"
+            "madc.lo.cc.u32 %2, %5, %8, %2;\n\t"
+            "addc.cc.u32 %3, %3, 0;\n\t"
+            "addc.u32 %4, %4, 0;\n\t"
+            "mad.hi.cc.u32 %1, %5, %6, %1;\n\t"
+            "madc.hi.cc.u32 %2, %5, %7, %2;\n\t"
+            "madc.hi.cc.u32 %3, %5, %8, %3;\n\t"
+            "addc.u32 %4, %4, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4)
+            : "r"(m), "r"(n[0]), "r"(n[1]), "r"(n[2]));
+        t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = 0;
+    }
+    r[0] = t0; r[1] = t1; r[2] = t2;
+    if (t3 || ge<3>(r, n)) sub_n<3>(r, r, n);
+}
+
+template <>
+__device__ __forceinline__ void montmul<4>(uint32_t (&r)[4], const uint32_t (&a)[4],
+                                           const uint32_t (&b)[4], const uint32_t (&n)[4],
+                                           uint32_t ninv) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const uint32_t ai = a[i];
+        asm(
+            "mad.lo.cc.u32 %0, %6, %7, %0;\n\t"
+            "madc.lo.cc.u32 %1, %6, %8, %1;\n\t"
+            "madc.lo.cc.u32 %2, %6, %9, %2;\n\t"
+            "madc.lo.cc.u32 %3, %6, %10, %3;\n\t"
+            "addc.cc.u32 %4, %4, 0;\n\t"
+            "addc.u32 %5, %5, 0;\n\t"
+            "mad.hi.cc.u32 %1, %6, %7, %1;\n\t"
+            "madc.hi.cc.u32 %2, %6, %8, %2;\n\t"
+            "madc.hi.cc.u32 %3, %6, %9, %3;\n\t"
+            "madc.hi.cc.u32 %4, %6, %10, %4;\n\t"
+            "addc.u32 %5, %5, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5)
+            : "r"(ai), "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]));
+        const uint32_t m = t0 * ninv;
+        asm(
+            "mad.lo.cc.u32 %0, %6, %7, %0;\n\t"
+            "madc.lo.cc.u32 %1, %6, %8, %1;\n\t"
+            "madc.lo.cc.u32 %2, %6, %9, %2;\n\t"
+            "madc.lo.cc.u32 %3, %6, %10, %3;\n\t"
+            "addc.cc.u32 %4, %4, 0;\n\t"
+            "addc.u32 %5, %5, 0;\n\t"
+            "mad.hi.cc.u32 %1, %6, %7, %1;\n\t"
+            "madc.hi.cc.u32 %2, %6, %8, %2;\n\t"
+            "madc.hi.cc.u32 %3, %6, %9, %3;\n\t"
+            "madc.hi.cc.u32 %4, %6, %10, %4;\n\t"
+            "addc.u32 %5, %5, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5)
+            : "r"(m), "r"(n[0]), "r"(n[1]), "r"(n[2]), "r"(n[3]));
+        t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = t5; t5 = 0;
+    }
+    r[0] = t0; r[1] = t1; r[2] = t2; r[3] = t3;
+    if (t4 || ge<4>(r, n)) sub_n<4>(r, r, n);
+}
+
+template <>
+__device__ __forceinline__ void montmul<5>(uint32_t (&r)[5], const uint32_t (&a)[5],
+                                           const uint32_t (&b)[5], const uint32_t (&n)[5],
+                                           uint32_t ninv) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0;
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        const uint32_t ai = a[i];
+        asm(
+            "mad.lo.cc.u32 %0, %7, %8, %0;\n\t"
+            "madc.lo.cc.u32 %1, %7, %9, %1;\n\t"
+            "madc.lo.cc.u32 %2, %7, %10, %2;\n\t"
+            "madc.lo.cc.u32 %3, %7, %11, %3;\n\t"
+            "madc.lo.cc.u32 %4, %7, %12, %4;\n\t"
+            "addc.cc.u32 %5, %5, 0;\n\t"
+            "addc.u32 %6, %6, 0;\n\t"
+            "mad.hi.cc.u32 %1, %7, %8, %1;\n\t"
+            "madc.hi.cc.u32 %2, %7, %9, %2;\n\t"
+            "madc.hi.cc.u32 %3, %7, %10, %3;\n\t"
+            "madc.hi.cc.u32 %4, %7, %11, %4;\n\t"
+            "madc.hi.cc.u32 %5, %7, %12, %5;\n\t"
+            "addc.u32 %6, %6, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6)
+            : "r"(ai), "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]));
+        const uint32_t m = t0 * ninv;
+        asm(
+            "mad.lo.cc.u32 %0, %7, %8, %0;\n\t"
+            "madc.lo.cc.u32 %1, %7, %9, %1;\n\t"
+            "madc.lo.cc.u32 %2, %7, %10, %2;\n\t"
+            "madc.lo.cc.u32 %3, %7, %11, %3;\n\t"
+            "madc.lo.cc.u32 %4, %7, %12, %4;\n\t"
+            "addc.cc.u32 %5, %5, 0;\n\t"
+            "addc.u32 %6, %6, 0;\n\t"
+            "mad.hi.cc.u32 %1, %7, %8, %1;\n\t"
+            "madc.hi.cc.u32 %2, %7, %9, %2;\n\t"
+            "madc.hi.cc.u32 %3, %7, %10, %3;\n\t"
+            "madc.hi.cc.u32 %4, %7, %11, %4;\n\t"
+            "madc.hi.cc.u32 %5, %7, %12, %5;\n\t"
+            "addc.u32 %6, %6, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6)
+            : "r"(m), "r"(n[0]), "r"(n[1]), "r"(n[2]), "r"(n[3]), "r"(n[4]));
+        t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = t5; t5 = t6; t6 = 0;
+    }
+    r[0] = t0; r[1] = t1; r[2] = t2; r[3] = t3; r[4] = t4;
+    if (t5 || ge<5>(r, n)) sub_n<5>(r, r, n);
+}
+
+template <>
+__device__ __forceinline__ void montmul<6>(uint32_t (&r)[6], const uint32_t (&a)[6],
+                                           const uint32_t (&b)[6], const uint32_t (&n)[6],
+                                           uint32_t ninv) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        const uint32_t ai = a[i];
+        asm(
+            "mad.lo.cc.u32 %0, %8, %9, %0;\n\t"
+            "madc.lo.cc.u32 %1, %8, %10, %1;\n\t"
+            "madc.lo.cc.u32 %2, %8, %11, %2;\n\t"
+            "madc.lo.cc.u32 %3, %8, %12, %3;\n\t"
+            "madc.lo.cc.u32 %4, %8, %13, %4;\n\t"
+            "madc.lo.cc.u32 %5, %8, %14, %5;\n\t"
+            "addc.cc.u32 %6, %6, 0;\n\t"
+            "addc.u32 %7, %7, 0;\n\t"
+            "mad.hi.cc.u32 %1, %8, %9, %1;\n\t"
+            "madc.hi.cc.u32 %2, %8, %10, %2;\n\t"
+            "madc.hi.cc.u32 %3, %8, %11, %3;\n\t"
+            "madc.hi.cc.u32 %4, %8, %12, %4;\n\t"
+            "madc.hi.cc.u32 %5, %8, %13, %5;\n\t"
+            "madc.hi.cc.u32 %6, %8, %14, %6;\n\t"
+            "addc.u32 %7, %7, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7)
+            : "r"(ai), "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]));
+        const uint32_t m = t0 * ninv;
+        asm(
+            "mad.lo.cc.u32 %0, %8, %9, %0;\n\t"
+            "madc.lo.cc.u32 %1, %8, %10, %1;\n\t"
+            "madc.lo.cc.u32 %2, %8, %11, %2;\n\t"
+            "madc.lo.cc.u32 %3, %8, %12, %3;\n\t"
+            "madc.lo.cc.u32 %4, %8, %13, %4;\n\t"
+            "madc.lo.cc.u32 %5, %8, %14, %5;\n\t"
+            "addc.cc.u32 %6, %6, 0;\n\t"
+            "addc.u32 %7, %7, 0;\n\t"
+            "mad.hi.cc.u32 %1, %8, %9, %1;\n\t"
+            "madc.hi.cc.u32 %2, %8, %10, %2;\n\t"
+            "madc.hi.cc.u32 %3, %8, %11, %3;\n\t"
+            "madc.hi.cc.u32 %4, %8, %12, %4;\n\t"
+            "madc.hi.cc.u32 %5, %8, %13, %5;\n\t"
+            "madc.hi.cc.u32 %6, %8, %14, %6;\n\t"
+            "addc.u32 %7, %7, 0;\n\t"
+            : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7)
+            : "r"(m), "r"(n[0]), "r"(n[1]), "r"(n[2]), "r"(n[3]), "r"(n[4]), "r"(n[5]));
+        t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = t5; t5 = t6; t6 = t7; t7 = 0;
+    }
+    r[0] = t0; r[1] = t1; r[2] = t2; r[3] = t3; r[4] = t4; r[5] = t5;
+    if (t6 || ge<6>(r, n)) sub_n<6>(r, r, n);
+}
+
 
 template <int NL>
 __device__ __forceinline__ void mont_setup(Mont<NL>& M, const Big& nb, int nbits) {
@@ -1044,7 +1267,7 @@ walk_scatter_kernel(WalkArgs a) {
     }
 }
 
-template <int NL>
+template <int NL, uint32_t PRED>
 __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& pc, int stage) {
     const uint32_t off = a.st->off_region[NL];
     const uint32_t n = stage == 0 ? a.st->n_region[NL] : a.st->n_lucas[NL];
@@ -1065,24 +1288,23 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
             Mont<NL> M;
             mont_setup<NL>(M, b, nbits);
             M.count = 0;
-            const uint32_t pred = (a.screen && it.len >= 1) ? a.link_pred : a.pred;
             if (stage == 0) {
                 // the first test for every member; the rest only for its
                 // probable primes, in a second launch of uniform warps
-                if (pred == kPredBPSW || pred == kPredMR235) {
+                if (PRED == kPredBPSW || PRED == kPredMR235) {
                     to_lucas = strong_prp<NL>(M, b, 2);
-                } else if (pred == kPredFermat2) {
+                } else if (PRED == kPredFermat2) {
                     prime = fermat2<NL>(M, b);
                 } else if (pc.n_wit <= 1) {
                     prime = pc.n_wit == 0 || strong_prp<NL>(M, b, pc.wit[0]);
                 } else {
                     to_lucas = strong_prp<NL>(M, b, pc.wit[0]);
                 }
-            } else if (pred == kPredBPSW) {
+            } else if (PRED == kPredBPSW) {
                 prime = strong_lucas<NL>(M, b);
-            } else if (pred == kPredMR235) {
+            } else if (PRED == kPredMR235) {
                 prime = strong_prp<NL>(M, b, 3) && strong_prp<NL>(M, b, 5);
-            } else {
+            } else if (PRED == kPredMR) {
                 prime = true;
                 for (uint32_t k = 1; k < pc.n_wit && prime; k++) prime = strong_prp<NL>(M, b, pc.wit[k]);
             }
@@ -1100,16 +1322,18 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
 }
 
 // blockIdx.y selects the limb count (2 + y); stage 0 = base-2 strong test
-// (first witness), stage 1 = strong Lucas test (the other witnesses)
+// (first witness), stage 1 = strong Lucas test (the other witnesses).  One
+// kernel per test (PRED), so a launch carries only the code of its own test.
+template <uint32_t PRED>
 __global__ void __launch_bounds__(128, 4)
 walk_test_kernel(WalkArgs a, int stage) {
     const ProveConst& pc = c_prove[a.profile];
     switch (blockIdx.y + 2) {
-        case 2: walk_test_region<2>(a, pc, stage); break;
-        case 3: walk_test_region<3>(a, pc, stage); break;
-        case 4: walk_test_region<4>(a, pc, stage); break;
-        case 5: walk_test_region<5>(a, pc, stage); break;
-        default: walk_test_region<6>(a, pc, stage); break;
+        case 2: walk_test_region<2, PRED>(a, pc, stage); break;
+        case 3: walk_test_region<3, PRED>(a, pc, stage); break;
+        case 4: walk_test_region<4, PRED>(a, pc, stage); break;
+        case 5: walk_test_region<5, PRED>(a, pc, stage); break;
+        default: walk_test_region<6, PRED>(a, pc, stage); break;
     }
 }
 
@@ -1120,14 +1344,22 @@ cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n
     return cudaGetLastError();
 }
 
-cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, cudaStream_t st) {
+cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage, uint32_t round_pred,
+                              cudaStream_t st) {
     const uint32_t blocks = std::min<uint32_t>((n_act + 255) / 256, 148 * 8);
     walk_screen_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(a);
     walk_regions_kernel<<<1, 32, 0, st>>>(a.st);
     walk_scatter_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(a);
     const uint32_t tb = std::min<uint32_t>((n_act + 127) / 128, 148 * 16);
-    walk_test_kernel<<<dim3(tb ? tb : 1, kMaxLimbs - 1), 128, 0, st>>>(a, 0);
-    if (two_stage) walk_test_kernel<<<dim3(tb ? tb : 1, kMaxLimbs - 1), 128, 0, st>>>(a, 1);
+    const dim3 grid(tb ? tb : 1, kMaxLimbs - 1);
+    for (int stage = 0; stage < (two_stage ? 2 : 1); stage++) {
+        switch (round_pred) {
+            case kPredBPSW: walk_test_kernel<kPredBPSW><<<grid, 128, 0, st>>>(a, stage); break;
+            case kPredMR235: walk_test_kernel<kPredMR235><<<grid, 128, 0, st>>>(a, stage); break;
+            case kPredFermat2: walk_test_kernel<kPredFermat2><<<grid, 128, 0, st>>>(a, stage); break;
+            default: walk_test_kernel<kPredMR><<<grid, 128, 0, st>>>(a, stage); break;
+        }
+    }
     return cudaGetLastError();
 }
 

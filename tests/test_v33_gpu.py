@@ -56,10 +56,11 @@ def test_v33_prove_equals_reference(ccs, golden):
 
 
 def test_v33_batched_equals_reference(ccs, golden):
-    runs = [r for r in golden("v33_native.json")["runs"] if r["target"] == 8]
-    eng = engine(ccs, runs[0])
-    b = ccs.Batch([eng], len(runs), surv_cap=1 << 18, chain_cap=1 << 16)
-    res, surv, chains = b.run([(int(r["tile_start"]), r["n_tiles"], 0, r["bits"]) for r in runs])
+    """Every run as one range of one batched launch (one profile per run)."""
+    runs = golden("v33_native.json")["runs"]
+    engs = [engine(ccs, r) for r in runs]
+    b = ccs.Batch(engs, len(runs), surv_cap=1 << 18, chain_cap=1 << 16)
+    res, surv, chains = b.run([(int(r["tile_start"]), r["n_tiles"], i, r["bits"]) for i, r in enumerate(runs)])
     b.close()
     rid = surv["_pad"].astype(np.int64)
     crid = rid[chains["survivor"].astype(np.int64)]
@@ -71,7 +72,8 @@ def test_v33_batched_equals_reference(ccs, golden):
             root = sum(int(r[4 + w]) << (32 * w) for w in range(6))
             got[(int(r[0]), int(r[1]), int(r[2]))] = (int(r[3]), root, bool(r[10] & 1))
         assert got == want and res[i]["n_primes"] == want_primes
-    eng.close()
+    for e in engs:
+        e.close()
 
 
 def test_v33_walk_equals_reference(ccs, golden):
