@@ -123,13 +123,15 @@ struct WalkItem {
     uint32_t idx;            // position in the caller's batch
     uint32_t len;            // primes found so far
 };
+constexpr int kWalkBits = 32 * kMaxLimbs + 1;   // bit lengths 0..192
 struct WalkState {
     uint32_t n_act;                      // items tested this round
     uint32_t n_next;                     // items for the next round
     uint32_t n_region[kMaxLimbs + 1];    // items per Montgomery limb count
     uint32_t off_region[kMaxLimbs + 1];
-    uint32_t fill[kMaxLimbs + 1];
     uint32_t n_lucas[kMaxLimbs + 1];     // base-2 probable primes per limb count
+    uint32_t n_bits[kWalkBits];          // items needing a test, per bit length
+    uint32_t fill_bits[kWalkBits];       // next slot of each bit length in the sorted list
 };
 // Primality tests a walk round can apply (CCS_PRIME_MR / CCS_PRIME_BPSW,
 // plus the two native tests of the reference CPU engine v33)

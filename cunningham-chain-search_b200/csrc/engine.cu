@@ -846,7 +846,7 @@ static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint
         const bool second = rp == kPredBPSW || rp == kPredMR235 ||
                             (rp == kPredMR && E->hp.witnesses.size() > 1);
         CU(launch_walk_round(a, n_act, second, rp, st));
-        E->launches += second ? 5 : 4;
+        E->launches += 3 + (second ? 10 : 5);
         CU(cudaMemcpyAsync(hs, &E->w_state.p->n_next, 4, cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         n_act = hs->n_act;

@@ -1234,21 +1234,37 @@ walk_screen_kernel(WalkArgs a) {
             if (v == 0) a.lengths[it.idx] = it.len;
         }
         walk_advance(it, nbits, live && v == 1, a, pc.kind);
-#pragma unroll
-        for (int nl = 2; nl <= kMaxLimbs; nl++) {
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, live && v == nl);
-            if (m && (threadIdx.x & 31) == (uint32_t)(__ffs(m) - 1)) atomicAdd(&a.st->n_region[nl], __popc(m));
+        // count the members that need a test per bit length (one atomic per
+        // distinct length in the warp)
+        const bool need = live && v >= 2;
+        const uint32_t nm = __ballot_sync(0xFFFFFFFFu, need);
+        if (need) {
+            const uint32_t grp = __match_any_sync(nm, (uint32_t)nbits);
+            if ((threadIdx.x & 31) == (uint32_t)(__ffs(grp) - 1)) atomicAdd(&a.st->n_bits[nbits], __popc(grp));
         }
     }
 }
 
+// limb count of the Montgomery arithmetic for a member of nbits bits (the
+// trial stage's code)
+__host__ __device__ constexpr int limbs_of_bits(int nbits) {
+    return nbits <= 64 ? 2 : (nbits + 31) >> 5;
+}
+
+// members sorted by bit length: ascending lengths, so the regions of one
+// limb count are contiguous, and the warps of a test run members of one
+// length (the same exponent loop lengths)
 __global__ void walk_regions_kernel(WalkState* st) {
     if (threadIdx.x == 0) {
+        for (int nl = 0; nl <= kMaxLimbs; nl++) { st->n_region[nl] = 0; st->off_region[nl] = 0; }
         uint32_t o = 0;
-        for (int nl = 0; nl <= kMaxLimbs; nl++) {
-            st->off_region[nl] = o;
-            st->fill[nl] = o;
-            o += st->n_region[nl];
+        int cur = -1;
+        for (int b = 0; b < kWalkBits; b++) {
+            const int nl = limbs_of_bits(b);
+            if (nl != cur) { st->off_region[nl] = o; cur = nl; }
+            st->fill_bits[b] = o;
+            st->n_region[nl] += st->n_bits[b];
+            o += st->n_bits[b];
         }
     }
 }
@@ -1256,13 +1272,24 @@ __global__ void walk_regions_kernel(WalkState* st) {
 __global__ void __launch_bounds__(256)
 walk_scatter_kernel(WalkArgs a) {
     const uint32_t n = a.st->n_act;
+    const uint32_t lane = threadIdx.x & 31;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
         const uint32_t i = i0 + threadIdx.x;
         const int v = i < n ? a.code[i] : 0;
+        const bool need = v >= 2;
+        const uint32_t nm = __ballot_sync(0xFFFFFFFFu, need);
+        if (need) {
+            const WalkItem it = a.act[i];
+            Big b;
 #pragma unroll
-        for (int nl = 2; nl <= kMaxLimbs; nl++) {
-            const uint32_t pos = warp_append(&a.st->fill[nl], v == nl);
-            if (v == nl) a.sorted[pos] = a.act[i];
+            for (int w = 0; w < kMaxLimbs; w++) b.w[w] = it.x[w];
+            const uint32_t nbits = (uint32_t)big_bits(b);
+            const uint32_t grp = __match_any_sync(nm, nbits);
+            const uint32_t leader = __ffs(grp) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&a.st->fill_bits[nbits], __popc(grp));
+            base = __shfl_sync(grp, base, leader);
+            a.sorted[base + __popc(grp & ((1u << lane) - 1u))] = it;
         }
     }
 }
@@ -1321,20 +1348,29 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
     }
 }
 
-// blockIdx.y selects the limb count (2 + y); stage 0 = base-2 strong test
-// (first witness), stage 1 = strong Lucas test (the other witnesses).  One
-// kernel per test (PRED), so a launch carries only the code of its own test.
-template <uint32_t PRED>
+// One kernel per test (PRED), stage (0 = base-2 strong test or the first
+// witness, 1 = strong Lucas test or the other witnesses) and limb count, one
+// launch per limb count: an SM runs the code of one of them at a time.
+template <uint32_t PRED, int STAGE, int NL>
 __global__ void __launch_bounds__(128, 4)
-walk_test_kernel(WalkArgs a, int stage) {
+walk_test_kernel(WalkArgs a) {
     const ProveConst& pc = c_prove[a.profile];
-    switch (blockIdx.y + 2) {
-        case 2: walk_test_region<2, PRED>(a, pc, stage); break;
-        case 3: walk_test_region<3, PRED>(a, pc, stage); break;
-        case 4: walk_test_region<4, PRED>(a, pc, stage); break;
-        case 5: walk_test_region<5, PRED>(a, pc, stage); break;
-        default: walk_test_region<6, PRED>(a, pc, stage); break;
-    }
+    walk_test_region<NL, PRED>(a, pc, STAGE);
+}
+
+template <uint32_t PRED, int STAGE>
+static void launch_walk_tests(const WalkArgs& a, uint32_t grid, cudaStream_t st) {
+    walk_test_kernel<PRED, STAGE, 2><<<grid, 128, 0, st>>>(a);
+    walk_test_kernel<PRED, STAGE, 3><<<grid, 128, 0, st>>>(a);
+    walk_test_kernel<PRED, STAGE, 4><<<grid, 128, 0, st>>>(a);
+    walk_test_kernel<PRED, STAGE, 5><<<grid, 128, 0, st>>>(a);
+    walk_test_kernel<PRED, STAGE, 6><<<grid, 128, 0, st>>>(a);
+}
+
+template <uint32_t PRED>
+static void launch_walk_stage(const WalkArgs& a, int stage, uint32_t grid, cudaStream_t st) {
+    if (stage == 0) launch_walk_tests<PRED, 0>(a, grid, st);
+    else launch_walk_tests<PRED, 1>(a, grid, st);
 }
 
 cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
@@ -1351,13 +1387,13 @@ cudaError_t launch_walk_round(const WalkArgs& a, uint32_t n_act, bool two_stage,
     walk_regions_kernel<<<1, 32, 0, st>>>(a.st);
     walk_scatter_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(a);
     const uint32_t tb = std::min<uint32_t>((n_act + 127) / 128, 148 * 16);
-    const dim3 grid(tb ? tb : 1, kMaxLimbs - 1);
+    const uint32_t grid = tb ? tb : 1;
     for (int stage = 0; stage < (two_stage ? 2 : 1); stage++) {
         switch (round_pred) {
-            case kPredBPSW: walk_test_kernel<kPredBPSW><<<grid, 128, 0, st>>>(a, stage); break;
-            case kPredMR235: walk_test_kernel<kPredMR235><<<grid, 128, 0, st>>>(a, stage); break;
-            case kPredFermat2: walk_test_kernel<kPredFermat2><<<grid, 128, 0, st>>>(a, stage); break;
-            default: walk_test_kernel<kPredMR><<<grid, 128, 0, st>>>(a, stage); break;
+            case kPredBPSW: launch_walk_stage<kPredBPSW>(a, stage, grid, st); break;
+            case kPredMR235: launch_walk_stage<kPredMR235>(a, stage, grid, st); break;
+            case kPredFermat2: launch_walk_stage<kPredFermat2>(a, stage, grid, st); break;
+            default: launch_walk_stage<kPredMR>(a, stage, grid, st); break;
         }
     }
     return cudaGetLastError();
