@@ -192,7 +192,7 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "config": {"workload": WORKLOAD, "bits": BITS, "target": 16},
             "cpu_baseline": {"value": v, "unit": "candidates/s", "cores": s["cores"],
-                             "kind": "reference", "sample": sample},
+                             "cpu_model": cpu_model(), "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": "candidates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     if not args.headline_only:
@@ -557,8 +557,9 @@ def section_cpu_method(ccs, torch, dev, local, seconds_goal=8.0):
     rinfo = e_ref.info
     bases = e_ref.bases()
     M, WP = rinfo["lattice_m"], rinfo["wheel_period"]
-    # about 2.5e8 candidates per second on 16 cores at target 8: size the range
-    want = 2.5e8 / 16 * cores * seconds_goal
+    # about 1.5e6 candidates per second per core at target 8 with its prove
+    # (2.37e7 measured on 16 cores): size the range
+    want = 1.5e6 * cores * seconds_goal
     pbits = 2
     while pbits < ref_bits - 1:
         t0_, t1_ = v33_prefix_range(ref_bits, 1 << (pbits - 1), pbits, bases, M, WP)[:2]
@@ -1006,6 +1007,7 @@ def run_ours(args):
         s = v33_sample(BITS, 16)
         if s:
             cpu = {"value": s["rate"], "unit": "candidates/s", "cores": s["cores"], "kind": "reference",
+                   "cpu_model": cpu_model(),
                    "sample": (f"cc_gmp_v33 --sieve-only --sequential --prefix {s['prefix']} --bits {BITS} "
                               f"--target 16 --threads {s['cores']}: {s['candidates']} candidates in "
                               f"{s['seconds']:.1f} s (reference stage primes 37..863 on the same "
