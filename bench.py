@@ -936,6 +936,7 @@ def run_ours(args):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     launches0 = eng.launches()
+    eng.prove_stats(reset=True)
     n_surv = n_chain = n_prime = 0
     torch.cuda.synchronize()
     t_wall = time.time()
@@ -957,6 +958,7 @@ def run_ours(args):
     t_wall = time.time() - t_wall
     step_ms = [a.elapsed_time(b) for a, b in ev]
     launches = eng.launches() - launches0
+    pstats = eng.prove_stats(reset=True)
     clk = clocks.stop()
     ms_total = sum(step_ms)
     if pg:
@@ -1065,6 +1067,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "candidates/s", "h2d_bytes_per_step": h2d // e2e_steps,
                     "d2h_bytes_per_step": d2h // e2e_steps},
             "gpu_launches": launches,
+            "prove_stats": pstats,
             "wall_s_timed": t_wall,
         }
         line.update(extra)

@@ -863,9 +863,11 @@ ccs_status ccs_walk_numbers(ccs_engine* E, const uint32_t* numbers_dev, uint64_t
     CU(cudaSetDevice(E->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : E->own_stream;
     if (!n) return CCS_OK;
-    // numbers are walked in chunks of up to 2^22, each in rounds until every
-    // walk has ended (at most MAX_CHAIN rounds)
-    const uint64_t chunk = std::min<uint64_t>(n, 1ull << 22);
+    // numbers are walked in chunks of up to 2^24 (32 bytes per item in each
+    // of four lists), each in rounds until every walk has ended (at most
+    // MAX_CHAIN rounds); the late rounds of a chunk hold few walks and cost
+    // about their launches, so fewer, larger chunks pay
+    const uint64_t chunk = std::min<uint64_t>(n, 1ull << 24);
     {
         ccs_status s = walk_reserve(E, chunk);
         if (s != CCS_OK) return s;

@@ -543,8 +543,11 @@ __device__ __forceinline__ void to_mont_small(uint32_t (&r)[NL], uint32_t a, con
     for (int i = 0; i < NL; i++) r[i] = acc[i];
 }
 
-// strong probable-prime test to base a (n odd, n > a)
-template <int NL>
+// strong probable-prime test to base a (n odd, n > a).  SYNC: every lane of
+// the warp runs the test (the walk kernels give idle lanes a copy of a live
+// lane's number) and the lanes are reconverged after the set-up loops, so the
+// exponent loop runs once for the whole warp.
+template <int NL, bool SYNC = false>
 __device__ bool strong_prp(Mont<NL>& M, const Big& nb, uint32_t a) {
     // n - 1 = d 2^s
     Big d = nb;
@@ -572,8 +575,10 @@ __device__ bool strong_prp(Mont<NL>& M, const Big& nb, uint32_t a) {
             }
         }
     }
+    if (SYNC) __syncwarp();
     uint32_t am[NL], x[NL];
     to_mont_small<NL>(am, a, M);
+    if (SYNC) __syncwarp();
 #pragma unroll
     for (int i = 0; i < NL; i++) x[i] = am[i];
     // left-to-right over the bits of d below its top bit; the limb loop is
@@ -593,6 +598,7 @@ __device__ bool strong_prp(Mont<NL>& M, const Big& nb, uint32_t a) {
             }
         }
     }
+    if (SYNC) __syncwarp();
     if (eq<NL>(x, M.one) || eq<NL>(x, M.mone)) return true;
     for (int r = 1; r < s; r++) {
         montmul<NL>(x, x, x, M.n, M.ninv);
@@ -634,23 +640,30 @@ __device__ int jacobi_small(int D, const Big& nb) {
     return y == 1 ? sign : 0;
 }
 
-// strong Lucas probable-prime test, Selfridge method A (P = 1, Q = (1 - D)/4)
-template <int NL>
+// strong Lucas probable-prime test, Selfridge method A (P = 1, Q = (1 - D)/4).
+// SYNC as in strong_prp: a lane whose D search decides the verdict still runs
+// the ladder (on its last D) with the warp and returns its decided verdict.
+template <int NL, bool SYNC = false>
 __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
     int D = 5;
     int tries = 0;
+    bool decided = false, dres = false;
     for (;;) {
         int j = jacobi_small(D, nb);
         if (j == -1) break;
         if (j == 0) {
             uint32_t ad = (uint32_t)(D < 0 ? -D : D);
-            return big_lt_u32(nb, ad + 1) && nb.w[0] == ad;   // n == |D|
+            dres = big_lt_u32(nb, ad + 1) && nb.w[0] == ad;   // n == |D|
+            decided = true;
+            break;
         }
         D = D > 0 ? -(D + 2) : -(D - 2);
         // no D with (D/n) = -1 among the first 64 candidates: n is (almost
         // surely) a perfect square; squares are composite
-        if (++tries > 64) return false;
+        if (++tries > 64) { decided = true; dres = false; break; }
     }
+    if (!SYNC && decided) return dres;
+    if (SYNC) __syncwarp();
     const int Qs = (1 - D) / 4;
     uint32_t Qm[NL];
     if (Qs >= 0) to_mont_small<NL>(Qm, (uint32_t)Qs, M);
@@ -658,6 +671,7 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
 #pragma unroll
         for (int i = 0; i < NL; i++) z[i] = 0;
         submod<NL>(Qm, z, t, M.n); }
+    if (SYNC) __syncwarp();
     // n + 1 = d 2^s
     Big d = nb;
     {
@@ -713,25 +727,31 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
       }
     }
     // V0 = V_d, V1 = V_(d+1), Qk = Q^d
+    if (SYNC) __syncwarp();
+    bool res = false;
     dblmod<NL>(t1, V1, M.n);
-    if (eq<NL>(t1, V0) || is_zero<NL>(V0)) return true;
-    for (int r = 1; r < s; r++) {
-        montmul<NL>(t1, V0, V0, M.n, M.ninv);
-        dblmod<NL>(t2, Qk, M.n);
-        submod<NL>(V0, t1, t2, M.n);
-        if (is_zero<NL>(V0)) return true;
-        montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
-        M.count += 2;
+    if (eq<NL>(t1, V0) || is_zero<NL>(V0)) {
+        res = true;
+    } else {
+        for (int r = 1; r < s; r++) {
+            montmul<NL>(t1, V0, V0, M.n, M.ninv);
+            dblmod<NL>(t2, Qk, M.n);
+            submod<NL>(V0, t1, t2, M.n);
+            if (is_zero<NL>(V0)) { res = true; break; }
+            montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
+            M.count += 2;
+        }
     }
-    return false;
+    return decided ? dres : res;
 }
 
 // Fermat test to base 2: 2^(n-1) == 1 (mod n), n odd > 2 (the link test of
 // the reference CPU engine, is_prime_pocklington_native, v33:1290-1302)
-template <int NL>
+template <int NL, bool SYNC = false>
 __device__ bool fermat2(Mont<NL>& M, const Big& nb) {
     Big e = nb;
     e.w[0] -= 1;                              // n odd: no borrow
+    if (SYNC) __syncwarp();
     uint32_t x[NL];
 #pragma unroll
     for (int i = 0; i < NL; i++) x[i] = M.one[i];
@@ -1300,45 +1320,54 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
     const uint32_t n = stage == 0 ? a.st->n_region[NL] : a.st->n_lucas[NL];
     const WalkItem* src = stage == 0 ? a.sorted : a.lucas;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        // whole warps: lanes past the end test a copy of the warp's first
+        // member (and record nothing), so the tests reconverge the warp
+        const uint32_t wbase = i0 + (threadIdx.x & ~31u);
+        if (wbase >= n) continue;
         const uint32_t i = i0 + threadIdx.x;
         const bool live = i < n;
-        WalkItem it;
+        const WalkItem it = src[off + (live ? i : wbase)];
         Big b;
-        int nbits = 0;
-        bool prime = false, to_lucas = false;
-        uint32_t mm = 0, words = 0;
-        if (live) {
-            it = src[off + i];
 #pragma unroll
-            for (int w = 0; w < kMaxLimbs; w++) b.w[w] = it.x[w];
-            nbits = big_bits(b);
-            Mont<NL> M;
-            mont_setup<NL>(M, b, nbits);
-            M.count = 0;
-            if (stage == 0) {
-                // the first test for every member; the rest only for its
-                // probable primes, in a second launch of uniform warps
-                if (PRED == kPredBPSW || PRED == kPredMR235) {
-                    to_lucas = strong_prp<NL>(M, b, 2);
-                } else if (PRED == kPredFermat2) {
-                    prime = fermat2<NL>(M, b);
-                } else if (pc.n_wit <= 1) {
-                    prime = pc.n_wit == 0 || strong_prp<NL>(M, b, pc.wit[0]);
-                } else {
-                    to_lucas = strong_prp<NL>(M, b, pc.wit[0]);
-                }
-            } else if (PRED == kPredBPSW) {
-                prime = strong_lucas<NL>(M, b);
-            } else if (PRED == kPredMR235) {
-                prime = strong_prp<NL>(M, b, 3) && strong_prp<NL>(M, b, 5);
-            } else if (PRED == kPredMR) {
-                prime = true;
-                for (uint32_t k = 1; k < pc.n_wit && prime; k++) prime = strong_prp<NL>(M, b, pc.wit[k]);
+        for (int w = 0; w < kMaxLimbs; w++) b.w[w] = it.x[w];
+        const int nbits = big_bits(b);
+        bool prime = false, to_lucas = false;
+        Mont<NL> M;
+        mont_setup<NL>(M, b, nbits);
+        M.count = 0;
+        __syncwarp();
+        if (stage == 0) {
+            // the first test for every member; the rest only for its
+            // probable primes, in a second launch of uniform warps
+            if (PRED == kPredBPSW || PRED == kPredMR235) {
+                to_lucas = strong_prp<NL, true>(M, b, 2);
+            } else if (PRED == kPredFermat2) {
+                prime = fermat2<NL, true>(M, b);
+            } else if (pc.n_wit <= 1) {
+                prime = pc.n_wit == 0 || strong_prp<NL, true>(M, b, pc.wit[0]);
+            } else {
+                to_lucas = strong_prp<NL, true>(M, b, pc.wit[0]);
             }
-            mm = M.count;
-            words = M.count * (2 * NL * NL + NL);
-            if (!prime && !to_lucas) a.lengths[it.idx] = it.len;
+        } else if (PRED == kPredBPSW) {
+            prime = strong_lucas<NL, true>(M, b);
+        } else if (PRED == kPredMR235) {
+            // both tests on every lane: a test reconverges the warp inside
+            const bool r3 = strong_prp<NL, true>(M, b, 3);
+            const bool r5 = strong_prp<NL, true>(M, b, 5);
+            prime = r3 && r5;
+        } else if (PRED == kPredMR) {
+            prime = true;
+            for (uint32_t k = 1; k < pc.n_wit; k++) {
+                const bool r = strong_prp<NL, true>(M, b, pc.wit[k]);
+                prime = prime && r;
+                if (!__any_sync(0xFFFFFFFFu, live && prime)) break;
+            }
         }
+        prime = prime && live;
+        to_lucas = to_lucas && live;
+        const uint32_t mm = live ? M.count : 0u;
+        const uint32_t words = mm * (2 * NL * NL + NL);
+        if (live && !prime && !to_lucas) a.lengths[it.idx] = it.len;
         walk_count_mm(mm, words);
         if (stage == 0) {
             const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas);
