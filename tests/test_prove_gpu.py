@@ -154,9 +154,9 @@ def test_roots_mode_matches_reference_k2(ccs, ob):
 
 
 def test_walk_rounds_across_chunks(ccs, ob, eng_bpsw):
-    """5e6 numbers (two walk chunks of 2^22): 40,000 distinct 80..110-bit odd
-    numbers repeated 125 times give 125 identical length vectors, equal to
-    the oracle's on a seeded sample."""
+    """1.7e7 numbers (two walk chunks of 2^24): 40,000 distinct 80..110-bit
+    odd numbers repeated 425 times give 425 identical length vectors, equal
+    to the oracle's on a seeded sample."""
     import torch
     r = random.Random(2024)
     distinct = []
@@ -168,10 +168,10 @@ def test_walk_rounds_across_chunks(ccs, ob, eng_bpsw):
         for w in range(4):
             arr[i, w] = (v >> (32 * w)) & 0xFFFFFFFF
     base = torch.from_numpy(arr.view(np.int32)).cuda()
-    nums = base.repeat(125, 1).contiguous()
+    nums = base.repeat(425, 1).contiguous()
     lengths = torch.full((nums.shape[0],), -1, dtype=torch.int32, device="cuda")
     eng_bpsw.walk_numbers_dev(nums, 4, lengths)
-    L = lengths.cpu().numpy().reshape(125, -1)
+    L = lengths.cpu().numpy().reshape(425, -1)
     assert (L == L[0]).all()
     for i in r.sample(range(len(distinct)), 300):
         assert L[0, i] == ob.chain_from(distinct[i], ob.PRIME_BPSW), distinct[i]
