@@ -36,7 +36,7 @@ constexpr double kTAdmit = 0.18;       // table-window admission (level-A surviv
 constexpr uint32_t t_words(uint32_t q) { return (q - 1) / 32 + 5; }
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
-constexpr int kLevelBRound = 4;        // level-B primes tested per lane per round
+constexpr int kLevelBRound = 8;        // level-B primes tested per lane per round
 
 // One bit-sliced ("level A") prime.  Register-window primes (A1, A2) keep
 // their 64/96-bit kill window in registers and advance it by shifts per 64

@@ -140,7 +140,7 @@ __device__ constexpr uint32_t std_toff(int i) {
     return o;
 }
 
-constexpr int kQCap = 512;               // per-warp level-B queue (entries, power of two)
+constexpr int kQCap = 256;               // per-warp level-B queue (entries, power of two)
 constexpr uint32_t kQLow = 96;           // level-B rounds run until at most this many are queued
 constexpr int kCCap = 64;                // per-warp level-C list (entries)
 constexpr int kBK = kLevelBRound;        // level-B primes tested per lane per round
