@@ -141,7 +141,7 @@ __device__ constexpr uint32_t std_toff(int i) {
 }
 
 constexpr int kQCap = 256;               // per-warp level-B queue (entries, power of two)
-constexpr uint32_t kQLow = 96;           // level-B rounds run until at most this many are queued
+constexpr uint32_t kQLow = 64;           // level-B rounds run until at most this many are queued
 constexpr int kCCap = 64;                // per-warp level-C list (entries)
 constexpr int kBK = kLevelBRound;        // level-B primes tested per lane per round
 constexpr int kPAWords = kNumAR * 8 + kPatTMax;   // per-warp copy of the level-A patterns (u32)
