@@ -37,6 +37,8 @@ constexpr uint32_t t_words(uint32_t q) { return (q - 1) / 32 + 5; }
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
 constexpr int kLevelBRound = 8;        // level-B primes tested per lane per round
+constexpr uint32_t kCBitmapMax = 8192; // level-C primes below this test a G_q bitmap with
+                                       // 32-bit phase arithmetic (q^2 < 2^32)
 
 // One bit-sliced ("level A") prime.  Register-window primes (A1, A2) keep
 // their 64/96-bit kill window in registers and advance it by shifts per 64
@@ -104,6 +106,9 @@ struct ProfileConst {
     uint32_t std_a;                  // 1: level-A slots hold the standard set 37..127
     const PrimeC* primesC;           // level C primes (ascending)
     const uint32_t* listC;           // sorted G_q lists of level C primes
+    const uint32_t* bitmapC;         // G_q bitmaps of the first nCb level C primes (q < kCBitmapMax)
+    uint32_t nCb;
+    uint32_t _cpad;
     // line phases r W^-1 mod q, [line][ptab_stride] u16 (null: computed per
     // work unit): level-A slot i at i, level-B prime p at kSlotB + p; and the
     // constants of those ptab_stride slots
@@ -155,6 +160,8 @@ struct HostProfile {
     std::vector<PrimeB> packB;
     uint32_t std_a = 0;
     std::vector<uint32_t> bitmapB, listC;
+    std::vector<uint32_t> bitmapC;   // level C primes below kCBitmapMax (PrimeC.off: first word)
+    uint32_t nCb = 0;
     // index of every level-A/B prime for the per-range J0 mod q table
     std::vector<uint32_t> range_primes;   // A slots (kNumA, dummies as 1) then B then C
 };

@@ -129,7 +129,9 @@ struct WalkState {
     uint32_t n_next;                     // items for the next round
     uint32_t n_region[kMaxLimbs + 1];    // items per Montgomery limb count
     uint32_t off_region[kMaxLimbs + 1];
-    uint32_t n_lucas[kMaxLimbs + 1];     // base-2 probable primes per limb count
+    uint32_t n_lucas[kMaxLimbs + 1];     // base-2 probable primes per limb count (from the
+                                         // bottom of the region)
+    uint32_t n_lucas5[kMaxLimbs + 1];    // of them with (5/n) = -1 (BPSW; from the top)
     uint32_t n_bits[kWalkBits];          // items needing a test, per bit length
     uint32_t fill_bits[kWalkBits];       // next slot of each bit length in the sorted list
 };

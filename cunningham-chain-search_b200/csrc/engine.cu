@@ -71,12 +71,12 @@ struct FilterSet {
     DevBuf<Line> lines;
     DevBuf<PrimeC> primesB, primesC;
     DevBuf<PrimeB> packB;
-    DevBuf<uint32_t> bitmapB, listC, range_primes, patT;
+    DevBuf<uint32_t> bitmapB, listC, bitmapC, range_primes, patT;
     DevBuf<uint16_t> ptab;           // line phase table (may stay empty)
     DevBuf<SlotConst> pq;
     void free_() {
         lines.free_(); primesB.free_(); primesC.free_(); packB.free_();
-        bitmapB.free_(); listC.free_(); range_primes.free_(); patT.free_();
+        bitmapB.free_(); listC.free_(); bitmapC.free_(); range_primes.free_(); patT.free_();
         ptab.free_(); pq.free_();
     }
 };
@@ -204,6 +204,9 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     CU(f.listC.alloc(hp.listC.size()));
     if (!hp.listC.empty())
         CU(cudaMemcpy(f.listC.p, hp.listC.data(), 4 * hp.listC.size(), cudaMemcpyHostToDevice));
+    CU(f.bitmapC.alloc(hp.bitmapC.size()));
+    if (!hp.bitmapC.empty())
+        CU(cudaMemcpy(f.bitmapC.p, hp.bitmapC.data(), 4 * hp.bitmapC.size(), cudaMemcpyHostToDevice));
     CU(f.patT.alloc(hp.patT.size()));
     CU(cudaMemcpy(f.patT.p, hp.patT.data(), 4 * hp.patT.size(), cudaMemcpyHostToDevice));
     CU(f.range_primes.alloc(hp.range_primes.size()));
@@ -227,6 +230,8 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     pc.std_a = hp.std_a;
     pc.primesC = f.primesC.p;
     pc.listC = f.listC.p;
+    pc.bitmapC = f.bitmapC.p;
+    pc.nCb = hp.nCb;
     // line phase table for every level-A slot and level-B prime, when it fits
     {
         const uint32_t nb = hp.primesB.empty() ? 1u : (uint32_t)hp.primesB.size();
@@ -846,7 +851,7 @@ static ccs_status walk_rounds(ccs_engine* E, uint32_t n, uint32_t* lengths, uint
         const bool second = rp == kPredBPSW || rp == kPredMR235 ||
                             (rp == kPredMR && E->hp.witnesses.size() > 1);
         CU(launch_walk_round(a, n_act, second, rp, st));
-        E->launches += 3 + (second ? 10 : 5);
+        E->launches += 3 + (second ? 10 : 5) + (rp == kPredBPSW ? 5 : 0);
         CU(cudaMemcpyAsync(hs, &E->w_state.p->n_next, 4, cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         n_act = hs->n_act;

@@ -193,7 +193,18 @@ __device__ __forceinline__ void c_process(LevelB& B, const SweepArgs& a, const R
         for (uint32_t base = 0; base < P.nC && !killed; base += 32) {
             const uint32_t p = base + lane;
             bool kill = false;
-            if (p < P.nC) {
+            if (p < P.nCb) {
+                // q < 2^13: the phase in 32-bit arithmetic, one bitmap word
+                const PrimeC pc = P.primesC[p];
+                const uint32_t q = pc.q;
+                uint32_t rm = mod_magic(ln.r_hi, q, pc.magic) * pc.c32 + mod_magic(ln.r_lo, q, pc.magic);
+                rm = mod_magic(rm, q, pc.magic);                          // r mod q
+                const uint32_t rw = mod_magic(rm * pc.winv, q, pc.magic);
+                uint32_t uph = rw + jm[p] + mod_magic(j, q, pc.magic);    // < 3q
+                uph = uph >= q ? uph - q : uph;
+                uph = uph >= q ? uph - q : uph;
+                kill = (__ldg(P.bitmapC + pc.off + (uph >> 5)) >> (uph & 31)) & 1u;
+            } else if (p < P.nC) {
                 const PrimeC pc = P.primesC[p];
                 const uint32_t rm = mod_magic64(r, pc.q, pc.magic64);
                 const uint32_t rw = mod_magic64((uint64_t)rm * pc.winv, pc.q, pc.magic64);

@@ -225,6 +225,8 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
     for (int i = 0; i < kNumA; i++) { hp.A[i].q = 1; hp.A[i].magic = 0xFFFFFFFFu; }   // dummy: no kills
     int nA1 = 0, nA2 = 0, nT = 0;
     hp.primesB.clear(); hp.primesC.clear(); hp.bitmapB.clear(); hp.listC.clear(); hp.packB.clear();
+    hp.bitmapC.clear();
+    hp.nCb = 0;
     hp.patT.clear();
     const uint64_t Wm = hp.W;
     // How many table-window primes: one costs about as much per 64-position
@@ -307,6 +309,15 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             pb.magic = pc.magic;
             pb.q_off = q | (pc.off << 16);
             hp.packB.push_back(pb);
+        } else if (q < kCBitmapMax) {
+            // small level-C primes (a prefix of the ascending list): G_q bitmap
+            pc.off = (uint32_t)hp.bitmapC.size();
+            pc.cnt = (uint32_t)g.size();
+            std::vector<uint32_t> bm((q + 31) / 32, 0);
+            for (uint32_t u : g) bm[u >> 5] |= 1u << (u & 31);
+            hp.bitmapC.insert(hp.bitmapC.end(), bm.begin(), bm.end());
+            hp.primesC.push_back(pc);
+            hp.nCb = (uint32_t)hp.primesC.size();
         } else {
             // sorted list padded to a multiple of 4 entries (0xFFFFFFFF never
             // matches a phase), 16-byte aligned for vector loads

@@ -745,6 +745,85 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
     return decided ? dres : res;
 }
 
+// The strong Lucas test above for the members whose Selfridge parameter is
+// the first one tried, D = 5 ((5/n) = -1, i.e. n = 2 or 3 mod 5): P = 1,
+// Q = -1, so Q^k = (-1)^k and the ladder needs no powers of Q -- two products
+// per bit instead of four, with the same verdict:
+//   V_2k+1 = V_k V_k+1 - (-1)^k,   V_2k = V_k^2 - 2 (-1)^k,
+//   V_2k+2 = V_k+1^2 - 2 (-1)^(k+1),
+// and after the ladder (d odd) V_2d = V_d^2 + 2, then V_2m = V_m^2 - 2.
+// The caller has checked n mod 5; every lane of the warp runs the ladder.
+template <int NL>
+__device__ bool strong_lucas_d5(Mont<NL>& M, const Big& nb) {
+    Big d = nb;
+    {
+        uint32_t c = 1;
+#pragma unroll
+        for (int i = 0; i < kMaxLimbs; i++) {
+            uint64_t s2 = (uint64_t)d.w[i] + c;
+            d.w[i] = (uint32_t)s2;
+            c = (uint32_t)(s2 >> 32);
+        }
+    }
+    int s = 0;
+    while ((d.w[0] & 1u) == 0) {
+#pragma unroll
+        for (int i = 0; i < kMaxLimbs; i++) {
+            uint32_t hi = (i + 1 < kMaxLimbs) ? d.w[i + 1] : 0;
+            d.w[i] = (d.w[i] >> 1) | (hi << 31);
+        }
+        s++;
+    }
+    __syncwarp();
+    uint32_t two[NL], mtwo[NL], V0[NL], V1[NL], t1[NL], S[NL], X[NL], C[NL];
+    dblmod<NL>(two, M.one, M.n);
+    sub_n<NL>(mtwo, M.n, two);
+    // from k = 1: V_1 = P = 1, V_2 = P^2 - 2Q = 3, k odd
+#pragma unroll
+    for (int i = 0; i < NL; i++) V0[i] = M.one[i];
+    addmod<NL>(V1, two, M.one, M.n);
+    bool odd = true;
+    const int top = big_bits(d) - 1;
+#pragma unroll
+    for (int wi = kMaxLimbs - 1; wi >= 0; wi--) {
+      if (32 * wi > top - 1) continue;
+      const uint32_t word = d.w[wi];
+      const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
+      for (int b = hb; b >= 0; b--) {
+        const bool bit = (word >> b) & 1u;
+        montmul<NL>(t1, V0, V1, M.n, M.ninv);
+#pragma unroll
+        for (int i = 0; i < NL; i++) C[i] = odd ? M.one[i] : M.mone[i];
+        addmod<NL>(t1, t1, C, M.n);                                // V_2k+1
+#pragma unroll
+        for (int i = 0; i < NL; i++) { X[i] = bit ? V1[i] : V0[i]; C[i] = (odd != bit) ? two[i] : mtwo[i]; }
+        montmul<NL>(S, X, X, M.n, M.ninv);
+        addmod<NL>(S, S, C, M.n);                                  // V_2k or V_2k+2
+#pragma unroll
+        for (int i = 0; i < NL; i++) { V0[i] = bit ? t1[i] : S[i]; V1[i] = bit ? S[i] : t1[i]; }
+        odd = bit;
+        M.count += 2;
+      }
+    }
+    // V0 = V_d, V1 = V_(d+1); U_d = 0 exactly when 2 V_(d+1) = V_d
+    __syncwarp();
+    bool res = false;
+    dblmod<NL>(t1, V1, M.n);
+    if (eq<NL>(t1, V0) || is_zero<NL>(V0)) {
+        res = true;
+    } else {
+        for (int r = 1; r < s; r++) {
+            montmul<NL>(t1, V0, V0, M.n, M.ninv);
+#pragma unroll
+            for (int i = 0; i < NL; i++) C[i] = r == 1 ? two[i] : mtwo[i];
+            addmod<NL>(V0, t1, C, M.n);                            // Q^d = -1, then Q^(2^r d) = 1
+            M.count += 1;
+            if (is_zero<NL>(V0)) { res = true; break; }
+        }
+    }
+    return res;
+}
+
 // Fermat test to base 2: 2^(n-1) == 1 (mod n), n odd > 2 (the link test of
 // the reference CPU engine, is_prime_pocklington_native, v33:1290-1302)
 template <int NL, bool SYNC = false>
@@ -1316,8 +1395,11 @@ walk_scatter_kernel(WalkArgs a) {
 
 template <int NL, uint32_t PRED>
 __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& pc, int stage) {
-    const uint32_t off = a.st->off_region[NL];
-    const uint32_t n = stage == 0 ? a.st->n_region[NL] : a.st->n_lucas[NL];
+    // stage 0: the sorted region; stage 1: the base-2 probable primes at the
+    // bottom of the region; stage 2: those with (5/n) = -1, at its top
+    const uint32_t off0 = a.st->off_region[NL];
+    const uint32_t n = stage == 0 ? a.st->n_region[NL] : stage == 1 ? a.st->n_lucas[NL] : a.st->n_lucas5[NL];
+    const uint32_t off = stage == 2 ? off0 + a.st->n_region[NL] - n : off0;
     const WalkItem* src = stage == 0 ? a.sorted : a.lucas;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
         // whole warps: lanes past the end test a copy of the warp's first
@@ -1348,6 +1430,8 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
             } else {
                 to_lucas = strong_prp<NL, true>(M, b, pc.wit[0]);
             }
+        } else if (PRED == kPredBPSW && stage == 2) {
+            prime = strong_lucas_d5<NL>(M, b);
         } else if (PRED == kPredBPSW) {
             prime = strong_lucas<NL, true>(M, b);
         } else if (PRED == kPredMR235) {
@@ -1370,15 +1454,27 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
         if (live && !prime && !to_lucas) a.lengths[it.idx] = it.len;
         walk_count_mm(mm, words);
         if (stage == 0) {
-            const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas);
-            if (to_lucas) a.lucas[off + pos] = it;
+            // BPSW: members with (5/n) = -1 (n = 2, 3 mod 5) take the D = 5
+            // ladder in a launch of their own
+            bool d5 = false;
+            if (PRED == kPredBPSW) {
+                const uint32_t m5 = big_mod_small(b, 5);
+                d5 = m5 == 2 || m5 == 3;
+            }
+            const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas && !d5);
+            if (PRED == kPredBPSW) {
+                const uint32_t pos5 = warp_append(&a.st->n_lucas5[NL], to_lucas && d5);
+                if (to_lucas && d5) a.lucas[off + a.st->n_region[NL] - 1 - pos5] = it;
+            }
+            if (to_lucas && !d5) a.lucas[off + pos] = it;
         }
         walk_advance(it, nbits, prime, a, pc.kind);
     }
 }
 
 // One kernel per test (PRED), stage (0 = base-2 strong test or the first
-// witness, 1 = strong Lucas test or the other witnesses) and limb count, one
+// witness, 1 = strong Lucas test or the other witnesses, 2 = the D = 5 strong
+// Lucas test) and limb count, one
 // launch per limb count: an SM runs the code of one of them at a time.
 template <uint32_t PRED, int STAGE, int NL>
 __global__ void __launch_bounds__(128, 4)
@@ -1400,6 +1496,7 @@ template <uint32_t PRED>
 static void launch_walk_stage(const WalkArgs& a, int stage, uint32_t grid, cudaStream_t st) {
     if (stage == 0) launch_walk_tests<PRED, 0>(a, grid, st);
     else launch_walk_tests<PRED, 1>(a, grid, st);
+    if (PRED == kPredBPSW && stage == 1) launch_walk_tests<kPredBPSW, 2>(a, grid, st);
 }
 
 cudaError_t launch_walk_load(const uint32_t* numbers, uint64_t first, uint32_t n, uint32_t limbs,
