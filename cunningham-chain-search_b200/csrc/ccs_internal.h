@@ -34,6 +34,37 @@ constexpr double kTAdmit = 0.18;       // table-window admission (level-A surviv
 // Pattern words of a table-window prime: a 128-bit window (two 64-position
 // words, the sweep's step) at any phase < q lies inside them.
 constexpr uint32_t t_words(uint32_t q) { return (q - 1) / 32 + 5; }
+
+// Merged table windows of the standard 22-prime table set (97..199): table
+// slots 2k and 2k + 1 (k < kMgPairs) share one pattern of period q1 q2 (bit t
+// set when t mod q1 or t mod q2 is a kill phase), the last slots keep their
+// own.  One merged window costs the same five shared loads and funnel shifts
+// per 128 positions as a single prime.  The patterns (kPatMWords words) are
+// staged once per block.
+constexpr int kMgPairs = 9;
+constexpr int kMgWin = kNumT - kMgPairs;          // windows of the merged set
+constexpr uint32_t std_t_prime(int i) {           // table slot i of the standard set
+    constexpr uint32_t t[kNumT] = {97, 101, 103, 107, 109, 113, 127, 131, 137, 139, 149,
+                                   151, 157, 163, 167, 173, 179, 181, 191, 193, 197, 199};
+    return t[i];
+}
+constexpr int mg_slot1(int k) { return k < kMgPairs ? 2 * k : kMgPairs + k; }
+constexpr int mg_slot2(int k) { return k < kMgPairs ? 2 * k + 1 : -1; }
+constexpr uint32_t mg_q1(int k) { return std_t_prime(mg_slot1(k)); }
+constexpr uint32_t mg_q2(int k) { return k < kMgPairs ? std_t_prime(mg_slot2(k)) : 1u; }
+constexpr uint32_t mg_period(int k) { return mg_q1(k) * mg_q2(k); }
+constexpr uint32_t mg_off(int k) {                // first word of window k's pattern
+    uint32_t o = 0;
+    for (int i = 0; i < k; i++) o += t_words(mg_period(i));
+    return o;
+}
+constexpr uint32_t mg_inv(int k) {                // q1^-1 mod q2 (pairs)
+    if (k >= kMgPairs) return 0;
+    for (uint32_t x = 1; x < mg_q2(k); x++)
+        if (x * mg_q1(k) % mg_q2(k) == 1) return x;
+    return 0;
+}
+constexpr uint32_t kPatMWords = mg_off(kMgWin);
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
 constexpr int kLevelBRound = 8;        // level-B primes tested per lane per round
@@ -109,6 +140,7 @@ struct ProfileConst {
     const uint32_t* bitmapC;         // G_q bitmaps of the first nCb level C primes (q < kCBitmapMax)
     uint32_t nCb;
     uint32_t _cpad;
+    const uint32_t* patM;            // merged table-window patterns (standard 22-prime sets; else null)
     // line phases r W^-1 mod q, [line][ptab_stride] u16 (null: computed per
     // work unit): level-A slot i at i, level-B prime p at kSlotB + p; and the
     // constants of those ptab_stride slots
@@ -161,6 +193,7 @@ struct HostProfile {
     uint32_t std_a = 0;
     std::vector<uint32_t> bitmapB, listC;
     std::vector<uint32_t> bitmapC;   // level C primes below kCBitmapMax (PrimeC.off: first word)
+    std::vector<uint32_t> patM;      // merged table windows (std_a 3 or 4: kPatMWords words)
     uint32_t nCb = 0;
     // index of every level-A/B prime for the per-range J0 mod q table
     std::vector<uint32_t> range_primes;   // A slots (kNumA, dummies as 1) then B then C

@@ -108,14 +108,18 @@ cudaError_t launch_phase_table(const Line* lines, uint32_t n_lines, const SlotCo
 cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, uint32_t max_ranges,
                                const uint32_t* primes, uint32_t max_primes, uint32_t* jmod,
                                uint32_t stride, cudaStream_t st);
-size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride);
+// merged: the launch stages the merged table windows of one profile per
+// block (and keeps no per-warp table-window copies)
+size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride, bool merged);
 // lowreg: the register-capped variant (needed for more than the default
-// variant's resident blocks; sweep_needs_lowreg tells)
+// variant's resident blocks; sweep_needs_lowreg tells); merge_slot: the
+// profile slot whose merged table windows the launch uses (every range of the
+// launch must be of that profile, a 22-prime standard set), or -1
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
                          uint32_t b_stride, uint32_t grid, uint32_t block_threads, bool lowreg,
-                         cudaStream_t st);
-bool sweep_needs_lowreg(uint32_t b_stride, uint32_t block_threads, uint32_t blocks_per_sm);
+                         int merge_slot, cudaStream_t st);
+bool sweep_needs_lowreg(uint32_t b_stride, uint32_t block_threads, uint32_t blocks_per_sm, bool merged);
 cudaError_t launch_prove(const ProveArgs& a, uint32_t grid, cudaStream_t st);
 // breadth-first chain walk (prove.cu)
 struct WalkItem {
@@ -191,7 +195,7 @@ struct StagedProve {
 // which: -1 seed, 0 after the top member, 1 after n, 2 after a predecessor, 3 emit
 cudaError_t launch_prove_stage(int which, const StagedProve& p, const WalkItem* in, uint32_t n,
                                cudaStream_t st);
-int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads);
+int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads, bool merged = false);
 
 // engine services used by the q-iteration object (engine.cu); set_error
 // records the message ccs_last_error returns

@@ -71,12 +71,13 @@ struct FilterSet {
     DevBuf<Line> lines;
     DevBuf<PrimeC> primesB, primesC;
     DevBuf<PrimeB> packB;
-    DevBuf<uint32_t> bitmapB, listC, bitmapC, range_primes, patT;
+    DevBuf<uint32_t> bitmapB, listC, bitmapC, range_primes, patT, patM;
     DevBuf<uint16_t> ptab;           // line phase table (may stay empty)
     DevBuf<SlotConst> pq;
     void free_() {
         lines.free_(); primesB.free_(); primesC.free_(); packB.free_();
         bitmapB.free_(); listC.free_(); bitmapC.free_(); range_primes.free_(); patT.free_();
+        patM.free_();
         ptab.free_(); pq.free_();
     }
 };
@@ -207,6 +208,9 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     CU(f.bitmapC.alloc(hp.bitmapC.size()));
     if (!hp.bitmapC.empty())
         CU(cudaMemcpy(f.bitmapC.p, hp.bitmapC.data(), 4 * hp.bitmapC.size(), cudaMemcpyHostToDevice));
+    CU(f.patM.alloc(hp.patM.size()));
+    if (!hp.patM.empty())
+        CU(cudaMemcpy(f.patM.p, hp.patM.data(), 4 * hp.patM.size(), cudaMemcpyHostToDevice));
     CU(f.patT.alloc(hp.patT.size()));
     CU(cudaMemcpy(f.patT.p, hp.patT.data(), 4 * hp.patT.size(), cudaMemcpyHostToDevice));
     CU(f.range_primes.alloc(hp.range_primes.size()));
@@ -232,6 +236,7 @@ ccs_status upload_filter(FilterSet& f, cudaStream_t st) {
     pc.listC = f.listC.p;
     pc.bitmapC = f.bitmapC.p;
     pc.nCb = hp.nCb;
+    pc.patM = hp.patM.empty() ? nullptr : f.patM.p;
     // line phase table for every level-A slot and level-B prime, when it fits
     {
         const uint32_t nb = hp.primesB.empty() ? 1u : (uint32_t)hp.primesB.size();
@@ -295,6 +300,14 @@ uint32_t max_level_b(const ccs_engine* E) {
 uint32_t max_blocks_per_sm(const ccs_engine* E, uint32_t block_threads) {
     const int bps = sweep_blocks_per_sm(b_stride_of(max_level_b(E)), block_threads);
     return bps > 0 ? (uint32_t)bps : 1u;
+}
+
+// A one-range sweep of filter set f uses the merged table windows when the
+// profile has them (22-prime standard sets) and the tuned resident-block
+// count still fits with their per-block copy in shared memory.
+static bool use_merged(const ccs_engine* E, const FilterSet& f, uint32_t b_stride) {
+    return f.hp.patM.size() == kPatMWords && f.slot >= 0 &&
+           sweep_blocks_per_sm(b_stride, E->tune.block_threads, true) >= (int)E->tune.blocks_per_sm;
 }
 
 // (Re)builds the engine's filter sets for a level-B/C split prime and a
@@ -652,9 +665,11 @@ static ccs_status filter_chunk(ccs_engine* E, unsigned __int128 ts, uint64_t n_t
     uint64_t need = (units + wpb - 1) / wpb;
     if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
     const uint32_t bs = b_stride_of((uint32_t)hp.primesB.size());
+    const bool mg = use_merged(E, f, bs);
     CU(launch_sweep(E->d_range.p, E->d_prefix.p, E->d_hdr.p, E->d_jmod.p,
                     (uint32_t)hp.range_primes.size(), bs, grid, E->tune.block_threads,
-                    sweep_needs_lowreg(bs, E->tune.block_threads, E->tune.blocks_per_sm), st));
+                    sweep_needs_lowreg(bs, E->tune.block_threads, E->tune.blocks_per_sm, mg),
+                    mg ? f.slot : -1, st));
     return CCS_OK;
 }
 
@@ -1239,8 +1254,10 @@ ccs_status ccs_filter_range_noalloc(ccs_engine* E, uint64_t ts_lo, uint64_t ts_h
         const uint64_t need = (units + wpb - 1) / wpb;
         if (need < grid) grid = (uint32_t)std::max<uint64_t>(need, 1);
         const uint32_t bs = b_stride_of((uint32_t)f.hp.primesB.size());
+        const bool mg = use_merged(E, f, bs);
         CU(launch_sweep(d_range, d_prefix, d_hdr, d_jmod, np, bs, grid, E->tune.block_threads,
-                        sweep_needs_lowreg(bs, E->tune.block_threads, E->tune.blocks_per_sm), st));
+                        sweep_needs_lowreg(bs, E->tune.block_threads, E->tune.blocks_per_sm, mg),
+                        mg ? f.slot : -1, st));
         E->launches += 2;
     }
     uint32_t* hcnt = (uint32_t*)((char*)E->h_stage + 3072);
@@ -1515,7 +1532,7 @@ static ccs_status batch_capture(ccs_batch* b) {
     b->blocks_per_sm = (b->req_blocks_per_sm == 0 || b->req_blocks_per_sm > (uint32_t)mx)
                            ? (uint32_t)mx : b->req_blocks_per_sm;
     b->grid = (uint32_t)b->prof[0]->sms * b->blocks_per_sm;
-    const bool lowreg = sweep_needs_lowreg(b->b_stride, bt, b->blocks_per_sm);
+    const bool lowreg = sweep_needs_lowreg(b->b_stride, bt, b->blocks_per_sm, false);
     const uint32_t max_ranges = b->max_ranges;
     const size_t nc = b->nc;
     cudaStream_t st = b->stream;
@@ -1528,7 +1545,7 @@ static ccs_status batch_capture(ccs_batch* b) {
     launch_range_setup(b->d_ranges.p, b->d_hdr.p, max_ranges, b->d_primes.p, b->max_range_primes,
                        b->d_jmod.p, b->jstride, st);
     launch_sweep(b->d_ranges.p, b->d_prefix.p, b->d_hdr.p, b->d_jmod.p, b->jstride, b->b_stride,
-                 b->grid, bt, lowreg, st);
+                 b->grid, bt, lowreg, -1, st);
     ProveArgs pa;
     pa.ranges = b->d_pranges.p;
     pa.surv = b->d_surv.p;

@@ -112,6 +112,8 @@ struct SweepArgs {
     const uint32_t* jmod;          // [n_ranges][jmod_stride]
     uint32_t jmod_stride;
     uint32_t b_stride;             // level-B primes per lane column in shared memory
+    uint32_t merge_slot;           // profile whose merged table windows are staged per
+                                   // block (every range of the launch has it), or kNone
 };
 
 // standard level-A sets, with compile-time primes: STD = 1, 2: primes
@@ -283,11 +285,17 @@ __device__ __forceinline__ void b_round(LevelB& B, const SweepArgs& a, const Ran
 // windows are rebuilt from the per-lane phases at the start of every level-A
 // phase, so they are dead while level B runs and its independent tests have
 // the registers.
-template <int STD>
+//
+// MG (standard 22-prime sets only): the table windows are the merged ones
+// (kMgWin patterns of period q1 q2, staged per block at PM) instead of the 22
+// per-prime patterns of the per-warp copy.
+template <int STD, bool MG>
 __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R, const ProfileConst& P,
                                            uint32_t cur_range, uint32_t g, uint32_t w0, uint32_t w1,
                                            uint32_t* Qw, uint32_t* Cw, uint32_t* PA, uint8_t* SA,
-                                           uint16_t* S, uint32_t lane, uint32_t lane_lt) {
+                                           uint16_t* S, const uint32_t* PM, uint32_t lane,
+                                           uint32_t lane_lt) {
+        static_assert(!MG || STD == 3 || STD == 4, "merged windows need the 22-prime standard set");
         const uint32_t* jm = a.jmod + (uint64_t)cur_range * a.jmod_stride;
         const uint32_t li = g * 32 + lane;
         const bool has_line = li < P.n_lines;
@@ -316,7 +324,8 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
         // ---- per-warp pattern copy, per-lane phases at block jbase ----
         for (uint32_t x = lane; x < (uint32_t)kNumAR * 8; x += 32) PA[x] = P.A[x >> 3].ext[x & 7];
         uint32_t* PT = PA + kNumAR * 8;
-        for (uint32_t x = lane; x < P.patT_words; x += 32) PT[x] = __ldg(P.patT + x);
+        if (!MG)
+            for (uint32_t x = lane; x < P.patT_words; x += 32) PT[x] = __ldg(P.patT + x);
         if (P.ptab) {
             // phase = line phase (one table row per line, read with 16-byte
             // loads) + (J0 + jbase) mod q; the second term is the same for
@@ -425,6 +434,21 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                     for (int m = 0; m < 3; m++) A2w[i - kNumA1][m] = __funnelshift_r(pa[m], pa[m + 1], b);
                 }
             }
+            // merged windows: the phase mod q1 q2 from the two phases (CRT)
+            uint32_t Mph[kMgWin];
+            if (MG) {
+#pragma unroll
+                for (int k = 0; k < kMgWin; k++) {
+                    const uint32_t a1 = Tph[mg_slot1(k)];
+                    if (k < kMgPairs) {
+                        const uint32_t q2 = mg_q2(k);
+                        const uint32_t d = (Tph[mg_slot2(k)] + q2 - a1) * mg_inv(k) % q2;   // a1 < q1 < q2
+                        Mph[k] = a1 + mg_q1(k) * d;
+                    } else {
+                        Mph[k] = a1;
+                    }
+                }
+            }
             for (;;) {
                 if (!__any_sync(kFull, (ma | mb) != 0)) {
                     if (w >= w1) break;
@@ -456,9 +480,22 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                         A2w[i][2] = __funnelshift_l(p1, p2, t);
                     }
                     // table windows: 128 pattern bits from the phase, phase += 128 mod q
+                    if (MG) {
+#pragma unroll
+                        for (int k = 0; k < kMgWin; k++) {
+                            const uint32_t ph = Mph[k];
+                            const uint32_t* pt = PM + mg_off(k) + (ph >> 5);
+                            const uint32_t b = ph & 31;
+                            const uint32_t x0 = pt[0], x1 = pt[1], x2 = pt[2], x3 = pt[3], x4 = pt[4];
+                            ka |= ((uint64_t)__funnelshift_r(x1, x2, b) << 32) | __funnelshift_r(x0, x1, b);
+                            kb |= ((uint64_t)__funnelshift_r(x3, x4, b) << 32) | __funnelshift_r(x2, x3, b);
+                            // periods > 128: one subtraction
+                            Mph[k] = min(ph + 128u, ph + 128u - mg_period(k));
+                        }
+                    }
 #pragma unroll
                     for (int i = 0; i < kNumT; i++) {
-                        if (STD && i >= kStdNT[STD]) continue;
+                        if (MG || (STD && i >= kStdNT[STD])) continue;
                         const uint32_t q = STD ? kStdQ[STD][kNumAR + i] : P.A[kNumAR + i].q;
                         const uint32_t toff = STD ? std_toff(i) : P.A[kNumAR + i].toff;
                         const uint32_t ph = Tph[i];
@@ -549,13 +586,23 @@ sweep_kernel(SweepArgs a) {
     const uint32_t lane_lt = (1u << lane) - 1u;
     const uint32_t warp_in_block = threadIdx.x >> 5;
     // per warp: level-B queue (kQCap u32), level-C list (kCCap u32), level-A
-    // patterns (kPAWords u32), level-A phases (kNumA * 32 u8), level-B
-    // phases (b_stride * 32 u16)
-    uint32_t* Qw = s_mem + (size_t)warp_in_block * (kQCap + kCCap + kPAWords + kSAWords + a.b_stride * 16);
+    // patterns (register windows, and the table windows unless merged),
+    // level-A phases (kNumA * 32 u8), level-B phases (b_stride * 32 u16);
+    // then, in a merged launch, the block's merged table windows
+    const bool mlaunch = a.merge_slot < (uint32_t)kMaxProfiles;
+    const uint32_t paw = mlaunch ? (uint32_t)kNumAR * 8 : (uint32_t)kPAWords;
+    const uint32_t ww = kQCap + kCCap + paw + kSAWords + a.b_stride * 16;
+    uint32_t* Qw = s_mem + (size_t)warp_in_block * ww;
     uint32_t* Cw = Qw + kQCap;
     uint32_t* PA = Cw + kCCap;
-    uint8_t* SA = reinterpret_cast<uint8_t*>(PA + kPAWords);
-    uint16_t* S = reinterpret_cast<uint16_t*>(PA + kPAWords + kSAWords);
+    uint8_t* SA = reinterpret_cast<uint8_t*>(PA + paw);
+    uint16_t* S = reinterpret_cast<uint16_t*>(PA + paw + kSAWords);
+    uint32_t* PM = s_mem + (size_t)(blockDim.x >> 5) * ww;
+    if (mlaunch) {
+        const uint32_t* src = c_prof[a.merge_slot].patM;
+        for (uint32_t x = threadIdx.x; x < kPatMWords; x += blockDim.x) PM[x] = __ldg(src + x);
+    }
+    __syncthreads();
     const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
@@ -579,12 +626,23 @@ sweep_kernel(SweepArgs a) {
         const uint32_t wc = (uint32_t)(local / n_groups);
         const uint32_t w0 = wc * R.unit_words;
         const uint32_t w1 = min(w0 + R.unit_words, R.n_words);
+        // a merged launch has no per-warp table-window copies: the host
+        // gives it only ranges of the merged profile (a unit of any other
+        // profile is not swept)
+        if (mlaunch) {
+            if (R.profile != a.merge_slot) continue;
+            if (P.std_a == 3)
+                sweep_unit<3, true>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, PM, lane, lane_lt);
+            else if (P.std_a == 4)
+                sweep_unit<4, true>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, PM, lane, lane_lt);
+            continue;
+        }
         switch (P.std_a) {
-        case 1: sweep_unit<1>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
-        case 2: sweep_unit<2>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
-        case 3: sweep_unit<3>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
-        case 4: sweep_unit<4>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
-        default: sweep_unit<0>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, lane, lane_lt); break;
+        case 1: sweep_unit<1, false>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, PM, lane, lane_lt); break;
+        case 2: sweep_unit<2, false>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, PM, lane, lane_lt); break;
+        case 3: sweep_unit<3, false>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, PM, lane, lane_lt); break;
+        case 4: sweep_unit<4, false>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, PM, lane, lane_lt); break;
+        default: sweep_unit<0, false>(a, R, P, cur_range, g, w0, w1, Qw, Cw, PA, SA, S, PM, lane, lane_lt); break;
         }
     }
 }
@@ -608,9 +666,10 @@ cudaError_t launch_range_setup(const RangeDev* ranges, const SweepHeader* hdr, u
     return cudaGetLastError();
 }
 
-size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride) {
-    return (size_t)(block_threads / 32) * (kQCap + kCCap + kPAWords + kSAWords + (size_t)b_stride * 16) *
-           sizeof(uint32_t);
+size_t sweep_smem_bytes(uint32_t block_threads, uint32_t b_stride, bool merged) {
+    const size_t paw = merged ? (size_t)kNumAR * 8 : (size_t)kPAWords;
+    return ((size_t)(block_threads / 32) * (kQCap + kCCap + paw + kSAWords + (size_t)b_stride * 16) +
+            (merged ? kPatMWords : 0)) * sizeof(uint32_t);
 }
 
 static bool g_sweep_attr_set = false;
@@ -619,7 +678,8 @@ static bool g_sweep_attr_set = false;
 // during stream capture: callers invoke this before capturing)
 static cudaError_t ensure_sweep_attr() {
     if (g_sweep_attr_set) return cudaSuccess;
-    const int lim = (int)sweep_smem_bytes(kSweepThreads, kMaxLevelB);
+    const int lim = (int)std::max(sweep_smem_bytes(kSweepThreads, kMaxLevelB, false),
+                                  sweep_smem_bytes(kSweepThreads, kMaxLevelB, true));
     cudaError_t e = cudaFuncSetAttribute(sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(sweep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -628,30 +688,33 @@ static cudaError_t ensure_sweep_attr() {
 }
 
 // resident blocks per SM of one register variant
-static int sweep_occupancy(bool lowreg, uint32_t b_stride, uint32_t block_threads) {
+static int sweep_occupancy(bool lowreg, uint32_t b_stride, uint32_t block_threads, bool merged) {
     int nb = 0;
     if (ensure_sweep_attr() != cudaSuccess) return 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lowreg ? sweep_kernel<3> : sweep_kernel<2>,
-                                                  (int)block_threads, sweep_smem_bytes(block_threads, b_stride));
+                                                  (int)block_threads,
+                                                  sweep_smem_bytes(block_threads, b_stride, merged));
     return nb;
 }
 
-int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads) {
-    const int a = sweep_occupancy(false, b_stride, block_threads);
-    const int b = sweep_occupancy(true, b_stride, block_threads);
+int sweep_blocks_per_sm(uint32_t b_stride, uint32_t block_threads, bool merged) {
+    const int a = sweep_occupancy(false, b_stride, block_threads, merged);
+    const int b = sweep_occupancy(true, b_stride, block_threads, merged);
     return a > b ? a : b;
 }
 
-bool sweep_needs_lowreg(uint32_t b_stride, uint32_t block_threads, uint32_t blocks_per_sm) {
-    return (int)blocks_per_sm > sweep_occupancy(false, b_stride, block_threads);
+bool sweep_needs_lowreg(uint32_t b_stride, uint32_t block_threads, uint32_t blocks_per_sm, bool merged) {
+    return (int)blocks_per_sm > sweep_occupancy(false, b_stride, block_threads, merged);
 }
 
 cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
                          const SweepHeader* hdr, const uint32_t* jmod, uint32_t stride,
                          uint32_t b_stride, uint32_t grid, uint32_t block_threads, bool lowreg,
-                         cudaStream_t st) {
+                         int merge_slot, cudaStream_t st) {
     if (block_threads != 128 && block_threads != 256) return cudaErrorInvalidValue;
-    size_t smem = sweep_smem_bytes(block_threads, b_stride);
+    if (merge_slot >= kMaxProfiles) return cudaErrorInvalidValue;
+    const bool merged = merge_slot >= 0;
+    size_t smem = sweep_smem_bytes(block_threads, b_stride, merged);
     cudaError_t e = ensure_sweep_attr();
     if (e != cudaSuccess) return e;
     SweepArgs a;
@@ -661,6 +724,7 @@ cudaError_t launch_sweep(const RangeDev* ranges, const uint64_t* unit_prefix,
     a.jmod = jmod;
     a.jmod_stride = stride;
     a.b_stride = b_stride;
+    a.merge_slot = merged ? (uint32_t)merge_slot : kNone;
     if (lowreg) sweep_kernel<3><<<grid, block_threads, smem, st>>>(a);
     else sweep_kernel<2><<<grid, block_threads, smem, st>>>(a);
     return cudaGetLastError();

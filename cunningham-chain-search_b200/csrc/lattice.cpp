@@ -369,6 +369,31 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             if (same) hp.std_a = 1 + v;
         }
     }
+    // merged table windows of the 22-prime standard sets: bit t of window k
+    // is set when t mod q1 (or t mod q2) is a kill phase of that slot, read
+    // from the slot's own pattern (bit x of it, x < q, is the phase x)
+    hp.patM.clear();
+    if (hp.std_a == 3 || hp.std_a == 4) {
+        auto kill = [&](int slot, uint32_t x) {
+            const LevelA& a = hp.A[kNumAR + slot];
+            return (hp.patT[a.toff + (x >> 5)] >> (x & 31)) & 1u;
+        };
+        for (int k = 0; k < kMgWin; k++) {
+            const uint32_t q1 = mg_q1(k), q2 = mg_q2(k), P = mg_period(k);
+            const int s1 = mg_slot1(k), s2 = mg_slot2(k);
+            if (hp.A[kNumAR + s1].q != q1 || (s2 >= 0 && hp.A[kNumAR + s2].q != q2))
+                return "merged table windows do not match the standard set";
+            for (uint32_t wd = 0; wd < t_words(P); wd++) {
+                uint32_t v = 0;
+                for (uint32_t bit = 0; bit < 32; bit++) {
+                    const uint32_t t = (wd * 32 + bit) % P;
+                    if (kill(s1, t % q1) | (s2 >= 0 ? kill(s2, t % q2) : 0u)) v |= 1u << bit;
+                }
+                hp.patM.push_back(v);
+            }
+        }
+        if (hp.patM.size() != kPatMWords) return "merged table windows: size mismatch";
+    }
     hp.range_primes.clear();
     for (int i = 0; i < kNumA; i++) hp.range_primes.push_back(hp.A[i].q);
     for (auto& p : hp.primesB) hp.range_primes.push_back(p.q);
