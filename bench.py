@@ -612,8 +612,9 @@ def section_qiter(ccs, torch, dev, local, steps=8, segs_per_step=256):
     --bits-max 107 --q-order random, extended sieve 509..1009 on): a seeded
     4248-variant synthetic pool, 256 random 2^24-Q chunks per step
     round-robin over the variants, filter then prove, device-timed on one
-    stream; e2e = QIter.run on host segment lists (packing, filter, prove
-    overlapped with the next filter, HIT lines), timed on the host."""
+    stream; e2e = QIter.run on host segment lists (packing beside the
+    filter, proves of groups of steps beside later filters, HIT lines),
+    timed on the host."""
     pool = ccs.synthetic_pool(QITER_CFG["pool"], SEED + 61)
     qi = ccs.QIter(pool, target=QITER_CFG["target"], depth=QITER_CFG["depth"], device=local)
     plan = [qi.pack(p) for p in qiter_plan(ccs, qi, steps + 1, segs_per_step)]

@@ -50,26 +50,39 @@ constexpr uint32_t std_t_prime(int i) {           // table slot i of the standar
 }
 constexpr int mg_slot1(int k) { return k < kMgPairs ? 2 * k : kMgPairs + k; }
 constexpr int mg_slot2(int k) { return k < kMgPairs ? 2 * k + 1 : -1; }
-constexpr uint32_t mg_q1(int k) { return std_t_prime(mg_slot1(k)); }
-constexpr uint32_t mg_q2(int k) { return k < kMgPairs ? std_t_prime(mg_slot2(k)) : 1u; }
-constexpr uint32_t mg_period(int k) { return mg_q1(k) * mg_q2(k); }
-constexpr uint32_t mg_off(int k) {                // first word of window k's pattern
-    uint32_t o = 0;
-    for (int i = 0; i < k; i++) o += t_words(mg_period(i));
-    return o;
+// Per-window constants, built once at compile time (device code indexes the
+// table with unrolled loop counters, so every entry folds to an immediate).
+struct MgWin {
+    uint32_t q1, q2, period, off, inv;   // inv = q1^-1 mod q2 (pairs)
+};
+struct MgTable {
+    MgWin w[kMgWin];
+    uint32_t words;                      // total pattern words
+};
+constexpr MgTable make_mg_table() {
+    MgTable t{};
+    uint32_t off = 0;
+    for (int k = 0; k < kMgWin; k++) {
+        MgWin& m = t.w[k];
+        m.q1 = std_t_prime(mg_slot1(k));
+        m.q2 = k < kMgPairs ? std_t_prime(mg_slot2(k)) : 1u;
+        m.period = m.q1 * m.q2;
+        m.off = off;
+        off += t_words(m.period);
+        m.inv = 0;
+        for (uint32_t x = 1; k < kMgPairs && x < m.q2; x++)
+            if (x * m.q1 % m.q2 == 1) { m.inv = x; break; }
+    }
+    t.words = off;
+    return t;
 }
-constexpr uint32_t mg_inv(int k) {                // q1^-1 mod q2 (pairs)
-    if (k >= kMgPairs) return 0;
-    for (uint32_t x = 1; x < mg_q2(k); x++)
-        if (x * mg_q1(k) % mg_q2(k) == 1) return x;
-    return 0;
-}
-constexpr uint32_t kPatMWords = mg_off(kMgWin);
+constexpr MgTable kMgHost = make_mg_table();
+constexpr uint32_t kPatMWords = kMgHost.words;
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
 constexpr int kLevelBRound = 8;        // level-B primes tested per lane per round
-constexpr uint32_t kCBitmapMax = 8192; // level-C primes below this test a G_q bitmap with
-                                       // 32-bit phase arithmetic (q^2 < 2^32)
+constexpr uint32_t kCBitmapMax = 65536; // level-C primes below this test a G_q bitmap with
+                                        // 32-bit phase arithmetic (q^2 + q < 2^32)
 
 // One bit-sliced ("level A") prime.  Register-window primes (A1, A2) keep
 // their 64/96-bit kill window in registers and advance it by shifts per 64

@@ -133,6 +133,7 @@ __device__ constexpr uint32_t kStdQ[5][kNumA] = {
 #undef CCS_STD_T22
 #undef CCS_NO_T15
 __device__ constexpr int kStdA1[5] = {kNumA1, 7, 6, 7, 6};
+__device__ constexpr MgTable kMg = make_mg_table();   // merged table windows
 __device__ constexpr int kStdNT[5] = {kNumT, 7, 7, 22, 22};
 // pattern-table offset of table-window slot i in a standard set (t_words(q)
 // words per prime, in slot order)
@@ -441,9 +442,9 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
                 for (int k = 0; k < kMgWin; k++) {
                     const uint32_t a1 = Tph[mg_slot1(k)];
                     if (k < kMgPairs) {
-                        const uint32_t q2 = mg_q2(k);
-                        const uint32_t d = (Tph[mg_slot2(k)] + q2 - a1) * mg_inv(k) % q2;   // a1 < q1 < q2
-                        Mph[k] = a1 + mg_q1(k) * d;
+                        const uint32_t q2 = kMg.w[k].q2;
+                        const uint32_t d = (Tph[mg_slot2(k)] + q2 - a1) * kMg.w[k].inv % q2;   // a1 < q1 < q2
+                        Mph[k] = a1 + kMg.w[k].q1 * d;
                     } else {
                         Mph[k] = a1;
                     }
@@ -484,13 +485,13 @@ __device__ __forceinline__ void sweep_unit(const SweepArgs& a, const RangeDev& R
 #pragma unroll
                         for (int k = 0; k < kMgWin; k++) {
                             const uint32_t ph = Mph[k];
-                            const uint32_t* pt = PM + mg_off(k) + (ph >> 5);
+                            const uint32_t* pt = PM + kMg.w[k].off + (ph >> 5);
                             const uint32_t b = ph & 31;
                             const uint32_t x0 = pt[0], x1 = pt[1], x2 = pt[2], x3 = pt[3], x4 = pt[4];
                             ka |= ((uint64_t)__funnelshift_r(x1, x2, b) << 32) | __funnelshift_r(x0, x1, b);
                             kb |= ((uint64_t)__funnelshift_r(x3, x4, b) << 32) | __funnelshift_r(x2, x3, b);
                             // periods > 128: one subtraction
-                            Mph[k] = min(ph + 128u, ph + 128u - mg_period(k));
+                            Mph[k] = min(ph + 128u, ph + 128u - kMg.w[k].period);
                         }
                     }
 #pragma unroll

@@ -379,7 +379,7 @@ std::string build_profile(HostProfile& hp, uint32_t split_prime, uint32_t q0) {
             return (hp.patT[a.toff + (x >> 5)] >> (x & 31)) & 1u;
         };
         for (int k = 0; k < kMgWin; k++) {
-            const uint32_t q1 = mg_q1(k), q2 = mg_q2(k), P = mg_period(k);
+            const uint32_t q1 = kMgHost.w[k].q1, q2 = kMgHost.w[k].q2, P = kMgHost.w[k].period;
             const int s1 = mg_slot1(k), s2 = mg_slot2(k);
             if (hp.A[kNumAR + s1].q != q1 || (s2 >= 0 && hp.A[kNumAR + s2].q != q2))
                 return "merged table windows do not match the standard set";

@@ -283,21 +283,27 @@ class QIter:
         return out[: n.value], pr.value
 
     def run(self, plan, min_report_len=8, surv_cap=1 << 22, chain_cap=1 << 16, pool_primes=None,
-            dedup_p0=True):
-        """Filters and proves a list of steps (each a segment list), the
-        prove of step i overlapping the filter of step i + 1 (two host
-        threads, two streams, two survivor buffers), as the reference
-        overlaps its sieve launches with its CPU prove pool (v16:5700-5800).
-        Returns the totals and the sorted HIT lines."""
+            dedup_p0=True, prove_steps=8, prove_survivors=2048):
+        """Filters and proves a list of steps (each a segment list) as a
+        pipeline of three host threads: the caller's thread packs step i + 1
+        while a filter thread runs the filter of step i on its own stream,
+        and a prover thread proves the survivors of earlier steps beside it,
+        as the reference overlaps its sieve launches with its CPU prove pool
+        (v16:5700-5800).  Survivors are proved in groups of up to
+        `prove_steps` steps (or once `prove_survivors` have collected): a
+        step holds a few dozen survivors, and one prove launch over a group
+        costs about what one over a step costs.  Returns the totals and the
+        sorted HIT lines."""
         import queue
         import threading
         from . import _torch
         torch = _torch()
         dev = f"cuda:{self.device}"
         bufs = [torch.empty((surv_cap, 4), dtype=torch.int32, device=dev) for _ in range(2)]
-        chains = torch.empty((chain_cap, 12), dtype=torch.int32, device=dev)
-        free = [threading.Semaphore(1), threading.Semaphore(1)]
-        work = queue.Queue(maxsize=1)
+        chains = [torch.empty((chain_cap, 12), dtype=torch.int32, device=dev)]
+        fstream = torch.cuda.Stream(device=dev)
+        packed_q = queue.Queue(maxsize=2)
+        work = queue.Queue(maxsize=2)
         tot = {"steps": 0, "q": 0, "survivors": 0, "chains": 0, "primes": 0}
         lines, err = [], []
         seen = set() if dedup_p0 else None
@@ -307,35 +313,77 @@ class QIter:
                 item = work.get()
                 if item is None:
                     return
-                i, segs, surv = item
+                segs, surv = item
                 try:
                     if not err:
-                        c, pr = self.prove(segs, surv, out=chains)
+                        if surv.shape[0] > chains[0].shape[0]:
+                            chains[0] = torch.empty((surv.shape[0], 12), dtype=torch.int32, device=dev)
+                        c, pr = self.prove(segs, surv, out=chains[0])
                         tot["chains"] += c.shape[0]
                         tot["primes"] += pr
                         lines.extend(self.hit_lines(segs, c, min_report_len, pool_primes, seen))
                 except Exception as ex:                   # reported to the caller below
                     err.append(ex)
-                finally:
-                    free[i % 2].release()
 
-        th = threading.Thread(target=prover, daemon=True)
-        th.start()
-        try:
-            for i, segs in enumerate(plan):
-                packed = self.pack(segs)
-                free[i % 2].acquire()
-                if err:
-                    free[i % 2].release()
-                    break
-                s_ = self.filter(packed, out=bufs[i % 2])
-                tot["steps"] += 1
-                tot["q"] += int(packed[: self._nsegs(segs), 4].astype(np.int64).sum())
-                tot["survivors"] += s_.shape[0]
-                work.put((i, packed, s_))
-        finally:
+        def filterer():
+            group = {"segs": [], "surv": [], "steps": 0, "n": 0}
+
+            def flush():
+                if group["segs"] and not err:
+                    # the group's survivors (segment indices into the
+                    # concatenated segment list) are complete on the filter
+                    # stream before the prover, on another stream, reads them
+                    surv = torch.cat(group["surv"])
+                    fstream.synchronize()
+                    work.put((np.concatenate(group["segs"]), surv))
+                group.update(segs=[], surv=[], steps=0, n=0)
+
+            with torch.cuda.stream(fstream):
+                i = 0
+                while True:
+                    packed = packed_q.get()
+                    if packed is None:
+                        break
+                    if err:
+                        continue                          # drain the queue
+                    try:
+                        s_ = self.filter(packed, out=bufs[i % 2], stream=fstream)
+                        n_seg = self._nsegs(packed)
+                        tot["steps"] += 1
+                        tot["q"] += int(packed[:n_seg, 4].astype(np.int64).sum())
+                        tot["survivors"] += s_.shape[0]
+                        base = sum(x.shape[0] for x in group["segs"])
+                        s2 = s_.clone()
+                        if base:
+                            s2[:, 1] += base
+                        group["segs"].append(packed[:n_seg])
+                        group["surv"].append(s2)
+                        group["steps"] += 1
+                        group["n"] += s_.shape[0]
+                        i += 1
+                        if group["steps"] >= prove_steps or group["n"] >= prove_survivors:
+                            flush()
+                    except Exception as ex:               # reported to the caller below
+                        err.append(ex)
+                try:
+                    flush()
+                except Exception as ex:
+                    err.append(ex)
             work.put(None)
-            th.join()
+
+        th_p = threading.Thread(target=prover, daemon=True)
+        th_f = threading.Thread(target=filterer, daemon=True)
+        th_p.start()
+        th_f.start()
+        try:
+            for segs in plan:
+                if err:
+                    break
+                packed_q.put(self.pack(segs))
+        finally:
+            packed_q.put(None)
+            th_f.join()
+            th_p.join()
         if err:
             raise err[0]
         return tot, sorted(lines)
