@@ -274,7 +274,9 @@ def section_prove(ccs, torch, eng, dev, local, n_unique=65536, copies=256, cpu=T
     nums = uniq.repeat(copies, 1).contiguous()
     total = nums.shape[0]
     lengths = torch.zeros(total, dtype=torch.int32, device=dev)
-    eng.walk_numbers_dev(nums[: 1 << 16], 4, lengths[: 1 << 16])       # warm-up
+    # warm-up over the whole batch: the walk's work lists (32 bytes per
+    # number in each of four lists) are reserved here, outside the timing
+    eng.walk_numbers_dev(nums, 4, lengths)
     torch.cuda.synchronize()
     eng.walk_word_products(reset=True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -135,7 +135,7 @@ struct WalkState {
     uint32_t off_region[kMaxLimbs + 1];
     uint32_t n_lucas[kMaxLimbs + 1];     // base-2 probable primes per limb count (from the
                                          // bottom of the region)
-    uint32_t n_lucas5[kMaxLimbs + 1];    // of them with (5/n) = -1 (BPSW; from the top)
+    uint32_t n_lucas_q2[kMaxLimbs + 1];  // of them with Selfridge D = -7 (BPSW; from the top)
     uint32_t n_bits[kWalkBits];          // items needing a test, per bit length
     uint32_t fill_bits[kWalkBits];       // next slot of each bit length in the sorted list
 };

@@ -643,12 +643,17 @@ __device__ int jacobi_small(int D, const Big& nb) {
 // strong Lucas probable-prime test, Selfridge method A (P = 1, Q = (1 - D)/4).
 // SYNC as in strong_prp: a lane whose D search decides the verdict still runs
 // the ladder (on its last D) with the warp and returns its decided verdict.
-template <int NL, bool SYNC = false>
+// Q2: the caller has found the search's answer to be D = -7 ((5/n) = 1,
+// (-7/n) = -1), so Q = 2 and Q^(k+1) = 2 Q^k is a modular doubling instead of
+// a product: three products per bit instead of four, the same verdict.  Every
+// member of a first-kind chain on a lattice with 5 in its CRT primes is -1 mod
+// 5, so (5/n) = 1 and D = -7 is the parameter of about half of them.
+template <int NL, bool SYNC = false, bool Q2 = false>
 __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
-    int D = 5;
+    int D = Q2 ? -7 : 5;
     int tries = 0;
     bool decided = false, dres = false;
-    for (;;) {
+    for (; !Q2;) {
         int j = jacobi_small(D, nb);
         if (j == -1) break;
         if (j == 0) {
@@ -714,7 +719,8 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
         uint32_t X[NL], Y[NL], S[NL];
         montmul<NL>(t1, V0, V1, M.n, M.ninv);
         submod<NL>(t1, t1, Qk, M.n);                // V_2k+1
-        montmul<NL>(t2, Qk, Qm, M.n, M.ninv);       // Q^(k+1)
+        if (Q2) dblmod<NL>(t2, Qk, M.n);            // Q^(k+1)
+        else montmul<NL>(t2, Qk, Qm, M.n, M.ninv);
 #pragma unroll
         for (int i = 0; i < NL; i++) { X[i] = bit ? V1[i] : V0[i]; Y[i] = bit ? t2[i] : Qk[i]; }
         montmul<NL>(S, X, X, M.n, M.ninv);
@@ -723,7 +729,7 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
         montmul<NL>(Qk, Qk, Y, M.n, M.ninv);        // Q^2k or Q^(2k+1)
 #pragma unroll
         for (int i = 0; i < NL; i++) { V0[i] = bit ? t1[i] : S[i]; V1[i] = bit ? S[i] : t1[i]; }
-        M.count += 4;
+        M.count += Q2 ? 3 : 4;
       }
     }
     // V0 = V_d, V1 = V_(d+1), Qk = Q^d
@@ -743,85 +749,6 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
         }
     }
     return decided ? dres : res;
-}
-
-// The strong Lucas test above for the members whose Selfridge parameter is
-// the first one tried, D = 5 ((5/n) = -1, i.e. n = 2 or 3 mod 5): P = 1,
-// Q = -1, so Q^k = (-1)^k and the ladder needs no powers of Q -- two products
-// per bit instead of four, with the same verdict:
-//   V_2k+1 = V_k V_k+1 - (-1)^k,   V_2k = V_k^2 - 2 (-1)^k,
-//   V_2k+2 = V_k+1^2 - 2 (-1)^(k+1),
-// and after the ladder (d odd) V_2d = V_d^2 + 2, then V_2m = V_m^2 - 2.
-// The caller has checked n mod 5; every lane of the warp runs the ladder.
-template <int NL>
-__device__ bool strong_lucas_d5(Mont<NL>& M, const Big& nb) {
-    Big d = nb;
-    {
-        uint32_t c = 1;
-#pragma unroll
-        for (int i = 0; i < kMaxLimbs; i++) {
-            uint64_t s2 = (uint64_t)d.w[i] + c;
-            d.w[i] = (uint32_t)s2;
-            c = (uint32_t)(s2 >> 32);
-        }
-    }
-    int s = 0;
-    while ((d.w[0] & 1u) == 0) {
-#pragma unroll
-        for (int i = 0; i < kMaxLimbs; i++) {
-            uint32_t hi = (i + 1 < kMaxLimbs) ? d.w[i + 1] : 0;
-            d.w[i] = (d.w[i] >> 1) | (hi << 31);
-        }
-        s++;
-    }
-    __syncwarp();
-    uint32_t two[NL], mtwo[NL], V0[NL], V1[NL], t1[NL], S[NL], X[NL], C[NL];
-    dblmod<NL>(two, M.one, M.n);
-    sub_n<NL>(mtwo, M.n, two);
-    // from k = 1: V_1 = P = 1, V_2 = P^2 - 2Q = 3, k odd
-#pragma unroll
-    for (int i = 0; i < NL; i++) V0[i] = M.one[i];
-    addmod<NL>(V1, two, M.one, M.n);
-    bool odd = true;
-    const int top = big_bits(d) - 1;
-#pragma unroll
-    for (int wi = kMaxLimbs - 1; wi >= 0; wi--) {
-      if (32 * wi > top - 1) continue;
-      const uint32_t word = d.w[wi];
-      const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
-      for (int b = hb; b >= 0; b--) {
-        const bool bit = (word >> b) & 1u;
-        montmul<NL>(t1, V0, V1, M.n, M.ninv);
-#pragma unroll
-        for (int i = 0; i < NL; i++) C[i] = odd ? M.one[i] : M.mone[i];
-        addmod<NL>(t1, t1, C, M.n);                                // V_2k+1
-#pragma unroll
-        for (int i = 0; i < NL; i++) { X[i] = bit ? V1[i] : V0[i]; C[i] = (odd != bit) ? two[i] : mtwo[i]; }
-        montmul<NL>(S, X, X, M.n, M.ninv);
-        addmod<NL>(S, S, C, M.n);                                  // V_2k or V_2k+2
-#pragma unroll
-        for (int i = 0; i < NL; i++) { V0[i] = bit ? t1[i] : S[i]; V1[i] = bit ? S[i] : t1[i]; }
-        odd = bit;
-        M.count += 2;
-      }
-    }
-    // V0 = V_d, V1 = V_(d+1); U_d = 0 exactly when 2 V_(d+1) = V_d
-    __syncwarp();
-    bool res = false;
-    dblmod<NL>(t1, V1, M.n);
-    if (eq<NL>(t1, V0) || is_zero<NL>(V0)) {
-        res = true;
-    } else {
-        for (int r = 1; r < s; r++) {
-            montmul<NL>(t1, V0, V0, M.n, M.ninv);
-#pragma unroll
-            for (int i = 0; i < NL; i++) C[i] = r == 1 ? two[i] : mtwo[i];
-            addmod<NL>(V0, t1, C, M.n);                            // Q^d = -1, then Q^(2^r d) = 1
-            M.count += 1;
-            if (is_zero<NL>(V0)) { res = true; break; }
-        }
-    }
-    return res;
 }
 
 // Fermat test to base 2: 2^(n-1) == 1 (mod n), n odd > 2 (the link test of
@@ -1396,9 +1323,10 @@ walk_scatter_kernel(WalkArgs a) {
 template <int NL, uint32_t PRED>
 __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& pc, int stage) {
     // stage 0: the sorted region; stage 1: the base-2 probable primes at the
-    // bottom of the region; stage 2: those with (5/n) = -1, at its top
+    // bottom of the region; stage 2: those whose Selfridge parameter is
+    // D = -7, at its top
     const uint32_t off0 = a.st->off_region[NL];
-    const uint32_t n = stage == 0 ? a.st->n_region[NL] : stage == 1 ? a.st->n_lucas[NL] : a.st->n_lucas5[NL];
+    const uint32_t n = stage == 0 ? a.st->n_region[NL] : stage == 1 ? a.st->n_lucas[NL] : a.st->n_lucas_q2[NL];
     const uint32_t off = stage == 2 ? off0 + a.st->n_region[NL] - n : off0;
     const WalkItem* src = stage == 0 ? a.sorted : a.lucas;
     for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
@@ -1431,7 +1359,7 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
                 to_lucas = strong_prp<NL, true>(M, b, pc.wit[0]);
             }
         } else if (PRED == kPredBPSW && stage == 2) {
-            prime = strong_lucas_d5<NL>(M, b);
+            prime = strong_lucas<NL, true, true>(M, b);
         } else if (PRED == kPredBPSW) {
             prime = strong_lucas<NL, true>(M, b);
         } else if (PRED == kPredMR235) {
@@ -1454,27 +1382,24 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
         if (live && !prime && !to_lucas) a.lengths[it.idx] = it.len;
         walk_count_mm(mm, words);
         if (stage == 0) {
-            // BPSW: members with (5/n) = -1 (n = 2, 3 mod 5) take the D = 5
-            // ladder in a launch of their own
-            bool d5 = false;
+            // BPSW: probable primes whose Selfridge parameter is D = -7
+            // (Q = 2) take the three-product ladder in a launch of their own
+            bool q2 = false;
+            if (PRED == kPredBPSW && to_lucas) q2 = jacobi_small(5, b) == 1 && jacobi_small(-7, b) == -1;
+            const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas && !q2);
             if (PRED == kPredBPSW) {
-                const uint32_t m5 = big_mod_small(b, 5);
-                d5 = m5 == 2 || m5 == 3;
+                const uint32_t pq = warp_append(&a.st->n_lucas_q2[NL], to_lucas && q2);
+                if (to_lucas && q2) a.lucas[off + a.st->n_region[NL] - 1 - pq] = it;
             }
-            const uint32_t pos = warp_append(&a.st->n_lucas[NL], to_lucas && !d5);
-            if (PRED == kPredBPSW) {
-                const uint32_t pos5 = warp_append(&a.st->n_lucas5[NL], to_lucas && d5);
-                if (to_lucas && d5) a.lucas[off + a.st->n_region[NL] - 1 - pos5] = it;
-            }
-            if (to_lucas && !d5) a.lucas[off + pos] = it;
+            if (to_lucas && !q2) a.lucas[off + pos] = it;
         }
         walk_advance(it, nbits, prime, a, pc.kind);
     }
 }
 
 // One kernel per test (PRED), stage (0 = base-2 strong test or the first
-// witness, 1 = strong Lucas test or the other witnesses, 2 = the D = 5 strong
-// Lucas test) and limb count, one
+// witness, 1 = strong Lucas test or the other witnesses, 2 = the strong
+// Lucas test of the members with D = -7) and limb count, one
 // launch per limb count: an SM runs the code of one of them at a time.
 template <uint32_t PRED, int STAGE, int NL>
 __global__ void __launch_bounds__(128, 4)

@@ -283,7 +283,7 @@ class QIter:
         return out[: n.value], pr.value
 
     def run(self, plan, min_report_len=8, surv_cap=1 << 22, chain_cap=1 << 16, pool_primes=None,
-            dedup_p0=True, prove_steps=8, prove_survivors=2048):
+            dedup_p0=True, prove_steps=2, prove_survivors=2048):
         """Filters and proves a list of steps (each a segment list) as a
         pipeline of three host threads: the caller's thread packs step i + 1
         while a filter thread runs the filter of step i on its own stream,
@@ -291,9 +291,10 @@ class QIter:
         as the reference overlaps its sieve launches with its CPU prove pool
         (v16:5700-5800).  Survivors are proved in groups of up to
         `prove_steps` steps (or once `prove_survivors` have collected): a
-        step holds a few dozen survivors, and one prove launch over a group
-        costs about what one over a step costs.  Returns the totals and the
-        sorted HIT lines."""
+        step may hold only a few dozen survivors, whose prove costs about
+        the latency of the longest walk, so a group's prove costs about one
+        step's and still ends beside the next group's filters.  Returns the
+        totals and the sorted HIT lines."""
         import queue
         import threading
         from . import _torch
@@ -301,7 +302,11 @@ class QIter:
         dev = f"cuda:{self.device}"
         bufs = [torch.empty((surv_cap, 4), dtype=torch.int32, device=dev) for _ in range(2)]
         chains = [torch.empty((chain_cap, 12), dtype=torch.int32, device=dev)]
-        fstream = torch.cuda.Stream(device=dev)
+        # one filter stream per instance: the caching allocator keeps the
+        # blocks of earlier runs on it (a new stream would allocate afresh)
+        if getattr(self, "_fstream", None) is None:
+            self._fstream = torch.cuda.Stream(device=dev)
+        fstream = self._fstream
         packed_q = queue.Queue(maxsize=2)
         work = queue.Queue(maxsize=2)
         tot = {"steps": 0, "q": 0, "survivors": 0, "chains": 0, "primes": 0}
