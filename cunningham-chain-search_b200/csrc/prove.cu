@@ -146,7 +146,16 @@ struct Mont {
     uint32_t one[NL];     // R mod n
     uint32_t mone[NL];    // n - (R mod n)  (Montgomery form of -1)
     uint32_t count;       // Montgomery products executed with this context
+    uint32_t sq;          // of them squares (montsqr)
 };
+
+// word products of one Montgomery product (CIOS: NL rows of NL + 1 + NL) and
+// of one square (montsqr: NL (NL - 1)/2 cross + NL diagonal + NL^2 + NL
+// reduction, for the specialised 3 and 4 limbs)
+__host__ __device__ constexpr uint32_t mul_words(int NL) { return 2 * NL * NL + NL; }
+__host__ __device__ constexpr uint32_t sqr_words(int NL) {
+    return (NL == 3 || NL == 4) ? NL * (NL - 1) / 2 + NL + NL * NL + NL : mul_words(NL);
+}
 
 template <int NL>
 __device__ __forceinline__ bool ge(const uint32_t (&a)[NL], const uint32_t (&b)[NL]) {
@@ -498,6 +507,137 @@ __device__ __forceinline__ void montmul<6>(uint32_t (&r)[6], const uint32_t (&a)
     if (t6 || ge<6>(r, n)) sub_n<6>(r, r, n);
 }
 
+// Montgomery square r = a^2 R^{-1} mod n (a < n): the full square first (each
+// cross product a_i a_j, i < j, once, the sum doubled, the squares a_i^2 added
+// on the diagonal), then the NL reduction rows.  NL (NL - 1)/2 + NL word
+// products for the square against NL^2 for a product.  A reduction row adds
+// m n at word i as one carry chain over the low halves and one over the high
+// halves; the carry out of word i + NL is kept in a register and added by the
+// next row (at its own word i + NL), so no row walks the carry to the top.
+// Specialised for 3 and 4 limbs (the members of 65..128 bits); the other
+// limb counts use the product.
+template <int NL>
+__device__ __forceinline__ void montsqr(uint32_t (&r)[NL], const uint32_t (&a)[NL],
+                                        const uint32_t (&n)[NL], uint32_t ninv) {
+    montmul<NL>(r, a, a, n, ninv);
+}
+
+// one reduction row of montsqr<3>: t_i..t_i+3 += m n, p into t_i+3, carry out in q
+#define CCS_SQR_ROW3(T0, T1, T2, T3)                                            \
+    {                                                                           \
+        const uint32_t m = T0 * ninv;                                           \
+        uint32_t q = 0;                                                         \
+        asm("mad.lo.cc.u32 %0, %6, %7, %0;\n\t"                                 \
+            "madc.lo.cc.u32 %1, %6, %8, %1;\n\t"                                \
+            "madc.lo.cc.u32 %2, %6, %9, %2;\n\t"                                \
+            "addc.cc.u32 %3, %3, %5;\n\t"                                       \
+            "addc.u32 %4, %4, 0;\n\t"                                           \
+            "mad.hi.cc.u32 %1, %6, %7, %1;\n\t"                                 \
+            "madc.hi.cc.u32 %2, %6, %8, %2;\n\t"                                \
+            "madc.hi.cc.u32 %3, %6, %9, %3;\n\t"                                \
+            "addc.u32 %4, %4, 0;\n\t"                                           \
+            : "+r"(T0), "+r"(T1), "+r"(T2), "+r"(T3), "+r"(q)                   \
+            : "r"(p), "r"(m), "r"(n[0]), "r"(n[1]), "r"(n[2]));                 \
+        p = q;                                                                  \
+    }
+
+template <>
+__device__ __forceinline__ void montsqr<3>(uint32_t (&r)[3], const uint32_t (&a)[3],
+                                           const uint32_t (&n)[3], uint32_t ninv) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0;
+    asm("mul.lo.u32 %1, %6, %7;\n\t"              // cross products
+        "mul.lo.u32 %2, %6, %8;\n\t"
+        "mad.hi.cc.u32 %2, %6, %7, %2;\n\t"
+        "madc.hi.u32 %3, %6, %8, %3;\n\t"
+        "mad.lo.cc.u32 %3, %7, %8, %3;\n\t"
+        "madc.hi.u32 %4, %7, %8, %4;\n\t"
+        "add.cc.u32 %1, %1, %1;\n\t"              // doubled
+        "addc.cc.u32 %2, %2, %2;\n\t"
+        "addc.cc.u32 %3, %3, %3;\n\t"
+        "addc.cc.u32 %4, %4, %4;\n\t"
+        "addc.u32 %5, %5, 0;\n\t"
+        "mul.lo.u32 %0, %6, %6;\n\t"              // the diagonal
+        "mad.hi.cc.u32 %1, %6, %6, %1;\n\t"
+        "madc.lo.cc.u32 %2, %7, %7, %2;\n\t"
+        "madc.hi.cc.u32 %3, %7, %7, %3;\n\t"
+        "madc.lo.cc.u32 %4, %8, %8, %4;\n\t"
+        "madc.hi.u32 %5, %8, %8, %5;\n\t"
+        : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]));
+    uint32_t p = 0;
+    CCS_SQR_ROW3(t0, t1, t2, t3)
+    CCS_SQR_ROW3(t1, t2, t3, t4)
+    CCS_SQR_ROW3(t2, t3, t4, t5)
+    r[0] = t3; r[1] = t4; r[2] = t5;
+    if (p || ge<3>(r, n)) sub_n<3>(r, r, n);
+}
+#undef CCS_SQR_ROW3
+
+// one reduction row of montsqr<4>: t_i..t_i+4 += m n, p into t_i+4, carry out in q
+#define CCS_SQR_ROW4(T0, T1, T2, T3, T4)                                        \
+    {                                                                           \
+        const uint32_t m = T0 * ninv;                                           \
+        uint32_t q = 0;                                                         \
+        asm("mad.lo.cc.u32 %0, %7, %8, %0;\n\t"                                 \
+            "madc.lo.cc.u32 %1, %7, %9, %1;\n\t"                                \
+            "madc.lo.cc.u32 %2, %7, %10, %2;\n\t"                               \
+            "madc.lo.cc.u32 %3, %7, %11, %3;\n\t"                               \
+            "addc.cc.u32 %4, %4, %6;\n\t"                                       \
+            "addc.u32 %5, %5, 0;\n\t"                                           \
+            "mad.hi.cc.u32 %1, %7, %8, %1;\n\t"                                 \
+            "madc.hi.cc.u32 %2, %7, %9, %2;\n\t"                                \
+            "madc.hi.cc.u32 %3, %7, %10, %3;\n\t"                               \
+            "madc.hi.cc.u32 %4, %7, %11, %4;\n\t"                               \
+            "addc.u32 %5, %5, 0;\n\t"                                           \
+            : "+r"(T0), "+r"(T1), "+r"(T2), "+r"(T3), "+r"(T4), "+r"(q)         \
+            : "r"(p), "r"(m), "r"(n[0]), "r"(n[1]), "r"(n[2]), "r"(n[3]));       \
+        p = q;                                                                  \
+    }
+
+template <>
+__device__ __forceinline__ void montsqr<4>(uint32_t (&r)[4], const uint32_t (&a)[4],
+                                           const uint32_t (&n)[4], uint32_t ninv) {
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0;
+    asm("mul.lo.u32 %1, %8, %9;\n\t"              // cross products
+        "mul.lo.u32 %2, %8, %10;\n\t"
+        "mul.lo.u32 %3, %8, %11;\n\t"
+        "mad.hi.cc.u32 %2, %8, %9, %2;\n\t"
+        "madc.hi.cc.u32 %3, %8, %10, %3;\n\t"
+        "madc.hi.u32 %4, %8, %11, %4;\n\t"
+        "mad.lo.cc.u32 %3, %9, %10, %3;\n\t"
+        "madc.lo.cc.u32 %4, %9, %11, %4;\n\t"
+        "addc.u32 %5, %5, 0;\n\t"
+        "mad.hi.cc.u32 %4, %9, %10, %4;\n\t"
+        "madc.hi.u32 %5, %9, %11, %5;\n\t"
+        "mad.lo.cc.u32 %5, %10, %11, %5;\n\t"
+        "madc.hi.u32 %6, %10, %11, %6;\n\t"
+        "add.cc.u32 %1, %1, %1;\n\t"              // doubled
+        "addc.cc.u32 %2, %2, %2;\n\t"
+        "addc.cc.u32 %3, %3, %3;\n\t"
+        "addc.cc.u32 %4, %4, %4;\n\t"
+        "addc.cc.u32 %5, %5, %5;\n\t"
+        "addc.cc.u32 %6, %6, %6;\n\t"
+        "addc.u32 %7, %7, 0;\n\t"
+        "mul.lo.u32 %0, %8, %8;\n\t"              // the diagonal
+        "mad.hi.cc.u32 %1, %8, %8, %1;\n\t"
+        "madc.lo.cc.u32 %2, %9, %9, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, %9, %3;\n\t"
+        "madc.lo.cc.u32 %4, %10, %10, %4;\n\t"
+        "madc.hi.cc.u32 %5, %10, %10, %5;\n\t"
+        "madc.lo.cc.u32 %6, %11, %11, %6;\n\t"
+        "madc.hi.u32 %7, %11, %11, %7;\n\t"
+        : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]));
+    uint32_t p = 0;
+    CCS_SQR_ROW4(t0, t1, t2, t3, t4)
+    CCS_SQR_ROW4(t1, t2, t3, t4, t5)
+    CCS_SQR_ROW4(t2, t3, t4, t5, t6)
+    CCS_SQR_ROW4(t3, t4, t5, t6, t7)
+    r[0] = t4; r[1] = t5; r[2] = t6; r[3] = t7;
+    if (p || ge<4>(r, n)) sub_n<4>(r, r, n);
+}
+#undef CCS_SQR_ROW4
+
 
 template <int NL>
 __device__ __forceinline__ void mont_setup(Mont<NL>& M, const Big& nb, int nbits) {
@@ -590,8 +730,9 @@ __device__ bool strong_prp(Mont<NL>& M, const Big& nb, uint32_t a) {
         const uint32_t word = d.w[wi];
         const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
         for (int b = hb; b >= 0; b--) {
-            montmul<NL>(x, x, x, M.n, M.ninv);
+            montsqr<NL>(x, x, M.n, M.ninv);
             M.count++;
+            M.sq++;
             if ((word >> b) & 1u) {
                 if (a == 2) dblmod<NL>(x, x, M.n);
                 else { montmul<NL>(x, x, am, M.n, M.ninv); M.count++; }
@@ -601,8 +742,9 @@ __device__ bool strong_prp(Mont<NL>& M, const Big& nb, uint32_t a) {
     if (SYNC) __syncwarp();
     if (eq<NL>(x, M.one) || eq<NL>(x, M.mone)) return true;
     for (int r = 1; r < s; r++) {
-        montmul<NL>(x, x, x, M.n, M.ninv);
+        montsqr<NL>(x, x, M.n, M.ninv);
         M.count++;
+        M.sq++;
         if (eq<NL>(x, M.mone)) return true;
         if (eq<NL>(x, M.one)) return false;
     }
@@ -723,13 +865,21 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
         else montmul<NL>(t2, Qk, Qm, M.n, M.ninv);
 #pragma unroll
         for (int i = 0; i < NL; i++) { X[i] = bit ? V1[i] : V0[i]; Y[i] = bit ? t2[i] : Qk[i]; }
-        montmul<NL>(S, X, X, M.n, M.ninv);
+        montsqr<NL>(S, X, M.n, M.ninv);
         dblmod<NL>(X, Y, M.n);
         submod<NL>(S, S, X, M.n);                   // V_2k (bit 0) or V_2k+2 (bit 1)
-        montmul<NL>(Qk, Qk, Y, M.n, M.ninv);        // Q^2k or Q^(2k+1)
+        if (Q2) {                                   // Q^2k, or 2 Q^2k = Q^(2k+1)
+            montsqr<NL>(Qk, Qk, M.n, M.ninv);
+            dblmod<NL>(X, Qk, M.n);
+#pragma unroll
+            for (int i = 0; i < NL; i++) Qk[i] = bit ? X[i] : Qk[i];
+        } else {
+            montmul<NL>(Qk, Qk, Y, M.n, M.ninv);    // Q^2k or Q^(2k+1)
+        }
 #pragma unroll
         for (int i = 0; i < NL; i++) { V0[i] = bit ? t1[i] : S[i]; V1[i] = bit ? S[i] : t1[i]; }
         M.count += Q2 ? 3 : 4;
+        M.sq += Q2 ? 2 : 1;
       }
     }
     // V0 = V_d, V1 = V_(d+1), Qk = Q^d
@@ -740,12 +890,13 @@ __device__ bool strong_lucas(Mont<NL>& M, const Big& nb) {
         res = true;
     } else {
         for (int r = 1; r < s; r++) {
-            montmul<NL>(t1, V0, V0, M.n, M.ninv);
+            montsqr<NL>(t1, V0, M.n, M.ninv);
             dblmod<NL>(t2, Qk, M.n);
             submod<NL>(V0, t1, t2, M.n);
             if (is_zero<NL>(V0)) { res = true; break; }
-            montmul<NL>(Qk, Qk, Qk, M.n, M.ninv);
+            montsqr<NL>(Qk, Qk, M.n, M.ninv);
             M.count += 2;
+            M.sq += 2;
         }
     }
     return decided ? dres : res;
@@ -769,8 +920,9 @@ __device__ bool fermat2(Mont<NL>& M, const Big& nb) {
         const uint32_t word = e.w[wi];
         const int hb = (32 * wi + 31 > top - 1) ? (top - 1 - 32 * wi) : 31;
         for (int b = hb; b >= 0; b--) {
-            montmul<NL>(x, x, x, M.n, M.ninv);
+            montsqr<NL>(x, x, M.n, M.ninv);
             M.count++;
+            M.sq++;
             if ((word >> b) & 1u) dblmod<NL>(x, x, M.n);
         }
     }
@@ -783,6 +935,7 @@ __device__ bool prp_suite(const Big& nb, int nbits, uint32_t pred, const ProveCo
     Mont<NL> M;
     mont_setup<NL>(M, nb, nbits);
     M.count = 0;
+    M.sq = 0;
     bool r = true;
     if (pred == kPredBPSW) {
         r = strong_prp<NL>(M, nb, 2) && strong_lucas<NL>(M, nb);
@@ -1345,6 +1498,7 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
         Mont<NL> M;
         mont_setup<NL>(M, b, nbits);
         M.count = 0;
+        M.sq = 0;
         __syncwarp();
         if (stage == 0) {
             // the first test for every member; the rest only for its
@@ -1378,7 +1532,8 @@ __device__ __forceinline__ void walk_test_region(WalkArgs& a, const ProveConst& 
         prime = prime && live;
         to_lucas = to_lucas && live;
         const uint32_t mm = live ? M.count : 0u;
-        const uint32_t words = mm * (2 * NL * NL + NL);
+        const uint32_t msq = live ? M.sq : 0u;
+        const uint32_t words = (mm - msq) * mul_words(NL) + msq * sqr_words(NL);
         if (live && !prime && !to_lucas) a.lengths[it.idx] = it.len;
         walk_count_mm(mm, words);
         if (stage == 0) {
