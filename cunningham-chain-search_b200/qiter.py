@@ -335,11 +335,10 @@ class QIter:
 
             def flush():
                 if group["segs"] and not err:
-                    # the group's survivors (segment indices into the
-                    # concatenated segment list) are complete on the filter
-                    # stream before the prover, on another stream, reads them
-                    surv = torch.cat(group["surv"])
-                    fstream.synchronize()
+                    # the group's survivors, segment indices into the
+                    # concatenated segment list, back on the device (a copy
+                    # from host memory: complete when it returns)
+                    surv = torch.from_numpy(np.concatenate(group["surv"])).to(dev)
                     work.put((np.concatenate(group["segs"]), surv))
                 group.update(segs=[], surv=[], steps=0, n=0)
 
@@ -357,8 +356,11 @@ class QIter:
                         tot["steps"] += 1
                         tot["q"] += int(packed[:n_seg, 4].astype(np.int64).sum())
                         tot["survivors"] += s_.shape[0]
+                        # survivors are few (tens per step): offset their
+                        # segment indices on the host, so the pipeline runs
+                        # copies only, no kernels of its own
                         base = sum(x.shape[0] for x in group["segs"])
-                        s2 = s_.clone()
+                        s2 = s_.cpu().numpy()
                         if base:
                             s2[:, 1] += base
                         group["segs"].append(packed[:n_seg])
