@@ -1432,19 +1432,43 @@ __host__ __device__ constexpr int limbs_of_bits(int nbits) {
 
 // members sorted by bit length: ascending lengths, so the regions of one
 // limb count are contiguous, and the warps of a test run members of one
-// length (the same exponent loop lengths)
-__global__ void walk_regions_kernel(WalkState* st) {
-    if (threadIdx.x == 0) {
-        for (int nl = 0; nl <= kMaxLimbs; nl++) { st->n_region[nl] = 0; st->off_region[nl] = 0; }
-        uint32_t o = 0;
-        int cur = -1;
-        for (int b = 0; b < kWalkBits; b++) {
-            const int nl = limbs_of_bits(b);
-            if (nl != cur) { st->off_region[nl] = o; cur = nl; }
+// length (the same exponent loop lengths).  One warp: each lane sums seven
+// bit lengths, a warp scan gives the offsets.
+__global__ void __launch_bounds__(32) walk_regions_kernel(WalkState* st) {
+    constexpr int kPer = (kWalkBits + 31) / 32;
+    const uint32_t lane = threadIdx.x;
+    uint32_t v[kPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        const int b = (int)lane * kPer + k;
+        v[k] = b < kWalkBits ? st->n_bits[b] : 0u;
+        sum += v[k];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    uint32_t o = incl - sum;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        const int b = (int)lane * kPer + k;
+        if (b < kWalkBits) {
             st->fill_bits[b] = o;
-            st->n_region[nl] += st->n_bits[b];
-            o += st->n_bits[b];
+            if (b == 0 || limbs_of_bits(b) != limbs_of_bits(b - 1)) st->off_region[limbs_of_bits(b)] = o;
         }
+        o += v[k];
+    }
+    __syncwarp();
+    if (lane == 0) {
+        // regions of limb counts 2..kMaxLimbs in ascending order (bit
+        // lengths 0..64 take 2 limbs), each ending where the next begins
+        st->n_region[0] = st->n_region[1] = 0;
+        st->off_region[0] = st->off_region[1] = 0;
+        for (int nl = limbs_of_bits(0); nl <= kMaxLimbs; nl++)
+            st->n_region[nl] = (nl < kMaxLimbs ? st->off_region[nl + 1] : total) - st->off_region[nl];
     }
 }
 
