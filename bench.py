@@ -1007,8 +1007,11 @@ def run_ours(args):
         except Exception as ex:
             headline_mm = {"error": repr(ex)}
 
+    # the CPU baseline and the sections after the headline run at N = 1 only:
+    # a multi-GPU run reports the headline (the other ranks would wait in the
+    # final barrier while rank 0 ran them)
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         s = v33_sample(BITS, 16)
         if s:
             cpu = {"value": s["rate"], "unit": "candidates/s", "cores": s["cores"], "kind": "reference",
@@ -1018,7 +1021,7 @@ def run_ours(args):
                               f"{s['seconds']:.1f} s (reference stage primes 37..863 on the same "
                               f"W=31# depth-16 lattice)")}
     extra = {}
-    if rank == 0 and not args.headline_only:
+    if rank == 0 and ws == 1 and not args.headline_only:
         try:
             extra["prove"] = section_prove(ccs, torch, eng, dev, local)
         except Exception as ex:                       # report, keep the headline
