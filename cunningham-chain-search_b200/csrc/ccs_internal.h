@@ -80,7 +80,7 @@ constexpr MgTable kMgHost = make_mg_table();
 constexpr uint32_t kPatMWords = kMgHost.words;
 constexpr int kMaxProfiles = 16;
 constexpr int kMaxLevelB = 256;        // per-lane cached phases (shared memory)
-constexpr int kLevelBRound = 8;        // level-B primes tested per lane per round
+constexpr int kLevelBRound = 6;        // level-B primes tested per lane per round
 constexpr uint32_t kCBitmapMax = 65536; // level-C primes below this test a G_q bitmap with
                                         // 32-bit phase arithmetic (q^2 + q < 2^32)
 

@@ -285,8 +285,12 @@ ccs_status upload_prove(ccs_engine* E, cudaStream_t st) {
     return CCS_OK;
 }
 
+// level-B phase rows per lane column in shared memory: the level-B records
+// padded to a whole number of rounds (the rows the rounds read), rounded up
+// to 8 rows (the phase-table rows are read 8 at a time)
 uint32_t b_stride_of(uint32_t nB) {
     uint32_t s = nB ? nB : 1;
+    s = (s + kLevelBRound - 1) / kLevelBRound * kLevelBRound;
     return (s + 7) & ~7u;
 }
 
